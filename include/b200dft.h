@@ -1,0 +1,124 @@
+/* b200dft C ABI: B200 (sm_100a) kernels for the restricted Kohn-Sham SCF hot path of
+ * pyscf-ipu.  Plain C types only.  Device buffers are caller-owned device pointers;
+ * `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).  Every
+ * function returns 0 on success or a negative B2_ERR_* code; nothing throws across the ABI.
+ *
+ * Molecules enter as the libcint atm/bas/env arrays that the reference packs for its own
+ * native ERI code (pyscf_ipu/electron_repulsion/direct.py:710-739 prepare_int_floats /
+ * prepare_integrals_2_inputs; consumed by int2e_sph, int2e_sph.cpp:6750).  A batch is the
+ * concatenation of each molecule's atm rows (6 ints), bas rows (8 ints) and env segment;
+ * pointers inside atm/bas are relative to the molecule's env segment (env_off[m]).
+ *
+ * Per-molecule device layouts (offsets from b2_plan_offsets):
+ *   s8 ERIs:   eri_off[m] + ij(ij+1)/2 + kl, ij = i(i+1)/2 + j, i>=j, k>=l, ij>=kl
+ *   matrices:  mat_off[m] + a*nao + b (row-major nao x nao, float64)
+ *   AO values: ao_off[m] + (c*G + g)*nao + n, c = value, d/dx, d/dy, d/dz
+ *   grid:      grid_off[m] + g (coords: 3 doubles per point)
+ */
+#ifndef B200DFT_H
+#define B200DFT_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B2_OK 0
+#define B2_ERR_ARG (-1)
+#define B2_ERR_CUDA (-2)
+#define B2_ERR_UNSUPPORTED (-3)
+#define B2_ERR_SIZE (-4)
+#define B2_ERR_NOT_PD (-5)
+#define B2_ERR_TIMEOUT (-6)
+
+typedef void *b2_plan_t;
+
+/* Library/ABI version (major*10000 + minor*100 + patch). */
+int b2_version(void);
+
+/* Last CUDA error string seen by the library (for diagnostics). */
+const char *b2_last_error(void);
+
+/* Build a batch plan from host libcint arrays and upload its tables to the current device.
+ * Replaces the host preparation of the reference's ERI path: prepare_int_floats and
+ * prepare_integrals_2_inputs (electron_repulsion/direct.py:710-944). */
+int b2_plan_create(int nmol, const int *natm, const int *nbas, const int *atm, const int *bas,
+                   const double *env, const int64_t *env_off, b2_plan_t *plan);
+int b2_plan_destroy(b2_plan_t plan);
+
+/* info[0..7] = n_eri_total, n_mat_total, nmol, max_nao, n_rows_total, n_shell_pairs,
+ *              jk_chunk, jk_nchunks */
+int b2_plan_info(b2_plan_t plan, int64_t *info);
+
+/* Host copies of per-molecule offsets/sizes (arrays of nmol). */
+int b2_plan_offsets(b2_plan_t plan, int64_t *eri_off, int64_t *mat_off, int *nao, int *nocc);
+
+/* Re-split the J/K work: `elems` s8 entries per CTA (0 = default policy). */
+int b2_plan_set_jk_chunk(b2_plan_t plan, int64_t elems);
+
+/* All unique ERIs of every molecule into the s8 layout, precision 64 (float64 out) or 32
+ * (float32 out).  Replaces int2e_sph (int2e_sph.cpp:6750) dispatched per shell quartet by
+ * compute_integrals_2 / integrals_v1 (direct.py:506-707), and mol.intor('int2e_sph',
+ * aosym='s8') (nanoDFT.py:285). */
+int b2_eri_s8(b2_plan_t plan, int precision, void *eri_out, void *stream);
+
+/* J and K (float64, nao x nao per molecule) from the s8 list and D (float64).  Arithmetic in
+ * `precision` (64 or 32, must match the ERI buffer).  Replaces sparse_symmetric_einsum
+ * (nanoDFT/sparse_symmetric_ERI.py:86) and ipu_direct_mult (electron_repulsion/direct.py:489);
+ * diff_JK = J - K*hyb/2 as in get_JK (nanoDFT.py:125-139). */
+int b2_jk_s8(b2_plan_t plan, int precision, const void *eri, const double *D, double *J,
+             double *K, void *stream);
+
+/* Register the grid layout: grid_off (host, nmol+1 prefix of per-molecule point counts).
+ * Allocates the plan's grid tables and XC scratch on the device. */
+int b2_grid_set(b2_plan_t plan, const int64_t *grid_off);
+/* Size (elements) of the AO buffer for the registered grid: sum_m 4*G_m*nao_m. */
+int b2_grid_info(b2_plan_t plan, int64_t *n_points, int64_t *n_ao);
+int b2_grid_ao_offsets(b2_plan_t plan, int64_t *ao_off);
+
+/* AO values and gradients on the grid (replaces mol.eval_gto('GTOval_sph_deriv1', coords, 4),
+ * dft.py:220).  coords: device float64 (n_points x 3); ao: device, precision 64 or 32. */
+int b2_ao_eval(b2_plan_t plan, int precision, const double *coords, void *ao, void *stream);
+
+/* E_xc (nmol float64) and symmetric V_xc (float64 matrices) for densities D; replaces
+ * exchange_correlation (nanoDFT.py:105-123) / xc (dft.py:899-1036) minus the J/K part. */
+int b2_xc(b2_plan_t plan, int precision, const void *ao, const double *weights, const double *D,
+          double *Vxc, double *Exc, void *stream);
+
+/* B3LYP at n points: rho (4 x n, device float64, rho[1:4] = half density gradient as the
+ * reference forms it) -> e_xc, vrho, vgamma (device float64).  Replaces b3lyp(rho, eps)
+ * (exchange_correlation/b3lyp.py:13). */
+int b2_b3lyp(int64_t n, const double *rho, double *exc, double *vrho, double *vgamma,
+             void *stream);
+
+/* L = inv(cholesky(S)) per molecule (dft.py:234, nanoDFT.py:239); status[m] = 0 or
+ * B2_ERR_NOT_PD (device int array, may be NULL). */
+int b2_chol_inv(b2_plan_t plan, const double *S, double *Linv, int *status, void *stream);
+
+/* One Fock build + DIIS step per molecule (nanoDFT.py:63-66, DIIS 338-364).  active (device
+ * int[nmol] or NULL = all), iter (device int[nmol]: the molecule's iteration index).
+ * ring_err / ring_h: device float64, 9 * n_mat each; bmat: device float64 100 * nmol;
+ * diis_err: device float64 [nmol] (max |SDH - HDS|). */
+int b2_fock_diis(b2_plan_t plan, const int *active, const int *iter, double hyb, int use_diis,
+                 const double *Hcore, const double *S, const double *D, const double *J,
+                 const double *K, const double *Vxc, double *H, double *diffJK, double *ring_err,
+                 double *ring_h, double *bmat, double *diis_err, void *stream);
+
+/* C = L^T eigvec(L H L^T), D = 2 C_occ C_occ^T (nanoDFT.py:68-72).  mo_energy: device float64
+ * nmol x 72 (ascending, first nao valid); C may be NULL; sweeps (device int[nmol]) may be NULL. */
+int b2_eigh_density(b2_plan_t plan, const int *active, const double *H, const double *Linv,
+                    double *D, double *mo_energy, double *C, int *sweeps, void *stream);
+
+/* energies (device float64 nmol x 5): [E, E_core, E_J_K/2, E_xc, E_nuc] (nanoDFT.py:20-38) */
+int b2_energy(b2_plan_t plan, const int *active, const double *D, const double *Hcore,
+              const double *diffJK, const double *Exc, const double *Enuc, double *out,
+              void *stream);
+
+/* Single-molecule convenience mirroring the reference's native entry int2e_sph
+ * (int2e_sph.cpp:6750): host libcint arrays in, all s8 ERIs of the molecule out (device). */
+int b2_int2e_sph_s8(const int *atm, int natm, const int *bas, int nbas, const double *env,
+                    int n_env, int precision, void *eri_out, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

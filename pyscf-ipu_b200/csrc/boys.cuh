@@ -1,0 +1,67 @@
+// Boys function F_m(T) = int_0^1 u^{2m} exp(-T u^2) du for the ERI kernels.
+//
+// T < B2_BOYS_TMAX: Taylor expansion of F_L around the nearest tabulated point T_k = k*dT
+//   (dF_m/dT = -F_{m+1}), then downward recursion F_m = (2T F_{m+1} + e^{-T}) / (2m+1),
+//   which is stable.  The table holds F_0..F_{B2_BOYS_NM-1} at every T_k and is filled on
+//   the host in double precision by the convergent series
+//   F_m(T) = e^{-T} sum_k (2T)^k / ((2m+1)(2m+3)...(2m+2k+1)).
+// T >= B2_BOYS_TMAX: F_0 = sqrt(pi/T)/2 (erf(sqrt T) = 1 to double precision) and upward
+//   recursion F_{m+1} = ((2m+1) F_m - e^{-T}) / (2T), stable for large T.
+#pragma once
+#include "common.cuh"
+
+#define B2_BOYS_DT 0.125
+#define B2_BOYS_INV_DT 8.0
+#define B2_BOYS_TMAX 40.0
+#define B2_BOYS_NT 322          // T_k = k*DT, k = 0..321 (covers TMAX + DT/2)
+#define B2_BOYS_NM 14           // m = 0..13 (L <= 4 plus 9 Taylor terms)
+
+// host: fill table[k*NM + m]
+static void b2_boys_fill_table(double *table) {
+  for (int k = 0; k < B2_BOYS_NT; ++k) {
+    double t = k * B2_BOYS_DT;
+    int mmax = B2_BOYS_NM - 1;
+    double term = 1.0 / (2 * mmax + 1), sum = term;
+    for (int j = 1; j < 2000; ++j) {
+      term *= 2.0 * t / (2 * mmax + 2 * j + 1);
+      sum += term;
+      if (term < 1e-20 * sum) break;
+    }
+    double et = exp(-t);
+    double f[B2_BOYS_NM];
+    f[mmax] = et * sum;
+    for (int m = mmax - 1; m >= 0; --m) f[m] = (2.0 * t * f[m + 1] + et) / (2 * m + 1);
+    for (int m = 0; m < B2_BOYS_NM; ++m) table[k * B2_BOYS_NM + m] = f[m];
+  }
+}
+
+template <typename T> struct B2BoysTerms;
+template <> struct B2BoysTerms<double> { static constexpr int n = 9; };
+template <> struct B2BoysTerms<float> { static constexpr int n = 6; };
+
+// F[0..L] at T; `table` is the double table (device global or host memory).
+template <typename T, int L>
+B2_HD void b2_boys(T t, const double *__restrict__ table, T *F) {
+  if (t < (T)B2_BOYS_TMAX) {
+    int k = (int)(t * (T)B2_BOYS_INV_DT + (T)0.5);
+    T dt = (T)(k * B2_BOYS_DT) - t;           // T_k - T
+    const double *row = table + k * B2_BOYS_NM + L;
+    constexpr int NT = B2BoysTerms<T>::n;
+    // Horner: sum_j F_{L+j}(T_k) dt^j / j!
+    T acc = (T)row[NT - 1];
+#pragma unroll
+    for (int j = NT - 1; j >= 1; --j) acc = (T)row[j - 1] + acc * dt / (T)j;
+    F[L] = acc;
+    if (L > 0) {
+      T et = exp(-t);
+      T t2 = t + t;
+#pragma unroll
+      for (int m = L - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + et) / (T)(2 * m + 1);
+    }
+  } else {
+    T inv = (T)1 / t;
+    F[0] = (T)0.886226925452758014 * sqrt(inv);      // sqrt(pi)/2 / sqrt(T)
+#pragma unroll
+    for (int m = 0; m < L; ++m) F[m + 1] = (T)(2 * m + 1) * (T)0.5 * inv * F[m];
+  }
+}

@@ -1,0 +1,217 @@
+// extern "C" entry points of libb200dft.so (declared in include/b200dft.h).
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <algorithm>
+#include "device_plan.cuh"
+#include "xc.cuh"
+#include "scf.cuh"
+#include "xc_math.cuh"
+
+static thread_local std::string g_last_error;
+
+static int b2_note(cudaError_t e) {
+  if (e != cudaSuccess) { g_last_error = cudaGetErrorString(e); return B2_ERR_CUDA; }
+  return B2_OK;
+}
+
+#define B2_TRY(x) do { int _rc = b2_note(x); if (_rc) return _rc; } while (0)
+
+template <typename T>
+static int b2_upload(T **dst, const std::vector<T> &src) {
+  size_t n = std::max<size_t>(1, src.size());
+  B2_TRY(cudaMalloc((void **)dst, sizeof(T) * n));
+  if (!src.empty()) B2_TRY(cudaMemcpy(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice));
+  return B2_OK;
+}
+
+static void b2_plan_free(B2PlanDev *P) {
+  if (!P) return;
+  b2_grid_free(*P);
+  cudaFree(P->mols); cudaFree(P->row_off); cudaFree(P->shells); cudaFree(P->pinfo);
+  cudaFree(P->pp64); cudaFree(P->pp32); cudaFree(P->ao2sh); cudaFree(P->cls_list);
+  cudaFree(P->cls_cnt); cudaFree(P->atom_xyz); cudaFree(P->atom_z); cudaFree(P->boys);
+  cudaFree(P->jk_chunk_off);
+  delete P;
+}
+
+static int b2_set_jk_chunk(B2PlanDev *P, long long elems) {
+  if (elems <= 0) elems = 32768;
+  const int nmol = P->h.nmol;
+  std::vector<long long> off(nmol + 1, 0);
+  for (int m = 0; m < nmol; ++m) off[m + 1] = off[m] + (P->h.mols[m].n4 + elems - 1) / elems;
+  cudaFree(P->jk_chunk_off);
+  P->jk_chunk_off = nullptr;
+  int rc = b2_upload(&P->jk_chunk_off, off);
+  if (rc) return rc;
+  P->jk_chunk = elems;
+  P->jk_nchunks = off[nmol];
+  return B2_OK;
+}
+
+extern "C" {
+
+int b2_version(void) { return 100; }
+
+const char *b2_last_error(void) { return g_last_error.c_str(); }
+
+int b2_plan_create(int nmol, const int *natm, const int *nbas, const int *atm, const int *bas,
+                   const double *env, const int64_t *env_off, void **plan) {
+  if (nmol <= 0 || !natm || !nbas || !atm || !bas || !env || !env_off || !plan) return B2_ERR_ARG;
+  B2PlanDev *P = new B2PlanDev();
+  int rc = b2_plan_build(P->h, nmol, natm, nbas, atm, bas, env, (const long long *)env_off);
+  if (rc) { delete P; return rc; }
+  std::vector<double> tab(B2_BOYS_NT * B2_BOYS_NM);
+  b2_boys_fill_table(tab.data());
+  std::vector<B2MolDev> mols = P->h.mols;
+  if ((rc = b2_upload(&P->mols, mols)) || (rc = b2_upload(&P->row_off, P->h.row_off)) ||
+      (rc = b2_upload(&P->shells, P->h.shells)) || (rc = b2_upload(&P->pinfo, P->h.pinfo)) ||
+      (rc = b2_upload(&P->pp64, P->h.pp64)) || (rc = b2_upload(&P->pp32, P->h.pp32)) ||
+      (rc = b2_upload(&P->ao2sh, P->h.ao2sh)) || (rc = b2_upload(&P->cls_list, P->h.cls_list)) ||
+      (rc = b2_upload(&P->cls_cnt, P->h.cls_cnt)) || (rc = b2_upload(&P->atom_xyz, P->h.atom_xyz)) ||
+      (rc = b2_upload(&P->atom_z, P->h.atom_z)) || (rc = b2_upload(&P->boys, tab)) ||
+      (rc = b2_set_jk_chunk(P, 0))) {
+    b2_plan_free(P);
+    return rc;
+  }
+  cudaGetDevice(&P->device);
+  *plan = P;
+  return B2_OK;
+}
+
+int b2_plan_destroy(void *plan) {
+  b2_plan_free((B2PlanDev *)plan);
+  return B2_OK;
+}
+
+int b2_plan_info(void *plan, int64_t *info) {
+  if (!plan || !info) return B2_ERR_ARG;
+  B2PlanDev *P = (B2PlanDev *)plan;
+  info[0] = P->h.n_eri; info[1] = P->h.n_mat; info[2] = P->h.nmol; info[3] = P->h.max_nao;
+  info[4] = P->h.n_rows; info[5] = P->h.n_sp; info[6] = P->jk_chunk; info[7] = P->jk_nchunks;
+  return B2_OK;
+}
+
+int b2_plan_offsets(void *plan, int64_t *eri_off, int64_t *mat_off, int *nao, int *nocc) {
+  if (!plan) return B2_ERR_ARG;
+  B2PlanDev *P = (B2PlanDev *)plan;
+  for (int m = 0; m < P->h.nmol; ++m) {
+    if (eri_off) eri_off[m] = P->h.mols[m].eri_off;
+    if (mat_off) mat_off[m] = P->h.mols[m].mat_off;
+    if (nao) nao[m] = P->h.mols[m].nao;
+    if (nocc) nocc[m] = P->h.mols[m].nocc;
+  }
+  return B2_OK;
+}
+
+int b2_plan_set_jk_chunk(void *plan, int64_t elems) {
+  if (!plan) return B2_ERR_ARG;
+  return b2_set_jk_chunk((B2PlanDev *)plan, elems);
+}
+
+int b2_eri_s8(void *plan, int precision, void *eri_out, void *stream) {
+  if (!plan || !eri_out) return B2_ERR_ARG;
+  int rc = b2_launch_eri_s8(*(B2PlanDev *)plan, precision, eri_out, (cudaStream_t)stream);
+  if (rc == B2_ERR_CUDA) b2_note(cudaGetLastError());
+  return rc;
+}
+
+int b2_jk_s8(void *plan, int precision, const void *eri, const double *D, double *J, double *K,
+             void *stream) {
+  if (!plan || !eri || !D || !J || !K) return B2_ERR_ARG;
+  return b2_launch_jk_s8(*(B2PlanDev *)plan, precision, eri, D, J, K, (cudaStream_t)stream);
+}
+
+int b2_grid_set(void *plan, const int64_t *grid_off) {
+  if (!plan || !grid_off) return B2_ERR_ARG;
+  return b2_grid_setup(*(B2PlanDev *)plan, (const long long *)grid_off);
+}
+
+int b2_grid_info(void *plan, int64_t *n_points, int64_t *n_ao) {
+  if (!plan) return B2_ERR_ARG;
+  B2PlanDev *P = (B2PlanDev *)plan;
+  if (n_points) *n_points = P->g.n_points;
+  if (n_ao) *n_ao = P->g.n_ao;
+  return B2_OK;
+}
+
+int b2_grid_ao_offsets(void *plan, int64_t *ao_off) {
+  if (!plan || !ao_off) return B2_ERR_ARG;
+  B2PlanDev *P = (B2PlanDev *)plan;
+  if (P->g.ao_off_h.empty()) return B2_ERR_ARG;
+  for (int m = 0; m < P->h.nmol; ++m) ao_off[m] = P->g.ao_off_h[m];
+  return B2_OK;
+}
+
+int b2_ao_eval(void *plan, int precision, const double *coords, void *ao, void *stream) {
+  if (!plan || !coords || !ao) return B2_ERR_ARG;
+  return b2_launch_ao_eval(*(B2PlanDev *)plan, precision, coords, ao, (cudaStream_t)stream);
+}
+
+int b2_xc(void *plan, int precision, const void *ao, const double *weights, const double *D,
+          double *Vxc, double *Exc, void *stream) {
+  if (!plan || !ao || !weights || !D || !Vxc || !Exc) return B2_ERR_ARG;
+  B2PlanDev *P = (B2PlanDev *)plan;
+  return b2_launch_xc(*P, precision, ao, weights, D, Vxc, Exc, P->g.rt, (cudaStream_t)stream);
+}
+
+__global__ void k_b3lyp_points(long long n, const double *__restrict__ rho, double *exc,
+                               double *vrho, double *vgamma) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  B2XcPoint<double> o = b2_b3lyp_point<double>(rho[g], rho[n + g], rho[2 * n + g], rho[3 * n + g]);
+  exc[g] = o.exc; vrho[g] = o.vrho; vgamma[g] = o.vgamma;
+}
+
+int b2_b3lyp(int64_t n, const double *rho, double *exc, double *vrho, double *vgamma, void *stream) {
+  if (n < 0 || (n > 0 && (!rho || !exc || !vrho || !vgamma))) return B2_ERR_ARG;
+  if (n == 0) return B2_OK;
+  k_b3lyp_points<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(n, rho, exc, vrho, vgamma);
+  B2_TRY(cudaGetLastError());
+  return B2_OK;
+}
+
+int b2_chol_inv(void *plan, const double *S, double *Linv, int *status, void *stream) {
+  if (!plan || !S || !Linv) return B2_ERR_ARG;
+  return b2_launch_chol_inv(*(B2PlanDev *)plan, S, Linv, status, (cudaStream_t)stream);
+}
+
+int b2_fock_diis(void *plan, const int *active, const int *iter, double hyb, int use_diis,
+                 const double *Hcore, const double *S, const double *D, const double *J,
+                 const double *K, const double *Vxc, double *H, double *diffJK, double *ring_err,
+                 double *ring_h, double *bmat, double *diis_err, void *stream) {
+  if (!plan || !Hcore || !S || !D || !J || !K || !Vxc || !H || !diffJK) return B2_ERR_ARG;
+  if (use_diis && (!iter || !ring_err || !ring_h || !bmat || !diis_err)) return B2_ERR_ARG;
+  return b2_launch_fock_diis(*(B2PlanDev *)plan, active, iter, hyb, use_diis, Hcore, S, D, J, K,
+                             Vxc, H, diffJK, ring_err, ring_h, bmat, diis_err, (cudaStream_t)stream);
+}
+
+int b2_eigh_density(void *plan, const int *active, const double *H, const double *Linv, double *D,
+                    double *mo_energy, double *C, int *sweeps, void *stream) {
+  if (!plan || !H || !Linv || !D || !mo_energy) return B2_ERR_ARG;
+  return b2_launch_eigh_density(*(B2PlanDev *)plan, active, H, Linv, D, mo_energy, C, sweeps,
+                                (cudaStream_t)stream);
+}
+
+int b2_energy(void *plan, const int *active, const double *D, const double *Hcore,
+              const double *diffJK, const double *Exc, const double *Enuc, double *out,
+              void *stream) {
+  if (!plan || !D || !Hcore || !diffJK || !Exc || !Enuc || !out) return B2_ERR_ARG;
+  return b2_launch_energy(*(B2PlanDev *)plan, active, D, Hcore, diffJK, Exc, Enuc, out,
+                          (cudaStream_t)stream);
+}
+
+int b2_int2e_sph_s8(const int *atm, int natm, const int *bas, int nbas, const double *env,
+                    int n_env, int precision, void *eri_out, void *stream) {
+  if (!atm || !bas || !env || !eri_out || natm <= 0 || nbas <= 0 || n_env <= 0) return B2_ERR_ARG;
+  int64_t eo = 0;
+  void *plan = nullptr;
+  int rc = b2_plan_create(1, &natm, &nbas, atm, bas, env, &eo, &plan);
+  if (rc) return rc;
+  rc = b2_eri_s8(plan, precision, eri_out, stream);
+  if (!rc) rc = b2_note(cudaStreamSynchronize((cudaStream_t)stream));
+  b2_plan_destroy(plan);
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,36 @@
+// Device copy of a batch plan (owned by the C-ABI plan handle).
+#pragma once
+#include "plan_host.hpp"
+#include "boys.cuh"
+
+struct B2GridDev {             // grid layout registered with b2_grid_set
+  long long n_points = 0, n_gblk = 0, n_vblk = 0, n_ao = 0;
+  long long *grid_off = nullptr, *gblk_off = nullptr, *vblk_off = nullptr, *ao_off = nullptr;
+  double *rt = nullptr;        // scratch: 4 x n_points
+  std::vector<long long> grid_off_h, ao_off_h;
+};
+
+struct B2PlanDev {
+  B2PlanHost h;
+  B2MolDev *mols = nullptr;
+  long long *row_off = nullptr;
+  B2Shell *shells = nullptr;
+  B2PairInfo *pinfo = nullptr;
+  B2PairPrim<double> *pp64 = nullptr;
+  B2PairPrim<float> *pp32 = nullptr;
+  int *ao2sh = nullptr;
+  int *cls_list = nullptr;
+  int *cls_cnt = nullptr;
+  double *atom_xyz = nullptr;
+  int *atom_z = nullptr;
+  double *boys = nullptr;
+  long long *jk_chunk_off = nullptr;      // nmol + 1 (J/K work split)
+  long long jk_chunk = 0;
+  long long jk_nchunks = 0;
+  int device = 0;
+  B2GridDev g;
+};
+
+int b2_launch_eri_s8(const B2PlanDev &P, int precision, void *out, cudaStream_t st);
+int b2_launch_jk_s8(const B2PlanDev &P, int precision, const void *eri, const double *D, double *J,
+                    double *K, cudaStream_t st);

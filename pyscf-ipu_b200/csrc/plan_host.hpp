@@ -1,0 +1,176 @@
+// Host-side batch plan: turns the libcint atm/bas/env arrays of a batch of molecules
+// (the inputs the reference packs for its ERI kernels, electron_repulsion/direct.py:710-739,
+// int2e_sph.cpp:6750) into the per-molecule tables the device kernels read.
+//
+// Per molecule:
+//   * shells (B2Shell): centre, exponents, coefficients (libcint coefficient times the
+//     angular factor 1/sqrt(4pi) or sqrt(3/(4pi))), l, first AO;
+//   * shell pairs I>=J, index sp = I(I+1)/2+J, each with up to 9 primitive pairs
+//     (zeta, P, K, P-A, P-B); K folds c_a c_b exp(-ab/zeta |AB|^2) sqrt(2) pi^{5/4}/zeta so that
+//     the primitive-quartet prefactor is K_bra K_ket / sqrt(zeta+eta);
+//   * shell pairs grouped by angular class (ss, ps, sp, pp), ascending, with for every
+//     bra shell pair IJ the number of class members KL <= IJ (so a row's ket work is a
+//     prefix of each class list);
+//   * offsets of the molecule's s8 ERI list (n2(n2+1)/2 entries, n2 = nao(nao+1)/2),
+//     of its AO-pair rows and of its nao x nao matrices.
+#pragma once
+#include <vector>
+#include <cmath>
+#include <cstring>
+#include <algorithm>
+#include "common.cuh"
+
+struct B2MolDev {
+  int nao, nbas, natm, nocc;
+  int sh_off, sp_off, ao_off, nsp;
+  int cls_start[5];
+  int atm_off, pad0, pad1;
+  long long eri_off, row_off, mat_off, n4;
+};
+
+struct B2PlanHost {
+  int nmol = 0;
+  int max_nao = 0;
+  long long n_eri = 0, n_rows = 0, n_mat = 0;
+  int n_sh = 0, n_sp = 0, n_ao = 0, n_atm = 0;
+  std::vector<B2MolDev> mols;
+  std::vector<long long> row_off;         // nmol + 1
+  std::vector<B2Shell> shells;
+  std::vector<B2PairInfo> pinfo;
+  std::vector<B2PairPrim<double>> pp64;
+  std::vector<B2PairPrim<float>> pp32;
+  std::vector<int> ao2sh;                 // per AO: local shell index
+  std::vector<int> cls_list;              // per molecule nsp entries (offset sp_off)
+  std::vector<int> cls_cnt;               // per molecule 4*nsp (offset 4*sp_off)
+  std::vector<double> atom_xyz;           // per atom (offset atm_off): x,y,z
+  std::vector<int> atom_z;
+};
+
+static inline int b2_class(int lK, int lL) { return lK + 2 * lL; }   // ss=0, ps=1, sp=2, pp=3
+
+// returns B2_OK or an error code
+static int b2_plan_build(B2PlanHost &P, int nmol, const int *natm, const int *nbas, const int *atm,
+                         const int *bas, const double *env, const long long *env_off) {
+  P = B2PlanHost();
+  P.nmol = nmol;
+  P.mols.resize(nmol);
+  P.row_off.assign(nmol + 1, 0);
+  const double k0 = std::sqrt(2.0) * std::pow(M_PI, 1.25);
+  int atm_row = 0, bas_row = 0;
+  for (int m = 0; m < nmol; ++m) {
+    const int *A = atm + (size_t)atm_row * B2_ATM_SLOTS;
+    const int *Bs = bas + (size_t)bas_row * B2_BAS_SLOTS;
+    const double *E = env + env_off[m];
+    B2MolDev md;
+    std::memset(&md, 0, sizeof(md));
+    md.natm = natm[m];
+    md.nbas = nbas[m];
+    md.sh_off = P.n_sh;
+    md.sp_off = P.n_sp;
+    md.ao_off = P.n_ao;
+    md.atm_off = P.n_atm;
+    int nao = 0, nel = 0;
+    for (int a = 0; a < natm[m]; ++a) {
+      nel += A[a * B2_ATM_SLOTS + 0];
+      const double *R = E + A[a * B2_ATM_SLOTS + B2_PTR_COORD];
+      P.atom_xyz.push_back(R[0]); P.atom_xyz.push_back(R[1]); P.atom_xyz.push_back(R[2]);
+      P.atom_z.push_back(A[a * B2_ATM_SLOTS + 0]);
+    }
+    for (int s = 0; s < nbas[m]; ++s) {
+      const int *b = Bs + s * B2_BAS_SLOTS;
+      int l = b[B2_ANG_OF], np = b[B2_NPRIM_OF];
+      if (l > B2_MAXL || np > B2_MAXPRIM || np < 1 || b[B2_NCTR_OF] != 1) return B2_ERR_UNSUPPORTED;
+      if (b[B2_ATOM_OF] < 0 || b[B2_ATOM_OF] >= natm[m]) return B2_ERR_ARG;
+      B2Shell sh;
+      std::memset(&sh, 0, sizeof(sh));
+      const double *R = E + A[b[B2_ATOM_OF] * B2_ATM_SLOTS + B2_PTR_COORD];
+      for (int d = 0; d < 3; ++d) sh.R[d] = R[d];
+      double fac = l == 0 ? B2_FAC_S : B2_FAC_P;
+      for (int k = 0; k < np; ++k) {
+        sh.exp[k] = E[b[B2_PTR_EXP] + k];
+        sh.coef[k] = E[b[B2_PTR_COEFF] + k] * fac;
+      }
+      sh.l = l; sh.ao0 = nao; sh.nprim = np; sh.atom = b[B2_ATOM_OF];
+      for (int c = 0; c < 2 * l + 1; ++c) P.ao2sh.push_back(s);
+      nao += 2 * l + 1;
+      P.shells.push_back(sh);
+    }
+    if (nao > B2_MAXNAO - 2) return B2_ERR_SIZE;
+    md.nao = nao;
+    md.nocc = nel / 2;
+    int nsp = nbas[m] * (nbas[m] + 1) / 2;
+    md.nsp = nsp;
+    long long n2 = (long long)nao * (nao + 1) / 2;
+    md.n4 = n2 * (n2 + 1) / 2;
+    md.eri_off = P.n_eri;
+    md.row_off = P.n_rows;
+    md.mat_off = P.n_mat;
+    // shell pairs
+    const B2Shell *S = &P.shells[md.sh_off];
+    std::vector<int> cls(nsp);
+    for (int I = 0; I < nbas[m]; ++I)
+      for (int J = 0; J <= I; ++J) {
+        const B2Shell &a = S[I], &b = S[J];
+        B2PairInfo pi;
+        pi.I = I; pi.J = J; pi.lI = a.l; pi.lJ = b.l; pi.ao0I = a.ao0; pi.ao0J = b.ao0;
+        pi.nprim = a.nprim * b.nprim; pi.pad = 0;
+        P.pinfo.push_back(pi);
+        cls[(int)b2_tri(I) + J] = b2_class(a.l, b.l);
+        double AB2 = 0;
+        for (int d = 0; d < 3; ++d) AB2 += (a.R[d] - b.R[d]) * (a.R[d] - b.R[d]);
+        for (int x = 0; x < B2_MAXPP; ++x) {
+          B2PairPrim<double> q;
+          std::memset(&q, 0, sizeof(q));
+          int pa = x / B2_MAXPRIM, pb = x % B2_MAXPRIM;
+          if (pa < a.nprim && pb < b.nprim) {
+            double al = a.exp[pa], be = b.exp[pb], z = al + be;
+            double Pc[3];
+            for (int d = 0; d < 3; ++d) Pc[d] = (al * a.R[d] + be * b.R[d]) / z;
+            double K = a.coef[pa] * b.coef[pb] * std::exp(-al * be / z * AB2) * k0 / z;
+            if (std::fabs(K) < 1e-300) K = 0;
+            q.zeta = z; q.Px = Pc[0]; q.Py = Pc[1]; q.Pz = Pc[2]; q.K = K;
+            q.PAx = Pc[0] - a.R[0]; q.PAy = Pc[1] - a.R[1]; q.PAz = Pc[2] - a.R[2];
+            q.PBx = Pc[0] - b.R[0]; q.PBy = Pc[1] - b.R[1]; q.PBz = Pc[2] - b.R[2];
+          } else {
+            q.zeta = 1.0;    // inert padding (K = 0)
+          }
+          P.pp64.push_back(q);
+          B2PairPrim<float> f;
+          f.zeta = (float)q.zeta; f.Px = (float)q.Px; f.Py = (float)q.Py; f.Pz = (float)q.Pz;
+          f.K = (float)q.K; f.PAx = (float)q.PAx; f.PAy = (float)q.PAy; f.PAz = (float)q.PAz;
+          f.PBx = (float)q.PBx; f.PBy = (float)q.PBy; f.PBz = (float)q.PBz; f.pad = 0.f;
+          P.pp32.push_back(f);
+        }
+      }
+    // class lists and prefix counts
+    int start = 0;
+    for (int c = 0; c < 4; ++c) {
+      md.cls_start[c] = start;
+      for (int sp = 0; sp < nsp; ++sp)
+        if (cls[sp] == c) { P.cls_list.push_back(sp); ++start; }
+    }
+    md.cls_start[4] = start;
+    size_t base = P.cls_cnt.size();
+    P.cls_cnt.resize(base + 4 * (size_t)nsp);
+    for (int c = 0; c < 4; ++c) {
+      int cnt = 0;
+      for (int sp = 0; sp < nsp; ++sp) {
+        if (cls[sp] == c) ++cnt;
+        P.cls_cnt[base + (size_t)c * nsp + sp] = cnt;
+      }
+    }
+    P.mols[m] = md;
+    P.n_sh += nbas[m];
+    P.n_sp += nsp;
+    P.n_ao += nao;
+    P.n_atm += natm[m];
+    P.n_eri += md.n4;
+    P.n_rows += n2;
+    P.n_mat += (long long)nao * nao;
+    P.row_off[m + 1] = P.n_rows;
+    P.max_nao = std::max(P.max_nao, nao);
+    atm_row += natm[m];
+    bas_row += nbas[m];
+  }
+  return B2_OK;
+}

@@ -1,0 +1,420 @@
+// Device-resident SCF step (sm_100a), FP64, one CTA per molecule.
+//
+// Follows the reference iteration (nanoDFT.py:40-102, dft.py:789-882):
+//   H = H_core + (J - hyb/2 K) + V_xc
+//   DIIS (nanoDFT.py:338-364): err = S D H - (S D H)^T stored in a ring of 9, B-matrix
+//     row/column head+1 <- <err_k, err>, masked until filled, c = pinv(B)[0,:]
+//     (pinv as jnp.linalg.pinv: singular values below 10*max(m,n)*eps*s_max dropped),
+//     H <- sum_k c[k+1] H_k
+//   C = L^T eigvec(L H L^T) with L = inv(cholesky(S)) (nanoDFT.py:69, 239)
+//   D = 2 C_occ C_occ^T (nanoDFT.py:72)
+// The eigensolver is a parallel cyclic Jacobi method (round-robin pair ordering) on the
+// matrix held in shared memory; the reference uses jnp.linalg.eigh or TessellateIPU's
+// Jacobi ipu_eigh (nanoDFT.py:370-393).
+#include "device_plan.cuh"
+#include "scf.cuh"
+
+__device__ double b2_block_sum(double v, double *red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[w] = v;
+  __syncthreads();
+  double s = 0;
+  for (int i = 0; i < nw; ++i) s += red[i];
+  __syncthreads();
+  return s;
+}
+
+__device__ double b2_block_max(double v, double *red) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[w] = v;
+  __syncthreads();
+  double s = 0;
+  for (int i = 0; i < nw; ++i) s = fmax(s, red[i]);
+  __syncthreads();
+  return s;
+}
+
+// C[N][N] = A * B (or A * B^T), all row-major in shared memory, ld = N
+__device__ void b2_mm(const double *A, const double *B, double *C, int N, bool transB) {
+  for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
+    const int r = e / N, c = e - (e / N) * N;
+    double s = 0;
+    if (transB)
+      for (int k = 0; k < N; ++k) s += A[r * N + k] * B[c * N + k];
+    else
+      for (int k = 0; k < N; ++k) s += A[r * N + k] * B[k * N + c];
+    C[e] = s;
+  }
+}
+
+// rotation (c, s) zeroing A_pq (Golub & Van Loan, sym.schur2)
+__device__ __host__ inline void b2_schur2(double app, double aqq, double apq, double &c, double &s) {
+  if (apq == 0.0) { c = 1.0; s = 0.0; return; }
+  const double tau = (aqq - app) / (2.0 * apq);
+  double t;
+  if (fabs(tau) > 1e150) t = 0.5 / tau;
+  else t = (tau >= 0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+  c = 1.0 / sqrt(1.0 + t * t);
+  s = t * c;
+}
+
+// parallel cyclic Jacobi on A (n x n, n even, ld = n) in shared memory; V <- eigenvectors
+__device__ int b2_jacobi(double *A, double *V, int n, double *rot, int *prs, double *red,
+                         int max_sweeps) {
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) V[e] = (e / n == e % n) ? 1.0 : 0.0;
+  __syncthreads();
+  const int half = n / 2;
+  int sweep = 0;
+  for (; sweep < max_sweeps; ++sweep) {
+    double off = 0, tot = 0;
+    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+      const double a = A[e];
+      tot += a * a;
+      if (e / n != e % n) off += a * a;
+    }
+    off = b2_block_sum(off, red);
+    tot = b2_block_sum(tot, red);
+    if (off <= 1e-30 * tot || off < 1e-300) break;
+    for (int r = 0; r < n - 1; ++r) {
+      if (threadIdx.x < half) {
+        const int k = threadIdx.x;
+        const int a = (k == 0) ? 0 : ((k - 1 + r) % (n - 1)) + 1;
+        const int kb = n - 1 - k;
+        const int b = ((kb - 1 + r) % (n - 1)) + 1;
+        const int p = min(a, b), q = max(a, b);
+        double c, s;
+        b2_schur2(A[p * n + p], A[q * n + q], A[p * n + q], c, s);
+        prs[2 * k] = p; prs[2 * k + 1] = q;
+        rot[2 * k] = c; rot[2 * k + 1] = s;
+      }
+      __syncthreads();
+      for (int e = threadIdx.x; e < half * n; e += blockDim.x) {      // rows: A <- J^T A
+        const int k = e / n, col = e - (e / n) * n;
+        const int p = prs[2 * k], q = prs[2 * k + 1];
+        const double c = rot[2 * k], s = rot[2 * k + 1];
+        const double apk = A[p * n + col], aqk = A[q * n + col];
+        A[p * n + col] = c * apk - s * aqk;
+        A[q * n + col] = s * apk + c * aqk;
+      }
+      __syncthreads();
+      for (int e = threadIdx.x; e < half * n; e += blockDim.x) {      // cols: A <- A J, V <- V J
+        const int k = e / n, row = e - (e / n) * n;
+        const int p = prs[2 * k], q = prs[2 * k + 1];
+        const double c = rot[2 * k], s = rot[2 * k + 1];
+        const double akp = A[row * n + p], akq = A[row * n + q];
+        A[row * n + p] = c * akp - s * akq;
+        A[row * n + q] = s * akp + c * akq;
+        const double vkp = V[row * n + p], vkq = V[row * n + q];
+        V[row * n + p] = c * vkp - s * vkq;
+        V[row * n + q] = s * vkp + c * vkq;
+      }
+      __syncthreads();
+    }
+  }
+  return sweep;
+}
+
+// serial Jacobi for the small DIIS matrix (n <= 10), thread-local
+__device__ void b2_jacobi_small(double *A, double *V, int n) {
+  for (int i = 0; i < n * n; ++i) V[i] = (i / n == i % n) ? 1.0 : 0.0;
+  for (int sweep = 0; sweep < 50; ++sweep) {
+    double off = 0, tot = 0;
+    for (int i = 0; i < n * n; ++i) { tot += A[i] * A[i]; if (i / n != i % n) off += A[i] * A[i]; }
+    if (off <= 1e-32 * tot || off < 1e-300) break;
+    for (int p = 0; p < n - 1; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        double c, s;
+        b2_schur2(A[p * n + p], A[q * n + q], A[p * n + q], c, s);
+        if (s == 0.0) continue;
+        for (int k = 0; k < n; ++k) {
+          const double apk = A[p * n + k], aqk = A[q * n + k];
+          A[p * n + k] = c * apk - s * aqk;
+          A[q * n + k] = s * apk + c * aqk;
+        }
+        for (int k = 0; k < n; ++k) {
+          const double akp = A[k * n + p], akq = A[k * n + q];
+          A[k * n + p] = c * akp - s * akq;
+          A[k * n + q] = s * akp + c * akq;
+          const double vkp = V[k * n + p], vkq = V[k * n + q];
+          V[k * n + p] = c * vkp - s * vkq;
+          V[k * n + q] = s * vkp + c * vkq;
+        }
+      }
+  }
+}
+
+// ------------------------------------------------------------------ Fock + DIIS
+// ring layout per molecule (offset mat_off * 9): errs[9][N*N], hams[9][N*N]; B: 100 doubles
+__global__ void __launch_bounds__(256)
+k_fock_diis(const B2MolDev *__restrict__ mols, const int *__restrict__ active,
+            const int *__restrict__ iter, double hyb, int use_diis, const double *__restrict__ Hcore,
+            const double *__restrict__ S, const double *__restrict__ D, const double *__restrict__ J,
+            const double *__restrict__ K, const double *__restrict__ Vxc, double *__restrict__ H,
+            double *__restrict__ diffJK, double *__restrict__ ring_err, double *__restrict__ ring_h,
+            double *__restrict__ Bmat, double *__restrict__ diis_err) {
+  const int m = blockIdx.x;
+  if (active && !active[m]) return;
+  extern __shared__ double sm[];
+  __shared__ double red[32];
+  __shared__ double sc[10];
+  __shared__ double stmp[9];
+  const B2MolDev md = mols[m];
+  const int N = md.nao, NN = N * N;
+  const long long mo = md.mat_off;
+  double *sH = sm, *sS = sH + NN, *sD = sS + NN, *sT = sD + NN;
+  for (int e = threadIdx.x; e < NN; e += blockDim.x) {
+    const double djk = J[mo + e] - 0.5 * hyb * K[mo + e];
+    diffJK[mo + e] = djk;
+    sH[e] = Hcore[mo + e] + djk + Vxc[mo + e];
+    sS[e] = S[mo + e];
+    sD[e] = D[mo + e];
+  }
+  __syncthreads();
+  if (!use_diis) {
+    for (int e = threadIdx.x; e < NN; e += blockDim.x) H[mo + e] = sH[e];
+    return;
+  }
+  const int it = iter[m];
+  const int nd = 9, head = it % nd;
+  b2_mm(sS, sD, sT, N, false);          // S D
+  __syncthreads();
+  b2_mm(sT, sH, sS, N, false);          // S D H  (into sS)
+  __syncthreads();
+  double *er = ring_err + mo * nd, *hr = ring_h + mo * nd;
+  double emax = 0;
+  for (int e = threadIdx.x; e < NN; e += blockDim.x) {
+    const int a = e / N, b = e - (e / N) * N;
+    const double v = sS[a * N + b] - sS[b * N + a];
+    sT[e] = v;
+    emax = fmax(emax, fabs(v));
+    er[(long long)head * NN + e] = v;
+    hr[(long long)head * NN + e] = sH[e];
+  }
+  emax = b2_block_max(emax, red);
+  __syncthreads();
+  const int nfill = min(it + 1, nd);
+  for (int k = 0; k < nd; ++k) {
+    double s = 0;
+    if (k < nfill)
+      for (int e = threadIdx.x; e < NN; e += blockDim.x) s += er[(long long)k * NN + e] * sT[e];
+    s = b2_block_sum(s, red);
+    if (threadIdx.x == 0) stmp[k] = (k < nfill) ? s : 0.0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double *B = Bmat + (long long)m * 100;
+    if (it == 0) {
+      for (int i = 0; i < 100; ++i) B[i] = 0;
+      for (int i = 1; i < 10; ++i) { B[i] = 1; B[i * 10] = 1; }
+    }
+    for (int k = 0; k < nd; ++k) { B[(head + 1) * 10 + 1 + k] = stmp[k]; B[(1 + k) * 10 + head + 1] = stmp[k]; }
+    double A[100], V[100];
+    double mask[10];
+    mask[0] = 1;
+    for (int k = 0; k < nd; ++k) mask[k + 1] = (k < nfill) ? 1.0 : 0.0;
+    for (int i = 0; i < 10; ++i)
+      for (int j = 0; j < 10; ++j) A[i * 10 + j] = B[i * 10 + j] * mask[i] * mask[j];
+    b2_jacobi_small(A, V, 10);
+    double smax = 0;
+    for (int i = 0; i < 10; ++i) smax = fmax(smax, fabs(A[i * 10 + i]));
+    const double cut = 10.0 * 10.0 * 2.220446049250313e-16 * smax;
+    for (int j = 0; j < 10; ++j) {
+      double c = 0;
+      for (int k = 0; k < 10; ++k) {
+        const double lam = A[k * 10 + k];
+        if (fabs(lam) > cut) c += V[0 * 10 + k] * V[j * 10 + k] / lam;
+      }
+      sc[j] = c;
+    }
+    diis_err[m] = emax;
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < NN; e += blockDim.x) {
+    double s = 0;
+    for (int k = 0; k < nfill; ++k) s += sc[k + 1] * hr[(long long)k * NN + e];
+    H[mo + e] = s;
+  }
+}
+
+// ------------------------------------------------------------------ eigensolve + density
+__global__ void __launch_bounds__(256)
+k_eigh_density(const B2MolDev *__restrict__ mols, const int *__restrict__ active,
+               const double *__restrict__ H, const double *__restrict__ Linv,
+               double *__restrict__ D, double *__restrict__ mo_energy, double *__restrict__ C,
+               int *__restrict__ sweeps) {
+  const int m = blockIdx.x;
+  if (active && !active[m]) return;
+  extern __shared__ double sm[];
+  __shared__ double red[32];
+  __shared__ double rot[B2_MAXNAO];
+  __shared__ int prs[B2_MAXNAO];
+  __shared__ int order[B2_MAXNAO];
+  const B2MolDev md = mols[m];
+  const int N = md.nao, NN = N * N;
+  const int n = (N + 1) & ~1;                     // even size for the round-robin ordering
+  const long long mo = md.mat_off;
+  double *sL = sm, *sT = sL + NN, *sA = sT + NN, *sV = sA + n * n;
+  for (int e = threadIdx.x; e < NN; e += blockDim.x) { sL[e] = Linv[mo + e]; sA[e] = H[mo + e]; }
+  __syncthreads();
+  b2_mm(sL, sA, sT, N, false);                    // L H
+  __syncthreads();
+  // A = (L H) L^T written with leading dimension n
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int r = e / n, c = e - (e / n) * n;
+    double s = 0;
+    if (r < N && c < N)
+      for (int k = 0; k < N; ++k) s += sT[r * N + k] * sL[c * N + k];
+    else if (r == c)
+      s = 1e30;                                    // padding: decoupled, sorts last
+    sA[e] = s;
+  }
+  __syncthreads();
+  const int sw = b2_jacobi(sA, sV, n, rot, prs, red, 30);
+  // ascending order of eigenvalues
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const double li = sA[i * n + i];
+    int rank = 0;
+    for (int j = 0; j < n; ++j) {
+      const double lj = sA[j * n + j];
+      rank += (lj < li) || (lj == li && j < i);
+    }
+    order[rank] = i;
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < N; k += blockDim.x) mo_energy[(long long)m * B2_MAXNAO + k] = sA[order[k] * n + order[k]];
+  // C[:, k] = L^T V[:, order[k]]  (all N columns, into sT)
+  for (int e = threadIdx.x; e < NN; e += blockDim.x) {
+    const int r = e / N, k = e - (e / N) * N;
+    const int col = order[k];
+    double s = 0;
+    for (int a = 0; a < N; ++a) s += sL[a * N + r] * sV[a * n + col];
+    sT[e] = s;
+  }
+  __syncthreads();
+  const int nocc = md.nocc;
+  for (int e = threadIdx.x; e < NN; e += blockDim.x) {
+    const int a = e / N, b = e - (e / N) * N;
+    double s = 0;
+    for (int k = 0; k < nocc; ++k) s += sT[a * N + k] * sT[b * N + k];
+    D[mo + e] = 2.0 * s;
+    if (C) C[mo + e] = sT[e];
+  }
+  if (threadIdx.x == 0 && sweeps) sweeps[m] = sw;
+}
+
+// energies [E, E_core, E_J_K/2, E_xc, E_nuc] (nanoDFT.py:20-38)
+__global__ void k_energy(const B2MolDev *__restrict__ mols, const int *__restrict__ active,
+                         const double *__restrict__ D, const double *__restrict__ Hcore,
+                         const double *__restrict__ diffJK, const double *__restrict__ exc,
+                         const double *__restrict__ enuc, double *__restrict__ out) {
+  const int m = blockIdx.x;
+  if (active && !active[m]) return;
+  __shared__ double red[32];
+  const B2MolDev md = mols[m];
+  const int NN = md.nao * md.nao;
+  double ec = 0, ej = 0;
+  for (int e = threadIdx.x; e < NN; e += blockDim.x) {
+    const double d = D[md.mat_off + e];
+    ec += d * Hcore[md.mat_off + e];
+    ej += d * diffJK[md.mat_off + e];
+  }
+  ec = b2_block_sum(ec, red);
+  ej = b2_block_sum(ej, red);
+  if (threadIdx.x == 0) {
+    double *o = out + (long long)m * 5;
+    o[0] = ec + 0.5 * ej + exc[m] + enuc[m];
+    o[1] = ec;
+    o[2] = 0.5 * ej;
+    o[3] = exc[m];
+    o[4] = enuc[m];
+  }
+}
+
+// L = inv(cholesky(S)) per molecule (FP64), one CTA per molecule (serial-ish, small N)
+__global__ void k_chol_inv(const B2MolDev *__restrict__ mols, const double *__restrict__ S,
+                           double *__restrict__ Linv, int *__restrict__ status) {
+  const int m = blockIdx.x;
+  extern __shared__ double sm[];
+  const B2MolDev md = mols[m];
+  const int N = md.nao, NN = N * N;
+  double *sC = sm, *sI = sm + NN;
+  for (int e = threadIdx.x; e < NN; e += blockDim.x) sC[e] = S[md.mat_off + e];
+  __shared__ int bad;
+  if (threadIdx.x == 0) bad = 0;
+  __syncthreads();
+  // right-looking Cholesky: lower triangle of sC
+  for (int k = 0; k < N; ++k) {
+    if (threadIdx.x == 0) {
+      const double d = sC[k * N + k];
+      if (!(d > 0)) bad = 1;
+      sC[k * N + k] = sqrt(fmax(d, 1e-300));
+    }
+    __syncthreads();
+    const double dk = sC[k * N + k];
+    for (int i = k + 1 + threadIdx.x; i < N; i += blockDim.x) sC[i * N + k] /= dk;
+    __syncthreads();
+    for (int e = threadIdx.x; e < (N - k - 1) * (N - k - 1); e += blockDim.x) {
+      const int i = k + 1 + e / (N - k - 1), j = k + 1 + e % (N - k - 1);
+      if (j <= i) sC[i * N + j] -= sC[i * N + k] * sC[j * N + k];
+    }
+    __syncthreads();
+  }
+  // inverse of the lower-triangular factor, column by column (forward substitution)
+  for (int c = threadIdx.x; c < N; c += blockDim.x) {
+    for (int i = 0; i < N; ++i) {
+      double s = (i == c) ? 1.0 : 0.0;
+      for (int k = c; k < i; ++k) s -= sC[i * N + k] * sI[k * N + c];
+      sI[i * N + c] = (i < c) ? 0.0 : s / sC[i * N + i];
+    }
+  }
+  __syncthreads();
+  for (int e = threadIdx.x; e < NN; e += blockDim.x) Linv[md.mat_off + e] = sI[e];
+  if (threadIdx.x == 0 && status) status[m] = bad ? B2_ERR_NOT_PD : B2_OK;
+}
+
+static size_t b2_fock_smem(int N) { return sizeof(double) * 4 * N * N; }
+static size_t b2_eigh_smem(int N) { int n = (N + 1) & ~1; return sizeof(double) * (2 * N * N + 2 * n * n); }
+
+int b2_launch_fock_diis(const B2PlanDev &P, const int *active, const int *iter, double hyb,
+                        int use_diis, const double *Hcore, const double *S, const double *D,
+                        const double *J, const double *K, const double *Vxc, double *H,
+                        double *diffJK, double *ring_err, double *ring_h, double *Bmat,
+                        double *diis_err, cudaStream_t st) {
+  size_t sm = b2_fock_smem(P.h.max_nao);
+  B2_CUDA_TRY(cudaFuncSetAttribute(k_fock_diis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  k_fock_diis<<<P.h.nmol, 256, sm, st>>>(P.mols, active, iter, hyb, use_diis, Hcore, S, D, J, K,
+                                          Vxc, H, diffJK, ring_err, ring_h, Bmat, diis_err);
+  B2_CUDA_TRY(cudaGetLastError());
+  return B2_OK;
+}
+
+int b2_launch_eigh_density(const B2PlanDev &P, const int *active, const double *H,
+                           const double *Linv, double *D, double *mo_energy, double *C,
+                           int *sweeps, cudaStream_t st) {
+  size_t sm = b2_eigh_smem(P.h.max_nao);
+  B2_CUDA_TRY(cudaFuncSetAttribute(k_eigh_density, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  k_eigh_density<<<P.h.nmol, 256, sm, st>>>(P.mols, active, H, Linv, D, mo_energy, C, sweeps);
+  B2_CUDA_TRY(cudaGetLastError());
+  return B2_OK;
+}
+
+int b2_launch_energy(const B2PlanDev &P, const int *active, const double *D, const double *Hcore,
+                     const double *diffJK, const double *exc, const double *enuc, double *out,
+                     cudaStream_t st) {
+  k_energy<<<P.h.nmol, 256, 0, st>>>(P.mols, active, D, Hcore, diffJK, exc, enuc, out);
+  B2_CUDA_TRY(cudaGetLastError());
+  return B2_OK;
+}
+
+int b2_launch_chol_inv(const B2PlanDev &P, const double *S, double *Linv, int *status,
+                       cudaStream_t st) {
+  size_t sm = sizeof(double) * 2 * P.h.max_nao * P.h.max_nao;
+  B2_CUDA_TRY(cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  k_chol_inv<<<P.h.nmol, 128, sm, st>>>(P.mols, S, Linv, status);
+  B2_CUDA_TRY(cudaGetLastError());
+  return B2_OK;
+}

@@ -1,0 +1,147 @@
+"""GPU parity: every kernel through the C ABI against the oracle / reference golden data."""
+import ctypes
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden
+from oracle import eri as oeri, rks
+from b200dft.mole import Mole, methane
+from b200dft.molgen import config2_molecule, random_molecule
+from b200dft.engine import RKSEngine, HostSetup, Plan
+from b200dft._lib import lib, check, ptr, stream_handle
+
+pytestmark = pytest.mark.gpu
+
+NAMES = ("h2", "ch4", "water", "tree3")
+
+
+def _mols():
+    gs = [golden(f"eri_ref_{n}.npz") for n in NAMES]
+    return [Mole(str(g["atom"]), unit=str(g["unit"])) for g in gs], gs
+
+
+def _eri(mols, prec, cuda):
+    P = Plan(mols)
+    out = torch.full((P.n_eri,), float("nan"), dtype=torch.float64 if prec == 64 else torch.float32,
+                     device=cuda)
+    check(lib().b2_eri_s8(P.h, prec, ptr(out), stream_handle()), "eri")
+    torch.cuda.synchronize()
+    return P, out.double().cpu().numpy()
+
+
+def test_eri_s8_fp64_vs_reference(cuda):
+    mols, gs = _mols()
+    P, v = _eri(mols, 64, cuda)
+    assert not np.isnan(v).any()
+    ref = np.concatenate([g["s8"] for g in gs])
+    err = np.abs(v - ref).max()
+    assert err <= 1e-10, err                       # north-star gate: 1e-10 abs
+
+
+def test_eri_s8_fp32(cuda):
+    mols, gs = _mols()
+    P, v = _eri(mols, 32, cuda)
+    ref = np.concatenate([g["s8"] for g in gs])
+    assert np.abs(v - ref).max() < 5e-6
+
+
+def test_eri_config2_full(cuda):
+    g = golden("eri_ref_sample_config2.npz")
+    m = Mole(str(g["atom"]))
+    P, v = _eri([m], 64, cuda)
+    assert len(v) == int(g["n"])
+    np.testing.assert_allclose(v[g["idx"]], g["val"], atol=1e-10, rtol=0)
+    assert abs(v.sum() - float(g["total"])) <= 1e-9 * abs(float(g["total"]))
+    assert abs((v * v).sum() - float(g["sumsq"])) <= 1e-9 * float(g["sumsq"])
+    ref = oeri.eri_s8(m)
+    assert np.abs(v - ref).max() <= 1e-10
+
+
+def test_int2e_sph_s8_single(cuda):
+    m = Mole(methane())
+    out = torch.zeros(oeri.n_s8(m.nao), dtype=torch.float64, device=cuda)
+    atm = np.ascontiguousarray(m._atm, np.int32)
+    bas = np.ascontiguousarray(m._bas, np.int32)
+    env = np.ascontiguousarray(m._env)
+    check(lib().b2_int2e_sph_s8(ptr(atm), m.natm, ptr(bas), m.nbas, ptr(env), len(env), 64, ptr(out),
+                                stream_handle()), "int2e")
+    np.testing.assert_allclose(out.cpu().numpy(), golden("eri_ref_ch4.npz")["s8"], atol=1e-10)
+
+
+def _sym_random(n, rng):
+    a = rng.normal(size=(n, n))
+    return (a + a.T) / 2
+
+
+@pytest.mark.parametrize("prec", [64, 32])
+def test_jk_parity(cuda, prec):
+    mols, gs = _mols()
+    P, v = _eri(mols, prec, cuda)
+    rng = np.random.default_rng(0)
+    Ds = [_sym_random(m.nao, rng) for m in mols]
+    eri_t = torch.from_numpy(v).to(cuda).to(torch.float64 if prec == 64 else torch.float32)
+    D = torch.from_numpy(P.pack(Ds)).to(cuda)
+    J = torch.zeros(P.n_mat, dtype=torch.float64, device=cuda)
+    K = torch.zeros_like(J)
+    for chunk in (0, 64, 1000):               # several work splits give the same answer
+        if chunk:
+            P.set_jk_chunk(chunk)
+        check(lib().b2_jk_s8(P.h, prec, ptr(eri_t), ptr(D), ptr(J), ptr(K), stream_handle()), "jk")
+        torch.cuda.synchronize()
+        Jh, Kh = J.cpu().numpy(), K.cpu().numpy()
+        for mi, (m, g) in enumerate(zip(mols, gs)):
+            _, Jr, Kr = rks.jk_from_s8(Ds[mi], g["s8"], m.nao)
+            tol = 1e-10 if prec == 64 else 2e-5 * max(1.0, np.abs(Jr).max())
+            np.testing.assert_allclose(P.unpack(Jh, mi), Jr, atol=tol)
+            np.testing.assert_allclose(P.unpack(Kh, mi), Kr, atol=tol)
+
+
+def test_ao_eval_and_xc(cuda):
+    mols = [Mole(methane()), Mole("O 0 0 0.1173; H 0 0.7572 -0.4692; H 0 -0.7572 -0.4692")]
+    eng = RKSEngine(mols, level=0, precision="fp64")
+    eng.compute_ao()
+    torch.cuda.synchronize()
+    ao = eng.ao.cpu().numpy()
+    for mi, (m, s) in enumerate(zip(mols, eng.setups)):
+        G, N = len(s.weights), m.nao
+        a = ao[eng.plan.ao_off[mi]:eng.plan.ao_off[mi] + 4 * G * N].reshape(4, G, N)
+        np.testing.assert_allclose(a, rks.ao_values(m, s.coords), atol=1e-12)
+    eng.D.copy_(eng.D0)
+    eng.xc()
+    torch.cuda.synchronize()
+    for mi, (m, s) in enumerate(zip(mols, eng.setups)):
+        exc, V, _ = rks.exchange_correlation(s.D0, rks.ao_values(m, s.coords), s.weights)
+        assert abs(eng.exc[mi].item() - exc) < 1e-10
+        np.testing.assert_allclose(eng.plan.unpack(eng.Vxc.cpu().numpy(), mi), V, atol=1e-10)
+    eng.close()
+
+
+def test_b3lyp_entry(cuda):
+    rng = np.random.default_rng(0)
+    n = 10000
+    rho = np.zeros((4, n))
+    rho[0] = 10 ** rng.uniform(-12, 3, n)
+    rho[1:] = rng.normal(size=(3, n)) * rho[0] ** (4 / 3)
+    r = torch.from_numpy(rho).to(cuda)
+    e, vr, vg = (torch.zeros(n, dtype=torch.float64, device=cuda) for _ in range(3))
+    check(lib().b2_b3lyp(n, ptr(r), ptr(e), ptr(vr), ptr(vg), stream_handle()), "b3lyp")
+    torch.cuda.synchronize()
+    e0, vr0, vg0 = rks.b3lyp(rho)
+    np.testing.assert_allclose(e.cpu().numpy(), e0, rtol=1e-12)
+    np.testing.assert_allclose(vr.cpu().numpy(), vr0, rtol=1e-12)
+    np.testing.assert_allclose(vg.cpu().numpy(), vg0, rtol=1e-10)
+
+
+def test_chol_inv(cuda):
+    mols, _ = _mols()
+    eng_setups = [HostSetup(m, 0) for m in mols]
+    P = Plan(mols)
+    S = torch.from_numpy(P.pack([s.S for s in eng_setups])).to(cuda)
+    L = torch.zeros_like(S)
+    st = torch.zeros(len(mols), dtype=torch.int32, device=cuda)
+    check(lib().b2_chol_inv(P.h, ptr(S), ptr(L), ptr(st), stream_handle()), "chol")
+    torch.cuda.synchronize()
+    assert (st.cpu().numpy() == 0).all()
+    for mi, s in enumerate(eng_setups):
+        np.testing.assert_allclose(P.unpack(L.cpu().numpy(), mi), s.L_inv, atol=1e-10)

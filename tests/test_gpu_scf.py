@@ -1,0 +1,81 @@
+"""GPU parity of the SCF loop and the drop-in entry points against the FP64 oracle."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden
+from oracle import eri as oeri, rks
+from b200dft.mole import Mole, methane
+from b200dft.molgen import random_molecule
+from b200dft.engine import RKSEngine, HostSetup
+from b200dft.int1e import int1e
+from b200dft.guess import minao
+from b200dft import nanodft, dft
+from b200dft.constants import HARTREE_TO_EV
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_scf(m, setup, its=20):
+    ao = rks.ao_values(m, setup.coords)
+    return rks.scf(setup.S, setup.T, setup.V, setup.D0, oeri.eri_s8(m), ao, setup.weights,
+                   m.nelectron // 2, setup.E_nuc, its=its)
+
+
+@pytest.mark.parametrize("name", ["ch4", "water"])
+def test_scf_fp64_vs_oracle(cuda, name):
+    g = golden(f"scf_oracle_{name}.npz")
+    m = Mole(str(g["atom"]), unit=str(g["unit"]))
+    eng = RKSEngine([m], level=0, precision="fp64")
+    res = eng.run(its=20)
+    eng.close()
+    E = res["energies"][:, 0, 0]
+    assert np.abs(E - g["energies"][:, 0]).max() <= 1e-6           # north-star gate (Ha)
+    np.testing.assert_allclose(res["mo_energy"][-1, 0, :m.nao], g["mo_energy"], atol=1e-6)
+
+
+def test_scf_batch_uneven_fp64(cuda):
+    rng = np.random.default_rng(5)
+    mols = [Mole(methane()), Mole(random_molecule(rng, 2)), Mole(random_molecule(rng, 3))]
+    eng = RKSEngine(mols, level=0, precision="fp64")
+    res = eng.run(its=15)
+    for mi, m in enumerate(mols):
+        ref = oracle_scf(m, eng.setups[mi], its=15)
+        assert np.abs(res["energies"][:, mi, 0] - ref["energies"][:, 0]).max() <= 1e-6
+    eng.close()
+
+
+def test_scf_mixed_precision(cuda):
+    rng = np.random.default_rng(11)
+    m = Mole(random_molecule(rng, 4))
+    eng = RKSEngine([m], level=0, precision="mixed")
+    res = eng.run(its=20)
+    eng.close()
+    ref = oracle_scf(m, HostSetup(m, 0), its=20)
+    assert abs(res["energies"][-1, 0, 0] - ref["energies"][-1, 0]) <= 1e-4   # north-star: 1e-4 Ha
+
+
+def test_nanodft_dropin(cuda):
+    opts, mol_str = nanodft.nanoDFT_options(its=12, mol_str="methane", level=0)
+    mol = nanodft.build_mol(mol_str, opts.basis)
+    E, (logged, hl, mo_e, mo_c, coords, w) = nanodft.nanoDFT(mol, opts)
+    assert E.shape == (12, 5) and logged.shape == (12, 5)
+    g = golden("scf_oracle_ch4.npz")
+    np.testing.assert_allclose(E[:, 0] / HARTREE_TO_EV, g["energies"][:12, 0], atol=1e-6)
+    np.testing.assert_allclose(E, logged, atol=1e-6)                 # host FP64 recompute == device
+    # orbitals: C^T S C = 1 and S C = F C e structure
+    S, T, V = int1e(mol)
+    np.testing.assert_allclose(mo_c.T @ S @ mo_c, np.eye(mol.nao), atol=1e-8)
+    assert hl[-1] > 0 and len(w) == len(coords)
+
+
+def test_dft_dropin(cuda):
+    args = dft.get_args(["-its", "10", "-level", "0"])
+    m = Mole(methane())
+    s = "; ".join(f"{sym} {x} {y} {z}" for sym, (x, y, z) in zip(m.symbols, m.coords))
+    energies, e_tot, hlgap, t, _, _ = dft.jax_dft(s, args)
+    g = golden("scf_oracle_ch4.npz")
+    np.testing.assert_allclose(energies / 27.2114, g["energies"][:10, 0], atol=1e-6)
+    e, energy, eigval, eigvec, dms, L_inv = dft.density_functional_theory(None, args)
+    assert dms.shape == (10, 3, 9, 9)
+    np.testing.assert_allclose(dms[:, 0], np.transpose(dms[:, 0], (0, 2, 1)), atol=1e-12)

@@ -1,0 +1,84 @@
+"""Kernel arithmetic (the exact __host__ __device__ code of the CUDA kernels, built for the
+CPU in libb200dft_hostcheck.so) against the oracle."""
+import ctypes
+import os
+import numpy as np
+import pytest
+
+from conftest import golden
+from oracle import eri, rks
+from b200dft.mole import Mole, methane
+from b200dft._lib import HOSTCHECK_PATH
+
+
+def _hc():
+    if not os.path.exists(HOSTCHECK_PATH):
+        import subprocess, sys
+        subprocess.run([sys.executable, os.path.join(os.path.dirname(os.path.dirname(HOSTCHECK_PATH)),
+                        "..", "csrc", "build.py")], check=True)
+    return ctypes.CDLL(HOSTCHECK_PATH)
+
+
+def _p(a, t):
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def hc_eri(mols, prec):
+    hc = _hc()
+    atm = np.ascontiguousarray(np.concatenate([m._atm for m in mols]), np.int32)
+    bas = np.ascontiguousarray(np.concatenate([m._bas for m in mols]), np.int32)
+    env = np.concatenate([m._env for m in mols])
+    eo = np.cumsum([0] + [len(m._env) for m in mols[:-1]]).astype(np.int64)
+    natm = np.array([m.natm for m in mols], np.int32)
+    nbas = np.array([m.nbas for m in mols], np.int32)
+    out = np.full(sum(eri.n_s8(m.nao) for m in mols), np.nan)
+    rc = hc.b2hc_eri_s8(len(mols), _p(natm, ctypes.c_int), _p(nbas, ctypes.c_int), _p(atm, ctypes.c_int),
+                        _p(bas, ctypes.c_int), _p(env, ctypes.c_double), _p(eo, ctypes.c_longlong), prec,
+                        _p(out, ctypes.c_double))
+    assert rc == 0
+    return out
+
+
+def test_eri_math_fp64_vs_reference():
+    names = ("h2", "ch4", "water", "tree3")
+    gs = [golden(f"eri_ref_{n}.npz") for n in names]
+    mols = [Mole(str(g["atom"]), unit=str(g["unit"])) for g in gs]
+    v = hc_eri(mols, 64)
+    ref = np.concatenate([g["s8"] for g in gs])
+    assert not np.isnan(v).any()                     # every s8 slot written exactly by its row
+    np.testing.assert_allclose(v, ref, atol=1e-12, rtol=0)
+
+
+def test_eri_math_fp32():
+    g = golden("eri_ref_tree3.npz")
+    v = hc_eri([Mole(str(g["atom"]))], 32)
+    err = np.abs(v - g["s8"])
+    assert err.max() < 5e-6
+    assert (err / np.maximum(np.abs(g["s8"]), 1e-2)).max() < 5e-6
+
+
+def test_boys_device_math():
+    hc = _hc()
+    F = np.zeros(5)
+    for t in np.concatenate([np.linspace(0, 45, 301), [1e-9, 39.99, 40.0, 40.01, 120.0]]):
+        hc.b2hc_boys(4, ctypes.c_double(t), _p(F, ctypes.c_double))
+        ref = eri.boys(4, t)
+        np.testing.assert_allclose(F, ref, rtol=2e-14, atol=1e-17)
+
+
+def test_b3lyp_device_math():
+    hc = _hc()
+    rng = np.random.default_rng(0)
+    n = 4000
+    rho = np.zeros((4, n))
+    rho[0] = 10 ** rng.uniform(-12, 3, n)
+    rho[1:] = rng.normal(size=(3, n)) * rho[0] ** (4 / 3) * 10 ** rng.uniform(-3, 1, n)
+    rho[0, :4] = [0.0, 1e-10, -1e-5, 1e13]           # clipping edge cases (b3lyp.py:15)
+    rho = np.ascontiguousarray(rho)
+    e, vr, vg = np.zeros(n), np.zeros(n), np.zeros(n)
+    hc.b2hc_b3lyp(n, _p(rho, ctypes.c_double), _p(e, ctypes.c_double), _p(vr, ctypes.c_double),
+                  _p(vg, ctypes.c_double))
+    e0, vr0, vg0 = rks.b3lyp(rho)
+    np.testing.assert_allclose(e, e0, rtol=1e-12)
+    np.testing.assert_allclose(vr, vr0, rtol=1e-12)
+    np.testing.assert_allclose(vg, vg0, rtol=1e-10)
