@@ -62,9 +62,10 @@ __device__ __host__ inline void b2_schur2(double app, double aqq, double apq, do
   s = t * c;
 }
 
-// parallel cyclic Jacobi on A (n x n, n even, ld = n) in shared memory; V <- eigenvectors
-__device__ int b2_jacobi(double *A, double *V, int n, double *rot, int *prs, double *red,
-                         int max_sweeps) {
+// parallel cyclic Jacobi on A (n x n, n even, ld = n) in shared memory; V <- eigenvectors.
+// Rows/columns >= nreal are decoupled padding; convergence norms use the nreal block only.
+__device__ int b2_jacobi(double *A, double *V, int n, int nreal, double *rot, int *prs,
+                         double *red, int max_sweeps) {
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) V[e] = (e / n == e % n) ? 1.0 : 0.0;
   __syncthreads();
   const int half = n / 2;
@@ -72,9 +73,11 @@ __device__ int b2_jacobi(double *A, double *V, int n, double *rot, int *prs, dou
   for (; sweep < max_sweeps; ++sweep) {
     double off = 0, tot = 0;
     for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+      const int r = e / n, c = e - (e / n) * n;
+      if (r >= nreal || c >= nreal) continue;
       const double a = A[e];
       tot += a * a;
-      if (e / n != e % n) off += a * a;
+      if (r != c) off += a * a;
     }
     off = b2_block_sum(off, red);
     tot = b2_block_sum(tot, red);
@@ -273,7 +276,7 @@ k_eigh_density(const B2MolDev *__restrict__ mols, const int *__restrict__ active
     sA[e] = s;
   }
   __syncthreads();
-  const int sw = b2_jacobi(sA, sV, n, rot, prs, red, 30);
+  const int sw = b2_jacobi(sA, sV, n, N, rot, prs, red, 30);
   // ascending order of eigenvalues
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     const double li = sA[i * n + i];
