@@ -1,0 +1,340 @@
+"""Benchmark: SCF molecules/s on one B200 (batched mixed-precision engine).
+
+Workload: a seeded batch of synthetic molecules with the shape of the batched
+configuration (1-9 heavy atoms from C/N/O/F = 0.7/0.1/0.15/0.05, H to valence, STO-3G,
+B3LYP, level-0 grid); synthetic because the reference's GDB/QM1B data is not available.
+One step = the whole hot path over the batch from inputs resident in HBM: device setup
+(1e matrices, Becke grid, guess, L), ERIs (FP32, s8), AO values, and the SCF iterated per
+molecule until |dE| < 1e-6 Ha and DIIS error < 1e-4 with converged molecules retired.
+``e2e`` runs the same through the public API from host buffers (plan creation from the
+libcint host arrays, host->device copies, results copied back).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--nmol M] [--impl b200|reference]
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "pyscf-ipu_b200"))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "SCF molecules/s on 1 B200 at |dE|<=0.1 mHa: batched+learned vs plain FP64"
+UNIT = "molecules/s"
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampler during the timed region."""
+
+    def __init__(self):
+        self.samples = []
+        self.proc = None
+
+    def start(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            idx = os.environ.get("LOCAL_RANK", "0")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", idx, f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                                         text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(2)
+        except Exception:
+            self.proc.kill()
+        sm = [float(s[0]) for s in self.samples if s and s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if len(s) > 1 and s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = []
+        for k, n in enumerate(names):
+            if any(len(s) > 3 + k and s[3 + k].lower().startswith("active") for s in self.samples):
+                reasons.append(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def molecules(nmol, seed):
+    from b200dft.molgen import config3_batch
+    from b200dft.mole import Mole
+    return [Mole(s) for s in config3_batch(nmol, seed=seed)]
+
+
+# ------------------------------------------------------------------ CPU oracle baseline
+def _oracle_one(args):
+    atom, level, use_ref = args
+    import os as _os
+    import sys as _sys
+    _sys.path.insert(0, _os.path.join(ROOT, "pyscf-ipu_b200"))
+    _sys.path.insert(0, ROOT)
+    from oracle import eri as oeri, rks
+    from b200dft.mole import Mole
+    from b200dft.engine import HostSetup
+    m = Mole(atom)
+    s = HostSetup(m, level)
+    s8 = oeri.ref_eri_s8(m) if use_ref else oeri.eri_s8(m)
+    ao = rks.ao_values(m, s.coords)
+    r = rks.scf(s.S, s.T, s.V, s.D0, s8, ao, s.weights, m.nelectron // 2, s.E_nuc, its=20)
+    return float(r["energies"][-1, 0])
+
+
+def cpu_baseline(atoms, level, use_ref, procs):
+    import multiprocessing as mp
+    t0 = time.perf_counter()
+    if procs > 1:
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(procs) as pool:
+            es = pool.map(_oracle_one, [(a, level, use_ref) for a in atoms])
+    else:
+        es = [_oracle_one((a, level, use_ref)) for a in atoms]
+    dt = time.perf_counter() - t0
+    return len(atoms) / dt, dt, es
+
+
+def run_reference(a):
+    """--impl reference: the reference's CPU path (its own compiled int2e_sph for the ERIs,
+    the FP64 port for the rest) on the host cores, bounded sample per step."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import eri as oeri
+    use_ref = oeri.ref_available()
+    from b200dft.molgen import config3_batch
+    procs = os.cpu_count() or 1
+    per_step = max(procs, 8)
+    atoms = config3_batch(per_step * (a.steps + a.warmup), seed=a.seed)
+    vals = []
+    t_all = 0.0
+    for k in range(a.warmup + a.steps):
+        v, dt, _ = cpu_baseline(atoms[k * per_step:(k + 1) * per_step], a.level, use_ref, procs)
+        if k >= a.warmup:
+            vals.append(v)
+            t_all += dt
+    value = float(np.mean(vals))
+    kind = "reference" if use_ref else "port"
+    sample = f"{per_step} molecules per step of the batched distribution, 20 SCF iterations, level-{a.level} grid"
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": 1000 * t_all / max(1, a.steps), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": "batched uneven STO-3G B3LYP molecules (1-9 heavy atoms C/N/O/F), level-0 grid",
+                   "nmol": per_step},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+# ------------------------------------------------------------------ B200 arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--nmol", type=int, default=4096)
+    ap.add_argument("--level", type=int, default=0)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--plain-sample", type=int, default=32)
+    ap.add_argument("--cpu-sample", type=int, default=8)
+    ap.add_argument("--no-cpu", action="store_true")
+    a = ap.parse_args()
+    if a.impl == "reference":
+        return run_reference(a)
+
+    import torch
+    import torch.distributed as dist
+    from b200dft.engine import RKSEngine, Plan
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # weak scaling: every rank runs its own shard of molecules (no data-path collective)
+    mols = molecules(a.nmol, seed=a.seed + 1000 * rank)
+    eng = RKSEngine(mols, level=a.level, precision=a.precision)
+    ev = {k: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for k in ("setup", "eri", "ao", "scf")}
+
+    def one_step(record=False):
+        eng._setup_done = False
+        eng._eri_done = False
+        eng._ao_done = False
+        if record:
+            ev["setup"][0].record()
+        eng.device_setup()
+        if record:
+            ev["setup"][1].record()
+            ev["eri"][0].record()
+        eng.compute_eri()
+        if record:
+            ev["eri"][1].record()
+            ev["ao"][0].record()
+        eng.compute_ao()
+        if record:
+            ev["ao"][1].record()
+            ev["scf"][0].record()
+        r = eng.run_converged()
+        if record:
+            ev["scf"][1].record()
+        return r
+
+    for _ in range(a.warmup):
+        res = one_step()
+    barrier()
+    clk = Clocks()
+    clk.start()
+    phase = {k: 0.0 for k in ev}
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    barrier()
+    t_start.record()
+    its_total = 0
+    for _ in range(a.steps):
+        res = one_step(record=True)
+        its_total += res["its_run"]
+        torch.cuda.synchronize()
+        for k, (s, e) in ev.items():
+            phase[k] += s.elapsed_time(e)
+    t_end.record()
+    barrier()
+    clocks = clk.stop()
+    ms = max_over_ranks(t_start.elapsed_time(t_end)) / a.steps
+    value = world * a.nmol / (ms / 1000.0)
+    conv = res["converged"].cpu().numpy()
+    iters = res["iterations"].cpu().numpy()
+
+    # roofline of the ERI kernel's companion: the J/K kernel streams the s8 list once per call
+    P = eng.plan
+    hbm, peak_kind = _peaks()
+    rbytes = 4 if a.precision == "mixed" else 8
+    eng.D.copy_(eng.D0)
+    jk_ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    for _ in range(3):
+        eng.jk(active=None)
+    torch.cuda.synchronize()
+    njk = 10
+    jk_ev[0].record()
+    for _ in range(njk):
+        eng.jk(active=None)
+    jk_ev[1].record()
+    torch.cuda.synchronize()
+    jk_ms = jk_ev[0].elapsed_time(jk_ev[1]) / njk
+    jk_bytes = P.n_eri * rbytes
+    achieved = jk_bytes / (jk_ms / 1000.0) / 1e9
+    roofline = {"kernel": "k_jk_s8", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
+                "algorithmic_bytes_per_launch": jk_bytes, "ms_per_launch": jk_ms}
+
+    # e2e: public API from host buffers (plan creation = H2D of the libcint tables), results D2H
+    e2e = None
+    if rank == 0:
+        barrier()
+        t0 = time.perf_counter()
+        e2 = RKSEngine(mols, level=a.level, precision=a.precision)
+        r2 = e2.run_converged()
+        host_E = r2["energy"].cpu().numpy()
+        host_it = r2["iterations"].cpu().numpy()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        h2d = sum(m._atm.nbytes + m._bas.nbytes + m._env.nbytes for m in mols)
+        d2h = host_E.nbytes + host_it.nbytes
+        e2e = {"value": a.nmol / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+        e2.close()
+
+    # plain FP64 per-molecule GPU path on a sample (same convergence rule, minao guess)
+    plain = None
+    if rank == 0 and a.plain_sample > 0:
+        sample = mols[:a.plain_sample]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        plainE = []
+        for m in sample:
+            e1 = RKSEngine([m], level=a.level, precision="fp64")
+            r1 = e1.run_converged(graph=False)
+            plainE.append(float(r1["energy"][0]))
+            e1.close()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        dE = np.abs(np.array(plainE) - res["energy"].cpu().numpy()[:a.plain_sample])
+        plain = {"value": len(sample) / dt, "unit": UNIT, "sample": len(sample),
+                 "max_abs_dE_batched_vs_plain_Ha": float(dE.max())}
+
+    cpu = None
+    if rank == 0 and not a.no_cpu and a.cpu_sample > 0:
+        from oracle import eri as oeri
+        from b200dft.molgen import config3_batch
+        atoms = config3_batch(a.nmol, seed=a.seed)[:a.cpu_sample]
+        v, dt, _ = cpu_baseline(atoms, a.level, oeri.ref_available(), 1)
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "reference" if oeri.ref_available() else "port",
+               "sample": f"first {a.cpu_sample} molecules of the batch, 20 SCF iterations, FP64, 1 core ({dt:.1f}s)"}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64" if a.precision == "mixed" else "f64", "data": "synthetic",
+            "config": {"workload": "batched uneven STO-3G B3LYP molecules (1-9 heavy atoms C/N/O/F 0.7/0.1/0.15/0.05), level-0 grid",
+                       "nmol_per_gpu": a.nmol, "precision": a.precision,
+                       "l2": "inputs (s8 ERIs, AO values) larger than L2 between iterations",
+                       "convergence": "|dE|<1e-6 Ha and DIIS err<1e-4, retire converged"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "gpu_launches": None,
+            "phases_ms_per_step": {k: v / a.steps for k, v in phase.items()},
+            "scf": {"converged": int(conv.sum()), "of": int(len(conv)), "mean_its": float(iters[conv].mean()) if conv.any() else None,
+                    "p50_its": float(np.percentile(iters[conv], 50)) if conv.any() else None,
+                    "p99_its": float(np.percentile(iters[conv], 99)) if conv.any() else None},
+            "plain_fp64_per_molecule": plain,
+        }
+        print(json.dumps(out))
+    eng.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

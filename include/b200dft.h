@@ -64,9 +64,10 @@ int b2_eri_s8(b2_plan_t plan, int precision, void *eri_out, void *stream);
 /* J and K (float64, nao x nao per molecule) from the s8 list and D (float64).  Arithmetic in
  * `precision` (64 or 32, must match the ERI buffer).  Replaces sparse_symmetric_einsum
  * (nanoDFT/sparse_symmetric_ERI.py:86) and ipu_direct_mult (electron_repulsion/direct.py:489);
- * diff_JK = J - K*hyb/2 as in get_JK (nanoDFT.py:125-139). */
-int b2_jk_s8(b2_plan_t plan, int precision, const void *eri, const double *D, double *J,
-             double *K, void *stream);
+ * diff_JK = J - K*hyb/2 as in get_JK (nanoDFT.py:125-139).  active: device int[nmol] or NULL;
+ * molecules with active[m] == 0 are skipped and their J/K left untouched. */
+int b2_jk_s8(b2_plan_t plan, int precision, const int *active, const void *eri, const double *D,
+             double *J, double *K, void *stream);
 
 /* Register the grid layout: grid_off (host, nmol+1 prefix of per-molecule point counts).
  * Allocates the plan's grid tables and XC scratch on the device. */
@@ -81,8 +82,8 @@ int b2_ao_eval(b2_plan_t plan, int precision, const double *coords, void *ao, vo
 
 /* E_xc (nmol float64) and symmetric V_xc (float64 matrices) for densities D; replaces
  * exchange_correlation (nanoDFT.py:105-123) / xc (dft.py:899-1036) minus the J/K part. */
-int b2_xc(b2_plan_t plan, int precision, const void *ao, const double *weights, const double *D,
-          double *Vxc, double *Exc, void *stream);
+int b2_xc(b2_plan_t plan, int precision, const int *active, const void *ao,
+          const double *weights, const double *D, double *Vxc, double *Exc, void *stream);
 
 /* B3LYP at n points: rho (4 x n, device float64, rho[1:4] = half density gradient as the
  * reference forms it) -> e_xc, vrho, vgamma (device float64).  Replaces b3lyp(rho, eps)
@@ -112,6 +113,24 @@ int b2_eigh_density(b2_plan_t plan, const int *active, const double *H, const do
 int b2_energy(b2_plan_t plan, const int *active, const double *D, const double *Hcore,
               const double *diffJK, const double *Exc, const double *Enuc, double *out,
               void *stream);
+
+/* One-electron matrices S, T, V (float64 matrices) for every molecule; replaces
+ * mol.intor_symmetric('int1e_ovlp' / 'int1e_kin' / 'int1e_nuc') (dft.py:225-227). */
+int b2_int1e(b2_plan_t plan, double *S, double *T, double *V, void *stream);
+
+/* Becke-partitioned grid for every molecule (replaces Grids(mol).build(), dft.py:214-216 and
+ * pyscf_utils/build_grid.py:109-135).  tmpl: host float64 (x, y, z, w) per template point of
+ * each element's atom-centred grid, tmpl_off: host prefix (nz+1) indexed by nuclear charge.
+ * The layout registered by b2_grid_set must equal the sum of the atoms' template sizes.
+ * coords (n_points x 3) and weights (n_points): device float64. */
+int b2_grid_build(b2_plan_t plan, int nz, const double *tmpl, const int64_t *tmpl_off,
+                  double *coords, double *weights, void *stream);
+
+/* MINAO-style initial density (atomic occupations on the diagonal; minao, dft.py:223). */
+int b2_guess(b2_plan_t plan, double *D, void *stream);
+
+/* Nuclear repulsion per molecule (mol.energy_nuc(), dft.py:202); device float64 [nmol]. */
+int b2_enuc(b2_plan_t plan, double *enuc, void *stream);
 
 /* Single-molecule convenience mirroring the reference's native entry int2e_sph
  * (int2e_sph.cpp:6750): host libcint arrays in, all s8 ERIs of the molecule out (device). */

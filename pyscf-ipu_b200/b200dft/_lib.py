@@ -27,18 +27,22 @@ SIGNATURES = {
     "b2_plan_offsets": [_P, _P, _P, _P, _P],
     "b2_plan_set_jk_chunk": [_P, _L],
     "b2_eri_s8": [_P, _I, _P, _P],
-    "b2_jk_s8": [_P, _I, _P, _P, _P, _P, _P],
+    "b2_jk_s8": [_P, _I, _P, _P, _P, _P, _P, _P],
     "b2_grid_set": [_P, _P],
     "b2_grid_info": [_P, _P, _P],
     "b2_grid_ao_offsets": [_P, _P],
     "b2_ao_eval": [_P, _I, _P, _P, _P],
-    "b2_xc": [_P, _I, _P, _P, _P, _P, _P, _P],
+    "b2_xc": [_P, _I, _P, _P, _P, _P, _P, _P, _P],
     "b2_b3lyp": [_L, _P, _P, _P, _P, _P],
     "b2_chol_inv": [_P, _P, _P, _P, _P],
     "b2_fock_diis": [_P, _P, _P, _D, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "b2_eigh_density": [_P, _P, _P, _P, _P, _P, _P, _P, _P],
     "b2_energy": [_P, _P, _P, _P, _P, _P, _P, _P, _P],
     "b2_int2e_sph_s8": [_P, _I, _P, _I, _P, _I, _I, _P, _P],
+    "b2_int1e": [_P, _P, _P, _P, _P],
+    "b2_grid_build": [_P, _I, _P, _P, _P, _P, _P],
+    "b2_guess": [_P, _P, _P],
+    "b2_enuc": [_P, _P, _P],
 }
 
 

@@ -1,12 +1,14 @@
-"""Batched RKS engine on one B200: host setup + device SCF loop through the C ABI.
+"""Batched RKS engine on one B200: setup + device SCF loop through the C ABI.
 
 One ``RKSEngine`` holds a batch of molecules (one molecule for the drop-in entry points).
-Host setup mirrors what the reference does on the host with PySCF before its jitted SCF
-(dft.py:197-234, nanoDFT.py:208-257): molecule/basis (``Mole``), grid (``Grids``),
-one-electron matrices (``int1e``), L = inv(cholesky(S)) and the MINAO-style guess.  All
-arrays are then packed per molecule (offsets from the plan) into device buffers, and the
-SCF loop runs entirely on the device: ERIs once, then per iteration Fock+DIIS,
-orthogonalised eigensolve + density, XC and J/K, energies (nanoDFT.py:40-102).
+Setup mirrors what the reference does on the host with PySCF before its jitted SCF
+(dft.py:197-234, nanoDFT.py:208-257) -- molecule/basis (``Mole``), grid, one-electron
+matrices, L = inv(cholesky(S)), MINAO-style guess, nuclear repulsion -- and runs on the
+device by default (``setup="device"``) or on the host (``HostSetup`` list, numpy).  The SCF
+loop runs entirely on the device: ERIs once, then per iteration Fock+DIIS, orthogonalised
+eigensolve + density, XC and J/K, energies (nanoDFT.py:40-102).  ``run`` reproduces the
+reference's fixed iteration count; ``run_converged`` iterates each molecule until its DIIS
+error and energy change fall below thresholds and retires it (its kernels skip it).
 """
 import ctypes
 import numpy as np
@@ -14,11 +16,12 @@ import torch
 
 from ._lib import lib, check, ptr, stream_handle, B200DFTError
 from .constants import HYB_B3LYP
-from .grids import Grids
+from .grids import Grids, atomic_grid
 from .guess import minao
 from .int1e import int1e
 
 NMO = 72     # mo_energy row stride used by the device kernels
+NZ = 10      # nuclear charges 0..9 indexed in the grid template table
 
 
 class Plan:
@@ -73,7 +76,6 @@ class Plan:
         except Exception:
             pass
 
-    # matrices ------------------------------------------------------------------------
     def pack(self, mats):
         out = np.zeros(self.n_mat, np.float64)
         for m, a in enumerate(mats):
@@ -93,7 +95,7 @@ def _require_cuda():
 
 
 class HostSetup:
-    """Per-molecule host inputs (the reference's PySCF-side setup)."""
+    """Per-molecule host inputs (the reference's PySCF-side setup, numpy)."""
 
     def __init__(self, mol, level=0, grid=None, D0=None):
         self.mol = mol
@@ -109,40 +111,75 @@ class HostSetup:
         self.E_nuc = mol.energy_nuc()
 
 
+_TEMPLATES = {}
+
+
+def grid_templates(level):
+    """Atom-centred grid templates (x, y, z, w) per nuclear charge for ``level``."""
+    if level not in _TEMPLATES:
+        parts, off = [], [0]
+        for z in range(NZ):
+            if z in (1, 6, 7, 8, 9):
+                c, w = atomic_grid(z, level)
+                parts.append(np.concatenate([c, w[:, None]], 1))
+                off.append(off[-1] + len(w))
+            else:
+                off.append(off[-1])
+        _TEMPLATES[level] = (np.ascontiguousarray(np.concatenate(parts)), np.array(off, np.int64))
+    return _TEMPLATES[level]
+
+
 class RKSEngine:
     """Device SCF for a batch of molecules.
 
     precision: "fp64" (plain: FP64 ERIs, J/K and grid path) or "mixed" (FP32 ERIs, J/K and
     grid path; FP64 Fock/DIIS/eigensolve/energies).
+    setups: None (device setup) or a list of ``HostSetup``.
     """
 
-    def __init__(self, mols, level=0, precision="fp64", setups=None, device=None, jk_chunk=None):
+    def __init__(self, mols, level=0, precision="fp64", setups=None, device=None, jk_chunk=None,
+                 plan=None):
         _require_cuda()
         self.mols = list(mols)
+        self.level = level
         self.precision = precision
         self.prec = 64 if precision == "fp64" else 32
         self.device = torch.device(device or "cuda")
-        self.setups = setups or [HostSetup(m, level) for m in self.mols]
-        self.plan = Plan(self.mols)
+        self.setups = setups
+        self.plan = plan if plan is not None else Plan(self.mols)
         if jk_chunk:
             self.plan.set_jk_chunk(jk_chunk)
         P = self.plan
-        self.plan.set_grid([len(s.weights) for s in self.setups])
         dev = self.device
         f64 = dict(dtype=torch.float64, device=dev)
         rdt = torch.float64 if self.prec == 64 else torch.float32
-        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
-        self.S = t(P.pack([s.S for s in self.setups]))
-        self.Hcore = t(P.pack([s.Hcore for s in self.setups]))
-        self.Linv = t(P.pack([s.L_inv for s in self.setups]))
-        self.D0 = t(P.pack([s.D0 for s in self.setups]))
-        self.coords = t(np.concatenate([s.coords for s in self.setups]).reshape(-1))
-        self.weights = t(np.concatenate([s.weights for s in self.setups]))
-        self.enuc = torch.tensor([s.E_nuc for s in self.setups], **f64)
         nm, nmat = P.nmol, P.n_mat
-        self.eri = torch.empty(P.n_eri, dtype=rdt, device=dev)
-        self.ao = torch.empty(max(1, P.n_ao), dtype=rdt, device=dev)
         z = lambda n: torch.zeros(n, **f64)
+        if setups is not None:
+            t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+            P.set_grid([len(s.weights) for s in setups])
+            self.S = t(P.pack([s.S for s in setups]))
+            self.Hcore = t(P.pack([s.Hcore for s in setups]))
+            self.Linv = t(P.pack([s.L_inv for s in setups]))
+            self.D0 = t(P.pack([s.D0 for s in setups]))
+            self.coords = t(np.concatenate([s.coords for s in setups]).reshape(-1))
+            self.weights = t(np.concatenate([s.weights for s in setups]))
+            self.enuc = torch.tensor([s.E_nuc for s in setups], **f64)
+            self._setup_done = True
+        else:
+            tmpl, toff = grid_templates(level)
+            cnt = toff[1:] - toff[:-1]
+            P.set_grid([int(sum(cnt[int(q)] for q in m.charges)) for m in self.mols])
+            self.S, self.T, self.V = z(nmat), z(nmat), z(nmat)
+            self.Hcore, self.Linv, self.D0 = z(nmat), z(nmat), z(nmat)
+            self.coords = z(3 * P.n_points)
+            self.weights = z(max(1, P.n_points))
+            self.enuc = z(nm)
+            self.chol_status = torch.zeros(nm, dtype=torch.int32, device=dev)
+            self._tmpl = (tmpl, toff)
+            self._setup_done = False
+        self.eri = torch.empty(max(1, P.n_eri), dtype=rdt, device=dev)
+        self.ao = torch.empty(max(1, P.n_ao), dtype=rdt, device=dev)
         self.D, self.J, self.K, self.Vxc = z(nmat), z(nmat), z(nmat), z(nmat)
         self.H, self.diffJK = z(nmat), z(nmat)
         self.ring_err, self.ring_h = z(9 * nmat), z(9 * nmat)
@@ -157,6 +194,23 @@ class RKSEngine:
         self.sweeps = torch.zeros(nm, dtype=torch.int32, device=dev)
         self._eri_done = False
         self._ao_done = False
+        self._graph = None
+
+    # --- setup -------------------------------------------------------------------------
+    def device_setup(self, stream=None):
+        """1e matrices, grid, guess, L and E_nuc on the device (no host round trip)."""
+        if self._setup_done:
+            return
+        P, s = self.plan, stream_handle(stream)
+        tmpl, toff = self._tmpl
+        check(lib().b2_int1e(P.h, ptr(self.S), ptr(self.T), ptr(self.V), s), "b2_int1e")
+        torch.add(self.T, self.V, out=self.Hcore)
+        check(lib().b2_grid_build(P.h, NZ, ptr(tmpl), ptr(toff), ptr(self.coords), ptr(self.weights), s),
+              "b2_grid_build")
+        check(lib().b2_guess(P.h, ptr(self.D0), s), "b2_guess")
+        check(lib().b2_enuc(P.h, ptr(self.enuc), s), "b2_enuc")
+        check(lib().b2_chol_inv(P.h, ptr(self.S), ptr(self.Linv), ptr(self.chol_status), s), "b2_chol_inv")
+        self._setup_done = True
 
     # --- kernels -----------------------------------------------------------------------
     def compute_eri(self, stream=None):
@@ -168,15 +222,15 @@ class RKSEngine:
                                stream_handle(stream)), "b2_ao_eval")
         self._ao_done = True
 
-    def jk(self, D=None, stream=None):
+    def jk(self, D=None, active=None, stream=None):
         D = self.D if D is None else D
-        check(lib().b2_jk_s8(self.plan.h, self.prec, ptr(self.eri), ptr(D), ptr(self.J), ptr(self.K),
-                             stream_handle(stream)), "b2_jk_s8")
+        check(lib().b2_jk_s8(self.plan.h, self.prec, ptr(active), ptr(self.eri), ptr(D), ptr(self.J),
+                             ptr(self.K), stream_handle(stream)), "b2_jk_s8")
 
-    def xc(self, D=None, stream=None):
+    def xc(self, D=None, active=None, stream=None):
         D = self.D if D is None else D
-        check(lib().b2_xc(self.plan.h, self.prec, ptr(self.ao), ptr(self.weights), ptr(D), ptr(self.Vxc),
-                          ptr(self.exc), stream_handle(stream)), "b2_xc")
+        check(lib().b2_xc(self.plan.h, self.prec, ptr(active), ptr(self.ao), ptr(self.weights), ptr(D),
+                          ptr(self.Vxc), ptr(self.exc), stream_handle(stream)), "b2_xc")
 
     def fock_diis(self, use_diis=True, hyb=HYB_B3LYP, stream=None):
         check(lib().b2_fock_diis(self.plan.h, ptr(self.active), ptr(self.iter), float(hyb), int(use_diis),
@@ -195,11 +249,9 @@ class RKSEngine:
                               ptr(self.exc), ptr(self.enuc), ptr(self.energy), stream_handle(stream)),
               "b2_energy")
 
-    def diff_jk(self, hyb=HYB_B3LYP):
-        return self.J - 0.5 * hyb * self.K
-
     # --- SCF ----------------------------------------------------------------------------
     def prepare(self):
+        self.device_setup()
         if not self._eri_done:
             self.compute_eri()
         if not self._ao_done:
@@ -215,20 +267,20 @@ class RKSEngine:
 
     def step(self, use_diis=True):
         """One SCF iteration for every active molecule (nanoDFT.py:63-80)."""
+        a = self.active
         self.fock_diis(use_diis)
         self.eigh_density()
-        self.xc()
-        self.jk()
-        self.diffJK.copy_(self.diff_jk())
+        self.xc(active=a)
+        self.jk(active=a)
+        torch.add(self.J, self.K, alpha=-0.5 * HYB_B3LYP, out=self.diffJK)
         self.energies()
-        self.iter.add_(1)
+        self.iter.add_(self.active)
 
     def run(self, its=20, use_diis=True, log=True):
         """Fixed-iteration SCF as in the reference (no convergence test, fori_loop of `its`)."""
         self.prepare()
         self.initial()
-        P = self.plan
-        nm = P.nmol
+        nm = self.plan.nmol
         E = torch.zeros((its, nm, 5), dtype=torch.float64, device=self.device)
         mo = torch.zeros((its, nm, NMO), dtype=torch.float64, device=self.device)
         derr = torch.zeros((its, nm), dtype=torch.float64, device=self.device)
@@ -245,6 +297,52 @@ class RKSEngine:
             out["logs"] = torch.stack(logs).cpu().numpy()      # (its, 4, n_mat): D, diff_JK, H, J
         out["C"] = self.C.cpu().numpy()
         return out
+
+    def _capture(self, use_diis):
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            self.step(use_diis)                       # warm-up launch outside capture
+        torch.cuda.current_stream().wait_stream(s)
+        return g
+
+    def run_converged(self, max_its=40, e_tol=1e-6, diis_tol=1e-4, use_diis=True, graph=True,
+                      check_every=1):
+        """Iterate until each molecule's |E_i - E_{i-1}| < e_tol and DIIS error < diis_tol, then
+        retire it (its kernels skip it).  Returns per-molecule energies, iterations and flags."""
+        self.prepare()
+        self.initial()
+        nm = self.plan.nmol
+        dev = self.device
+        e_prev = torch.full((nm,), float("inf"), dtype=torch.float64, device=dev)
+        conv_it = torch.full((nm,), -1, dtype=torch.int32, device=dev)
+        g = None
+        if graph:
+            # capture one iteration (all launches go to the capture stream); replay per step
+            st = torch.cuda.Stream()
+            st.wait_stream(torch.cuda.current_stream())
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.stream(st):
+                with torch.cuda.graph(g, stream=st):
+                    self.step(use_diis)
+            torch.cuda.current_stream().wait_stream(st)
+            # the capture did not execute the step: state is unchanged
+        for i in range(max_its):
+            if g is not None:
+                g.replay()
+            else:
+                self.step(use_diis)
+            e = self.energy.view(nm, 5)[:, 0]
+            newly = (self.active > 0) & ((e - e_prev).abs() < e_tol) & (self.diis_err < diis_tol)
+            conv_it = torch.where(newly, torch.full_like(conv_it, i + 1), conv_it)
+            self.active.masked_fill_(newly, 0)
+            e_prev = torch.where(self.active > 0, e, e_prev)
+            if (i + 1) % check_every == 0 and int(self.active.sum().item()) == 0:
+                break
+        E = self.energy.view(nm, 5)[:, 0].clone()
+        return dict(energy=E, iterations=conv_it, converged=conv_it > 0, mo_energy=self.mo_energy.view(nm, NMO),
+                    diis_err=self.diis_err.clone(), its_run=i + 1)
 
     def close(self):
         self.plan.close()

@@ -7,6 +7,7 @@
 #include "xc.cuh"
 #include "scf.cuh"
 #include "xc_math.cuh"
+#include "setup.cuh"
 
 static thread_local std::string g_last_error;
 
@@ -37,6 +38,7 @@ static void b2_plan_free(B2PlanDev *P) {
 
 static int b2_set_jk_chunk(B2PlanDev *P, long long elems) {
   if (elems <= 0) elems = 32768;
+  elems = (elems + 2047) / 2048 * 2048;          // whole runs of 8 for every thread of a CTA
   const int nmol = P->h.nmol;
   std::vector<long long> off(nmol + 1, 0);
   for (int m = 0; m < nmol; ++m) off[m + 1] = off[m] + (P->h.mols[m].n4 + elems - 1) / elems;
@@ -116,10 +118,10 @@ int b2_eri_s8(void *plan, int precision, void *eri_out, void *stream) {
   return rc;
 }
 
-int b2_jk_s8(void *plan, int precision, const void *eri, const double *D, double *J, double *K,
-             void *stream) {
+int b2_jk_s8(void *plan, int precision, const int *active, const void *eri, const double *D,
+             double *J, double *K, void *stream) {
   if (!plan || !eri || !D || !J || !K) return B2_ERR_ARG;
-  return b2_launch_jk_s8(*(B2PlanDev *)plan, precision, eri, D, J, K, (cudaStream_t)stream);
+  return b2_launch_jk_s8(*(B2PlanDev *)plan, precision, active, eri, D, J, K, (cudaStream_t)stream);
 }
 
 int b2_grid_set(void *plan, const int64_t *grid_off) {
@@ -148,11 +150,11 @@ int b2_ao_eval(void *plan, int precision, const double *coords, void *ao, void *
   return b2_launch_ao_eval(*(B2PlanDev *)plan, precision, coords, ao, (cudaStream_t)stream);
 }
 
-int b2_xc(void *plan, int precision, const void *ao, const double *weights, const double *D,
-          double *Vxc, double *Exc, void *stream) {
+int b2_xc(void *plan, int precision, const int *active, const void *ao, const double *weights,
+          const double *D, double *Vxc, double *Exc, void *stream) {
   if (!plan || !ao || !weights || !D || !Vxc || !Exc) return B2_ERR_ARG;
   B2PlanDev *P = (B2PlanDev *)plan;
-  return b2_launch_xc(*P, precision, ao, weights, D, Vxc, Exc, P->g.rt, (cudaStream_t)stream);
+  return b2_launch_xc(*P, precision, active, ao, weights, D, Vxc, Exc, nullptr, (cudaStream_t)stream);
 }
 
 __global__ void k_b3lyp_points(long long n, const double *__restrict__ rho, double *exc,
@@ -212,6 +214,28 @@ int b2_int2e_sph_s8(const int *atm, int natm, const int *bas, int nbas, const do
   if (!rc) rc = b2_note(cudaStreamSynchronize((cudaStream_t)stream));
   b2_plan_destroy(plan);
   return rc;
+}
+
+int b2_int1e(void *plan, double *S, double *T, double *V, void *stream) {
+  if (!plan || !S || !T || !V) return B2_ERR_ARG;
+  return b2_launch_int1e(*(B2PlanDev *)plan, S, T, V, (cudaStream_t)stream);
+}
+
+int b2_grid_build(void *plan, int nz, const double *tmpl, const int64_t *tmpl_off, double *coords,
+                  double *weights, void *stream) {
+  if (!plan || !tmpl || !tmpl_off || !coords || !weights) return B2_ERR_ARG;
+  return b2_launch_grid_build(*(B2PlanDev *)plan, nz, tmpl, (const long long *)tmpl_off, coords,
+                              weights, (cudaStream_t)stream);
+}
+
+int b2_guess(void *plan, double *D, void *stream) {
+  if (!plan || !D) return B2_ERR_ARG;
+  return b2_launch_guess(*(B2PlanDev *)plan, D, (cudaStream_t)stream);
+}
+
+int b2_enuc(void *plan, double *enuc, void *stream) {
+  if (!plan || !enuc) return B2_ERR_ARG;
+  return b2_launch_enuc(*(B2PlanDev *)plan, enuc, (cudaStream_t)stream);
 }
 
 }  // extern "C"

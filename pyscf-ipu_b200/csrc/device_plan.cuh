@@ -4,9 +4,13 @@
 #include "boys.cuh"
 
 struct B2GridDev {             // grid layout registered with b2_grid_set
-  long long n_points = 0, n_gblk = 0, n_vblk = 0, n_ao = 0;
-  long long *grid_off = nullptr, *gblk_off = nullptr, *vblk_off = nullptr, *ao_off = nullptr;
-  double *rt = nullptr;        // scratch: 4 x n_points
+  long long n_points = 0, n_gblk = 0, n_xblk32 = 0, n_xblk64 = 0, n_ao = 0;
+  long long *grid_off = nullptr, *gblk_off = nullptr, *ao_off = nullptr;
+  long long *xblk32 = nullptr, *xblk64 = nullptr;   // fused-XC CTA prefix per precision
+  int tpc32 = 1, tpc64 = 1;                         // tiles per CTA
+  double *rt = nullptr;        // unused (kept for layout compatibility)
+  double *tmpl = nullptr;      // atomic grid templates (x, y, z, w)
+  long long *tmpl_off = nullptr, *atom_pt_off = nullptr;
   std::vector<long long> grid_off_h, ao_off_h;
 };
 
@@ -32,5 +36,6 @@ struct B2PlanDev {
 };
 
 int b2_launch_eri_s8(const B2PlanDev &P, int precision, void *out, cudaStream_t st);
-int b2_launch_jk_s8(const B2PlanDev &P, int precision, const void *eri, const double *D, double *J,
-                    double *K, cudaStream_t st);
+int b2_launch_jk_s8(const B2PlanDev &P, int precision, const int *active, const void *eri,
+                    const double *D, double *J, double *K, cudaStream_t st);
+int b2_zero_active(const B2PlanDev &P, const int *active, double *A, double *B, cudaStream_t st);

@@ -30,9 +30,12 @@ int b2hc_eri_s8(int nmol, const int *natm, const int *nbas, const int *atm, cons
   if (rc) return rc;
   std::vector<double> tab(B2_BOYS_NT * B2_BOYS_NM);
   b2_boys_fill_table(tab.data());
+  long long packed = 0;                     // output: molecules' s8 lists back to back
   for (int m = 0; m < nmol; ++m) {
     const B2MolDev &md = P.mols[m];
     long long n2 = (long long)md.nao * (md.nao + 1) / 2;
+    double *om = out + packed;
+    packed += md.n4;
     for (long long ij = 0; ij < n2; ++ij) {
       B2RowInfo r = b2_row_info(md, ij, P.ao2sh.data(), P.pinfo.data());
       int cnt[4];
@@ -48,7 +51,7 @@ int b2hc_eri_s8(int nmol, const int *natm, const int *nbas, const int *atm, cons
             const B2PairInfo &kp = P.pinfo[md.sp_off + KL];
             double acc[3][3];
             b2_eri_dispatch<double>(r.bcls, c, bra, nb, &P.pp64[(size_t)(md.sp_off + KL) * 9], r.ci, r.cj, tab.data(), acc);
-            b2_eri_store<double, double>(out + md.eri_off, ij, kp, kp.I == kp.J, acc);
+            b2_eri_store<double, double>(om, ij, kp, kp.I == kp.J, acc);
           }
       } else {
         B2BraPrim<float> bra[9];
@@ -61,7 +64,7 @@ int b2hc_eri_s8(int nmol, const int *natm, const int *nbas, const int *atm, cons
             const B2PairInfo &kp = P.pinfo[md.sp_off + KL];
             float acc[3][3];
             b2_eri_dispatch<float>(r.bcls, c, bra, nb, &P.pp32[(size_t)(md.sp_off + KL) * 9], r.ci, r.cj, tab.data(), acc);
-            b2_eri_store<float, double>(out + md.eri_off, ij, kp, kp.I == kp.J, acc);
+            b2_eri_store<float, double>(om, ij, kp, kp.I == kp.J, acc);
           }
       }
     }

@@ -5,15 +5,21 @@
 // repetition count 2^(d_ij + d_kl + d_(ij,kl)) (num_repetitions_fast, lines 68-79) and
 // applied through all 8 index permutations to J[k,l] = sum (ij|kl) D[j,i] and
 // K[i,l] = sum (ij|kl) D[j,k] (nanoDFT.py:129-132).  With D symmetric the 8 permutations
-// reduce to 2 J and 4 K updates of one triangle-agnostic accumulator followed by
-// J = Jacc + Jacc^T, K = Kacc + Kacc^T.
+// reduce to 2 J and 4 K updates of one accumulator followed by J = Jacc + Jacc^T,
+// K = Kacc + Kacc^T.
 //
-// Decomposition: one CTA per chunk of one molecule's s8 list.  D, Jacc and Kacc live in
-// shared memory (nao <= 70), ERIs stream from HBM once with coalesced loads; the index
-// quadruple is decoded from the list position in registers (no index arrays, unlike the
-// reference's int16 index tensors, nanoDFT.py:310-313).  Each CTA adds its partial J and K
-// to global memory at the end.
+// Decomposition: one CTA per chunk of one molecule's s8 list; D, Jacc and Kacc live in
+// shared memory in float64 (nao <= 70).  Each thread walks runs of 8 consecutive list
+// entries (two 16-byte vector loads for float32 storage), decoding (i,j,k,l) once per run
+// and then incrementally.  Partial sums whose target is fixed along the run stay in
+// registers -- Jacc[i,j] for the row, Kacc[i,k] and Kacc[j,k] for a k-run -- and are added
+// when the run leaves that row / k-run; Jacc[k,l], Kacc[i,l], Kacc[j,l] are added per entry
+// with shared-memory float64 atomics.  ERIs may be stored in float32, but every product and
+// sum is float64: the SCF map stays a smooth (linear) function of D, which keeps DIIS
+// converging below the float32 rounding level.
 #include "device_plan.cuh"
+
+#define B2_JK_RUN 8
 
 __device__ __forceinline__ long long b2_untri_fast(long long p) {
   long long i = (long long)((sqrtf(8.0f * (float)p + 1.0f) - 1.0f) * 0.5f);
@@ -22,78 +28,146 @@ __device__ __forceinline__ long long b2_untri_fast(long long p) {
   return i;
 }
 
+template <typename T> struct B2Vec;
+template <> struct B2Vec<float> {
+  __device__ static void load8(const float *p, double *v) {
+    const float4 a = *reinterpret_cast<const float4 *>(p);
+    const float4 b = *reinterpret_cast<const float4 *>(p + 4);
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+  }
+};
+template <> struct B2Vec<double> {
+  __device__ static void load8(const double *p, double *v) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double2 a = *reinterpret_cast<const double2 *>(p + 2 * q);
+      v[2 * q] = a.x; v[2 * q + 1] = a.y;
+    }
+  }
+};
+
 template <typename T>
 __global__ void __launch_bounds__(256)
 k_jk_s8(const B2MolDev *__restrict__ mols, const long long *__restrict__ chunk_off, int nmol,
-        long long chunk, const T *__restrict__ eri, const double *__restrict__ D,
-        double *__restrict__ J, double *__restrict__ K) {
-  extern __shared__ unsigned char smem_raw[];
-  T *sD = reinterpret_cast<T *>(smem_raw);
+        long long chunk, const int *__restrict__ active, const T *__restrict__ eri,
+        const double *__restrict__ D, double *__restrict__ J, double *__restrict__ K) {
+  extern __shared__ double smem_d[];
   const long long cid = blockIdx.x;
   int lo = 0, hi = nmol - 1;
   while (lo < hi) {
     int mid = (lo + hi + 1) >> 1;
     if (chunk_off[mid] <= cid) lo = mid; else hi = mid - 1;
   }
+  if (active && !active[lo]) return;
   const B2MolDev md = mols[lo];
   const int N = md.nao, NN = N * N;
-  T *sJ = sD + NN;
-  T *sK = sJ + NN;
+  double *sD = smem_d, *sJ = sD + NN, *sK = sJ + NN;
   for (int e = threadIdx.x; e < NN; e += blockDim.x) {
-    sD[e] = (T)D[md.mat_off + e];
-    sJ[e] = (T)0;
-    sK[e] = (T)0;
+    sD[e] = D[md.mat_off + e];
+    sJ[e] = 0.0;
+    sK[e] = 0.0;
   }
   __syncthreads();
   const long long p0 = (cid - chunk_off[lo]) * chunk;
   const long long p1 = min(p0 + chunk, md.n4);
   const T *E = eri + md.eri_off;
-  for (long long p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
-    T v = E[p];
-    if (v == (T)0) continue;
-    const long long ij = b2_untri_fast(p);
-    const int kl = (int)(p - ij * (ij + 1) / 2);
-    const int i = (int)b2_untri_fast(ij);
-    const int j = (int)(ij - (long long)i * (i + 1) / 2);
-    const int k = (int)b2_untri_fast(kl);
-    const int l = kl - k * (k + 1) / 2;
-    if (i == j) v *= (T)0.5;
-    if (k == l) v *= (T)0.5;
-    if (ij == kl) v *= (T)0.5;
-    const T v2 = v + v;
-    atomicAdd(&sJ[i * N + j], v2 * sD[k * N + l]);
-    atomicAdd(&sJ[k * N + l], v2 * sD[i * N + j]);
-    atomicAdd(&sK[i * N + k], v * sD[j * N + l]);
-    atomicAdd(&sK[i * N + l], v * sD[j * N + k]);
-    atomicAdd(&sK[j * N + k], v * sD[i * N + l]);
-    atomicAdd(&sK[j * N + l], v * sD[i * N + k]);
+  for (long long base = p0 + (long long)threadIdx.x * B2_JK_RUN; base < p1;
+       base += (long long)blockDim.x * B2_JK_RUN) {
+    double v[B2_JK_RUN];
+    B2Vec<T>::load8(E + base, v);
+    // decode the first entry of the run
+    long long ij = b2_untri_fast(base);
+    int kl = (int)(base - ij * (ij + 1) / 2);
+    int i = (int)b2_untri_fast(ij), j = (int)(ij - (long long)i * (i + 1) / 2);
+    int k = (int)b2_untri_fast(kl), l = kl - k * (k + 1) / 2;
+    double Dij = sD[i * N + j];
+    double aJ = 0, aKi = 0, aKj = 0;
+    const int nrun = (int)min((long long)B2_JK_RUN, p1 - base);
+#pragma unroll
+    for (int r = 0; r < B2_JK_RUN; ++r) {
+      if (r < nrun) {
+        double f = v[r];
+        if (f != 0.0) {
+          if (i == j) f *= 0.5;
+          if (k == l) f *= 0.5;
+          if (ij == kl) f *= 0.5;
+          aJ += f * sD[k * N + l];
+          aKi += f * sD[j * N + l];
+          aKj += f * sD[i * N + l];
+          atomicAdd(&sJ[k * N + l], 2.0 * f * Dij);
+          atomicAdd(&sK[i * N + l], f * sD[j * N + k]);
+          atomicAdd(&sK[j * N + l], f * sD[i * N + k]);
+        }
+        const bool row_end = (kl == ij);
+        const bool run_end = row_end || (l == k) || (r == nrun - 1);
+        if (run_end) {                              // leave the k-run: flush its partials
+          if (aKi != 0.0) atomicAdd(&sK[i * N + k], aKi);
+          if (aKj != 0.0) atomicAdd(&sK[j * N + k], aKj);
+          aKi = 0; aKj = 0;
+        }
+        if (row_end || r == nrun - 1) {             // leave the row: flush Jacc[i,j]
+          if (aJ != 0.0) atomicAdd(&sJ[i * N + j], 2.0 * aJ);
+          aJ = 0;
+        }
+        if (row_end) {
+          ++ij; kl = 0; k = 0; l = 0;
+          if (++j > i) { ++i; j = 0; }
+          Dij = sD[i * N + j < NN ? i * N + j : 0];
+        } else {
+          ++kl;
+          if (l == k) { ++k; l = 0; } else { ++l; }
+        }
+      }
+    }
   }
   __syncthreads();
   for (int e = threadIdx.x; e < NN; e += blockDim.x) {
     const int a = e / N, b = e - (e / N) * N;
-    const T jv = sJ[a * N + b] + sJ[b * N + a];
-    const T kv = sK[a * N + b] + sK[b * N + a];
-    if (jv != (T)0) atomicAdd(&J[md.mat_off + e], (double)jv);
-    if (kv != (T)0) atomicAdd(&K[md.mat_off + e], (double)kv);
+    const double jv = sJ[a * N + b] + sJ[b * N + a];
+    const double kv = sK[a * N + b] + sK[b * N + a];
+    if (jv != 0.0) atomicAdd(&J[md.mat_off + e], jv);
+    if (kv != 0.0) atomicAdd(&K[md.mat_off + e], kv);
   }
 }
 
-int b2_launch_jk_s8(const B2PlanDev &P, int precision, const void *eri, const double *D, double *J,
-                    double *K, cudaStream_t st) {
+__global__ void k_zero_active(const B2MolDev *__restrict__ mols, const int *__restrict__ active,
+                              double *__restrict__ A, double *__restrict__ B) {
+  const int m = blockIdx.x;
+  if (active && !active[m]) return;
+  const B2MolDev md = mols[m];
+  for (int e = threadIdx.x; e < md.nao * md.nao; e += blockDim.x) {
+    A[md.mat_off + e] = 0.0;
+    if (B) B[md.mat_off + e] = 0.0;
+  }
+}
+
+int b2_zero_active(const B2PlanDev &P, const int *active, double *A, double *B, cudaStream_t st) {
+  k_zero_active<<<P.h.nmol, 256, 0, st>>>(P.mols, active, A, B);
+  B2_CUDA_TRY(cudaGetLastError());
+  return B2_OK;
+}
+
+int b2_launch_jk_s8(const B2PlanDev &P, int precision, const int *active, const void *eri,
+                    const double *D, double *J, double *K, cudaStream_t st) {
   if (P.jk_nchunks <= 0) return B2_OK;
-  B2_CUDA_TRY(cudaMemsetAsync(J, 0, sizeof(double) * P.h.n_mat, st));
-  B2_CUDA_TRY(cudaMemsetAsync(K, 0, sizeof(double) * P.h.n_mat, st));
+  if (P.jk_chunk % (256 * B2_JK_RUN) != 0) return B2_ERR_ARG;
+  if (active) {
+    int rc = b2_zero_active(P, active, J, K, st);
+    if (rc) return rc;
+  } else {
+    B2_CUDA_TRY(cudaMemsetAsync(J, 0, sizeof(double) * P.h.n_mat, st));
+    B2_CUDA_TRY(cudaMemsetAsync(K, 0, sizeof(double) * P.h.n_mat, st));
+  }
   const int N = P.h.max_nao;
+  const size_t sm = sizeof(double) * 3 * N * N;
   if (precision == 64) {
-    size_t sm = sizeof(double) * 3 * N * N;
     B2_CUDA_TRY(cudaFuncSetAttribute(k_jk_s8<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     k_jk_s8<double><<<(unsigned)P.jk_nchunks, 256, sm, st>>>(P.mols, P.jk_chunk_off, P.h.nmol,
-                                                            P.jk_chunk, (const double *)eri, D, J, K);
+        P.jk_chunk, active, (const double *)eri, D, J, K);
   } else if (precision == 32) {
-    size_t sm = sizeof(float) * 3 * N * N;
     B2_CUDA_TRY(cudaFuncSetAttribute(k_jk_s8<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     k_jk_s8<float><<<(unsigned)P.jk_nchunks, 256, sm, st>>>(P.mols, P.jk_chunk_off, P.h.nmol,
-                                                           P.jk_chunk, (const float *)eri, D, J, K);
+        P.jk_chunk, active, (const float *)eri, D, J, K);
   } else {
     return B2_ERR_ARG;
   }

@@ -32,7 +32,7 @@ struct B2PlanHost {
   int nmol = 0;
   int max_nao = 0;
   long long n_eri = 0, n_rows = 0, n_mat = 0;
-  int n_sh = 0, n_sp = 0, n_ao = 0, n_atm = 0;
+  int n_sh = 0, n_sp = 0, n_ao = 0, n_atm = 0;   // n_eri: padded total (see eri_off)
   std::vector<B2MolDev> mols;
   std::vector<long long> row_off;         // nmol + 1
   std::vector<B2Shell> shells;
@@ -164,7 +164,7 @@ static int b2_plan_build(B2PlanHost &P, int nmol, const int *natm, const int *nb
     P.n_sp += nsp;
     P.n_ao += nao;
     P.n_atm += natm[m];
-    P.n_eri += md.n4;
+    P.n_eri += (md.n4 + 31) / 32 * 32;          // 128-byte aligned per molecule (vector loads)
     P.n_rows += n2;
     P.n_mat += (long long)nao * nao;
     P.row_off[m + 1] = P.n_rows;

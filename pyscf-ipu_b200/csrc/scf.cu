@@ -62,26 +62,31 @@ __device__ __host__ inline void b2_schur2(double app, double aqq, double apq, do
   s = t * c;
 }
 
-// parallel cyclic Jacobi on A (n x n, n even, ld = n) in shared memory; V <- eigenvectors.
-// Rows/columns >= nreal are decoupled padding; convergence norms use the nreal block only.
+// parallel cyclic Jacobi on A (n x n, n even, leading dimension ld = n + 1) in shared memory;
+// V (same layout) <- eigenvectors.  Rows/columns >= nreal are decoupled padding; the
+// convergence norms use the nreal block only.  Stops when the off-diagonal Frobenius norm is
+// below 1e-13 of the total (eigenvectors then accurate to ~1e-13), or after max_sweeps.
 __device__ int b2_jacobi(double *A, double *V, int n, int nreal, double *rot, int *prs,
                          double *red, int max_sweeps) {
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) V[e] = (e / n == e % n) ? 1.0 : 0.0;
+  const int ld = n + 1;
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
+    const int r = e / n, c = e - (e / n) * n;
+    V[r * ld + c] = (r == c) ? 1.0 : 0.0;
+  }
   __syncthreads();
   const int half = n / 2;
   int sweep = 0;
   for (; sweep < max_sweeps; ++sweep) {
     double off = 0, tot = 0;
-    for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-      const int r = e / n, c = e - (e / n) * n;
-      if (r >= nreal || c >= nreal) continue;
-      const double a = A[e];
+    for (int e = threadIdx.x; e < nreal * nreal; e += blockDim.x) {
+      const int r = e / nreal, c = e - (e / nreal) * nreal;
+      const double a = A[r * ld + c];
       tot += a * a;
       if (r != c) off += a * a;
     }
     off = b2_block_sum(off, red);
     tot = b2_block_sum(tot, red);
-    if (off <= 1e-30 * tot || off < 1e-300) break;
+    if (off <= 1e-26 * tot || off < 1e-300) break;
     for (int r = 0; r < n - 1; ++r) {
       if (threadIdx.x < half) {
         const int k = threadIdx.x;
@@ -90,7 +95,12 @@ __device__ int b2_jacobi(double *A, double *V, int n, int nreal, double *rot, in
         const int b = ((kb - 1 + r) % (n - 1)) + 1;
         const int p = min(a, b), q = max(a, b);
         double c, s;
-        b2_schur2(A[p * n + p], A[q * n + q], A[p * n + q], c, s);
+        const double apq = A[p * ld + q];
+        if (fabs(apq) <= 1e-300 || fabs(apq) < 1e-17 * sqrt(fabs(A[p * ld + p] * A[q * ld + q]))) {
+          c = 1.0; s = 0.0;                         // already negligible
+        } else {
+          b2_schur2(A[p * ld + p], A[q * ld + q], apq, c, s);
+        }
         prs[2 * k] = p; prs[2 * k + 1] = q;
         rot[2 * k] = c; rot[2 * k + 1] = s;
       }
@@ -99,21 +109,23 @@ __device__ int b2_jacobi(double *A, double *V, int n, int nreal, double *rot, in
         const int k = e / n, col = e - (e / n) * n;
         const int p = prs[2 * k], q = prs[2 * k + 1];
         const double c = rot[2 * k], s = rot[2 * k + 1];
-        const double apk = A[p * n + col], aqk = A[q * n + col];
-        A[p * n + col] = c * apk - s * aqk;
-        A[q * n + col] = s * apk + c * aqk;
+        if (s == 0.0) continue;
+        const double apk = A[p * ld + col], aqk = A[q * ld + col];
+        A[p * ld + col] = c * apk - s * aqk;
+        A[q * ld + col] = s * apk + c * aqk;
       }
       __syncthreads();
       for (int e = threadIdx.x; e < half * n; e += blockDim.x) {      // cols: A <- A J, V <- V J
         const int k = e / n, row = e - (e / n) * n;
         const int p = prs[2 * k], q = prs[2 * k + 1];
         const double c = rot[2 * k], s = rot[2 * k + 1];
-        const double akp = A[row * n + p], akq = A[row * n + q];
-        A[row * n + p] = c * akp - s * akq;
-        A[row * n + q] = s * akp + c * akq;
-        const double vkp = V[row * n + p], vkq = V[row * n + q];
-        V[row * n + p] = c * vkp - s * vkq;
-        V[row * n + q] = s * vkp + c * vkq;
+        if (s == 0.0) continue;
+        const double akp = A[row * ld + p], akq = A[row * ld + q];
+        A[row * ld + p] = c * akp - s * akq;
+        A[row * ld + q] = s * akp + c * akq;
+        const double vkp = V[row * ld + p], vkq = V[row * ld + q];
+        V[row * ld + p] = c * vkp - s * vkq;
+        V[row * ld + q] = s * vkp + c * vkq;
       }
       __syncthreads();
     }
@@ -127,11 +139,13 @@ __device__ void b2_jacobi_small(double *A, double *V, int n) {
   for (int sweep = 0; sweep < 50; ++sweep) {
     double off = 0, tot = 0;
     for (int i = 0; i < n * n; ++i) { tot += A[i] * A[i]; if (i / n != i % n) off += A[i] * A[i]; }
-    if (off <= 1e-32 * tot || off < 1e-300) break;
+    if (off <= 1e-28 * tot || off < 1e-300) break;
     for (int p = 0; p < n - 1; ++p)
       for (int q = p + 1; q < n; ++q) {
+        const double apq = A[p * n + q];
+        if (fabs(apq) <= 1e-300 || fabs(apq) < 1e-18 * sqrt(fabs(A[p * n + p] * A[q * n + q]))) continue;
         double c, s;
-        b2_schur2(A[p * n + p], A[q * n + q], A[p * n + q], c, s);
+        b2_schur2(A[p * n + p], A[q * n + q], apq, c, s);
         if (s == 0.0) continue;
         for (int k = 0; k < n; ++k) {
           const double apk = A[p * n + k], aqk = A[q * n + k];
@@ -259,8 +273,9 @@ k_eigh_density(const B2MolDev *__restrict__ mols, const int *__restrict__ active
   const B2MolDev md = mols[m];
   const int N = md.nao, NN = N * N;
   const int n = (N + 1) & ~1;                     // even size for the round-robin ordering
+  const int ld = n + 1;                            // odd leading dimension: no bank conflicts
   const long long mo = md.mat_off;
-  double *sL = sm, *sT = sL + NN, *sA = sT + NN, *sV = sA + n * n;
+  double *sL = sm, *sT = sL + NN, *sA = sT + NN, *sV = sA + n * ld;
   for (int e = threadIdx.x; e < NN; e += blockDim.x) { sL[e] = Linv[mo + e]; sA[e] = H[mo + e]; }
   __syncthreads();
   b2_mm(sL, sA, sT, N, false);                    // L H
@@ -273,28 +288,28 @@ k_eigh_density(const B2MolDev *__restrict__ mols, const int *__restrict__ active
       for (int k = 0; k < N; ++k) s += sT[r * N + k] * sL[c * N + k];
     else if (r == c)
       s = 1e30;                                    // padding: decoupled, sorts last
-    sA[e] = s;
+    sA[r * ld + c] = s;
   }
   __syncthreads();
   const int sw = b2_jacobi(sA, sV, n, N, rot, prs, red, 30);
   // ascending order of eigenvalues
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const double li = sA[i * n + i];
+    const double li = sA[i * ld + i];
     int rank = 0;
     for (int j = 0; j < n; ++j) {
-      const double lj = sA[j * n + j];
+      const double lj = sA[j * ld + j];
       rank += (lj < li) || (lj == li && j < i);
     }
     order[rank] = i;
   }
   __syncthreads();
-  for (int k = threadIdx.x; k < N; k += blockDim.x) mo_energy[(long long)m * B2_MAXNAO + k] = sA[order[k] * n + order[k]];
+  for (int k = threadIdx.x; k < N; k += blockDim.x) mo_energy[(long long)m * B2_MAXNAO + k] = sA[order[k] * ld + order[k]];
   // C[:, k] = L^T V[:, order[k]]  (all N columns, into sT)
   for (int e = threadIdx.x; e < NN; e += blockDim.x) {
     const int r = e / N, k = e - (e / N) * N;
     const int col = order[k];
     double s = 0;
-    for (int a = 0; a < N; ++a) s += sL[a * N + r] * sV[a * n + col];
+    for (int a = 0; a < N; ++a) s += sL[a * N + r] * sV[a * ld + col];
     sT[e] = s;
   }
   __syncthreads();
@@ -380,7 +395,7 @@ __global__ void k_chol_inv(const B2MolDev *__restrict__ mols, const double *__re
 }
 
 static size_t b2_fock_smem(int N) { return sizeof(double) * 4 * N * N; }
-static size_t b2_eigh_smem(int N) { int n = (N + 1) & ~1; return sizeof(double) * (2 * N * N + 2 * n * n); }
+static size_t b2_eigh_smem(int N) { int n = (N + 1) & ~1; return sizeof(double) * (2 * N * N + 2 * n * (n + 1)); }
 
 int b2_launch_fock_diis(const B2PlanDev &P, const int *active, const int *iter, double hyb,
                         int use_diis, const double *Hcore, const double *S, const double *D,

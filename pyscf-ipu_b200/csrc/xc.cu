@@ -66,89 +66,150 @@ k_ao_eval(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
   }
 }
 
-// rho + B3LYP per point; writes rt[4][G] (scratch) and accumulates E_xc per molecule
-template <typename T>
-__global__ void __launch_bounds__(128)
-k_rho_b3lyp(const B2MolDev *__restrict__ mols, const long long *__restrict__ gblk_off,
-            const long long *__restrict__ grid_off, const long long *__restrict__ ao_off, int nmol,
-            const T *__restrict__ ao, const double *__restrict__ w, const double *__restrict__ D,
-            T *__restrict__ rt, double *__restrict__ exc) {
-  __shared__ T sD[B2_MAXNAO * B2_MAXNAO];
-  __shared__ double red[4];
-  const int m = b2_find(gblk_off, nmol, blockIdx.x);
+// Fused XC tile kernel: a CTA owns TPC consecutive tiles of PT points of one molecule.
+// Per tile: the 4 AO components (PT x nao) are staged in shared memory; threads (tx, ty) of a
+// 16x16 layout compute X = AO0 * D register-blocked (points ty+16r, orbitals tx+16q), reduce
+// rho_c = sum_n X AO_c across the 16 tx lanes with shuffles, evaluate B3LYP per point, form
+// Y = sum_c AO_c rt_c in place and accumulate V += AO0^T Y in registers (rows ty+16r, cols
+// tx+16q) across the CTA's tiles; one float64 atomic flush per CTA.
+#define B2_XC_NP 80          // padded orbital dimension (5 x 16)
+template <typename T, int PT>
+__global__ void __launch_bounds__(256)
+k_xc_fused(const B2MolDev *__restrict__ mols, const long long *__restrict__ xblk_off,
+           const long long *__restrict__ grid_off, const long long *__restrict__ ao_off, int nmol,
+           int tpc, const int *__restrict__ active, const T *__restrict__ ao,
+           const double *__restrict__ w, const double *__restrict__ D, double *__restrict__ V,
+           double *__restrict__ exc) {
+  constexpr int R = PT / 16;                 // points per thread (rows)
+  constexpr int NP = B2_XC_NP, LD = NP + 1;  // odd leading dimension
+  extern __shared__ unsigned char smem_raw[];
+  T *sD = reinterpret_cast<T *>(smem_raw);             // [NP][NP]
+  T *sA = sD + NP * NP;                                 // [4][PT][LD]
+  __shared__ T sRt[PT][4];
+  __shared__ double red[8];
+  const int m = b2_find(xblk_off, nmol, blockIdx.x);
+  if (active && !active[m]) return;
   const B2MolDev md = mols[m];
   const int N = md.nao;
-  for (int e = threadIdx.x; e < N * N; e += blockDim.x) sD[e] = (T)D[md.mat_off + e];
-  __syncthreads();
-  const long long G = grid_off[m + 1] - grid_off[m];
-  const long long g = (blockIdx.x - gblk_off[m]) * blockDim.x + threadIdx.x;
-  double e_part = 0;
-  if (g < G) {
-    const long long cs = G * N;
-    const T *a0 = ao + ao_off[m] + g * N;
-    T r0 = 0, r1 = 0, r2 = 0, r3 = 0;
-    for (int n = 0; n < N; ++n) {
-      T xn = 0;
-      for (int k = 0; k < N; ++k) xn += a0[k] * sD[k * N + n];
-      r0 += xn * a0[n];
-      r1 += xn * a0[cs + n];
-      r2 += xn * a0[2 * cs + n];
-      r3 += xn * a0[3 * cs + n];
-    }
-    const B2XcPoint<T> o = b2_b3lyp_point<T>(r0, r1, r2, r3);
-    const double wg = w[grid_off[m] + g];
-    e_part = (double)r0 * wg * (double)o.exc;
-    T *rtm = rt + 4 * grid_off[m];
-    rtm[g] = (T)(o.vrho * (T)0.5 * (T)wg);
-    const T f4 = (T)4 * o.vgamma * (T)wg;
-    rtm[G + g] = f4 * r1;
-    rtm[2 * G + g] = f4 * r2;
-    rtm[3 * G + g] = f4 * r3;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  for (int e = threadIdx.x; e < NP * NP; e += blockDim.x) {
+    const int a = e / NP, b = e - (e / NP) * NP;
+    sD[e] = (a < N && b < N) ? (T)D[md.mat_off + a * N + b] : (T)0;
   }
-  // block reduction of e_part
+  const long long G = grid_off[m + 1] - grid_off[m];
+  const long long cs = G * N;
+  const T *Am = ao + ao_off[m];
+  const double *wm = w + grid_off[m];
+  T vacc[5][5];
+#pragma unroll
+  for (int r = 0; r < 5; ++r)
+#pragma unroll
+    for (int q = 0; q < 5; ++q) vacc[r][q] = (T)0;
+  double e_part = 0;
+  const long long t0 = (blockIdx.x - xblk_off[m]) * (long long)tpc;
+  for (int tt = 0; tt < tpc; ++tt) {
+    const long long g0 = (t0 + tt) * PT;
+    if (g0 >= G) break;
+    const int np = (int)min((long long)PT, G - g0);
+    __syncthreads();                       // previous tile fully consumed
+    for (int c = 0; c < 4; ++c) {
+      const T *src = Am + c * cs + g0 * N;
+      for (int e = threadIdx.x; e < PT * NP; e += blockDim.x) {
+        const int p = e / NP, n = e - (e / NP) * NP;
+        sA[(c * PT + p) * LD + n] = (p < np && n < N) ? src[p * N + n] : (T)0;
+      }
+    }
+    __syncthreads();
+    // X = AO0 * D
+    T x[R][5];
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int q = 0; q < 5; ++q) x[r][q] = (T)0;
+    for (int k = 0; k < N; ++k) {
+      T a[R], d[5];
+#pragma unroll
+      for (int r = 0; r < R; ++r) a[r] = sA[(ty + 16 * r) * LD + k];
+#pragma unroll
+      for (int q = 0; q < 5; ++q) d[q] = sD[k * NP + tx + 16 * q];
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) x[r][q] += a[r] * d[q];
+    }
+    // rho_c for the thread's points, reduced over the 16 tx lanes
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int p = ty + 16 * r;
+      T rc[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        T s = 0;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) s += x[r][q] * sA[(c * PT + p) * LD + tx + 16 * q];
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        rc[c] = s;
+      }
+      if (tx == 0) {
+        double wg = 0;
+        T rt0 = 0, f4 = 0;
+        if (p < np) {
+          const B2XcPoint<T> o = b2_b3lyp_point<T>(rc[0], rc[1], rc[2], rc[3]);
+          wg = wm[g0 + p];
+          e_part += (double)rc[0] * wg * (double)o.exc;
+          rt0 = o.vrho * (T)0.5 * (T)wg;
+          f4 = (T)4 * o.vgamma * (T)wg;
+        }
+        sRt[p][0] = rt0;
+        sRt[p][1] = f4 * rc[1];
+        sRt[p][2] = f4 * rc[2];
+        sRt[p][3] = f4 * rc[3];
+      }
+    }
+    __syncthreads();
+    // Y = sum_c AO_c rt_c (into the AO_x tile)
+    for (int e = threadIdx.x; e < PT * NP; e += blockDim.x) {
+      const int p = e / NP, n = e - (e / NP) * NP;
+      const T y = sA[p * LD + n] * sRt[p][0] + sA[(PT + p) * LD + n] * sRt[p][1] +
+                  sA[(2 * PT + p) * LD + n] * sRt[p][2] + sA[(3 * PT + p) * LD + n] * sRt[p][3];
+      sA[(PT + p) * LD + n] = y;
+    }
+    __syncthreads();
+    // V += AO0^T Y
+    for (int p = 0; p < np; ++p) {
+      T a[5], y[5];
+#pragma unroll
+      for (int r = 0; r < 5; ++r) a[r] = sA[p * LD + ty + 16 * r];
+#pragma unroll
+      for (int q = 0; q < 5; ++q) y[q] = sA[(PT + p) * LD + tx + 16 * q];
+#pragma unroll
+      for (int r = 0; r < 5; ++r)
+#pragma unroll
+        for (int q = 0; q < 5; ++q) vacc[r][q] += a[r] * y[q];
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 5; ++r)
+#pragma unroll
+    for (int q = 0; q < 5; ++q) {
+      const int a = ty + 16 * r, b = tx + 16 * q;
+      if (a < N && b < N && vacc[r][q] != (T)0) atomicAdd(&V[md.mat_off + a * N + b], (double)vacc[r][q]);
+    }
   for (int o = 16; o > 0; o >>= 1) e_part += __shfl_down_sync(0xffffffffu, e_part, o);
   if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = e_part;
   __syncthreads();
-  if (threadIdx.x == 0) atomicAdd(&exc[m], red[0] + red[1] + red[2] + red[3]);
-}
-
-// V_raw[a,b] += sum_g AO0[g,a] * (sum_c AO_c[g,b] rt_c[g]) over a chunk of points
-#define B2_VXC_PTS 64
-template <typename T>
-__global__ void __launch_bounds__(256)
-k_vxc(const B2MolDev *__restrict__ mols, const long long *__restrict__ vblk_off,
-      const long long *__restrict__ grid_off, const long long *__restrict__ ao_off, int nmol,
-      const T *__restrict__ ao, const T *__restrict__ rt, double *__restrict__ V) {
-  extern __shared__ unsigned char smem_raw[];
-  T *sA = reinterpret_cast<T *>(smem_raw);                 // [PTS][N]
-  const int m = b2_find(vblk_off, nmol, blockIdx.x);
-  const B2MolDev md = mols[m];
-  const int N = md.nao;
-  T *sY = sA + B2_VXC_PTS * N;                            // [PTS][N]
-  const long long G = grid_off[m + 1] - grid_off[m];
-  const long long g0 = (blockIdx.x - vblk_off[m]) * B2_VXC_PTS;
-  const int np = (int)min((long long)B2_VXC_PTS, G - g0);
-  const long long cs = G * N;
-  const T *A = ao + ao_off[m];
-  const T *R = rt + 4 * grid_off[m];
-  for (int e = threadIdx.x; e < np * N; e += blockDim.x) {
-    const int p = e / N, b = e - (e / N) * N;
-    const long long gi = g0 + p;
-    sA[p * N + b] = A[gi * N + b];
-    sY[p * N + b] = A[gi * N + b] * R[gi] + A[cs + gi * N + b] * R[G + gi] +
-                    A[2 * cs + gi * N + b] * R[2 * G + gi] + A[3 * cs + gi * N + b] * R[3 * G + gi];
-  }
-  __syncthreads();
-  for (int e = threadIdx.x; e < N * N; e += blockDim.x) {
-    const int a = e / N, b = e - (e / N) * N;
-    T s = 0;
-    for (int p = 0; p < np; ++p) s += sA[p * N + a] * sY[p * N + b];
-    atomicAdd(&V[md.mat_off + e], (double)s);
+  if (threadIdx.x == 0) {
+    double s = 0;
+    for (int i = 0; i < 8; ++i) s += red[i];
+    atomicAdd(&exc[m], s);
   }
 }
 
 // V <- V + V^T per molecule
-__global__ void k_sym(const B2MolDev *__restrict__ mols, double *__restrict__ V) {
+__global__ void k_sym(const B2MolDev *__restrict__ mols, const int *__restrict__ active,
+                      double *__restrict__ V) {
+  if (active && !active[blockIdx.x]) return;
   const B2MolDev md = mols[blockIdx.x];
   const int N = md.nao;
   double *v = V + md.mat_off;
@@ -164,41 +225,57 @@ __global__ void k_sym(const B2MolDev *__restrict__ mols, double *__restrict__ V)
   }
 }
 
+static void b2_xc_split(const std::vector<long long> &goff, int nmol, int pt, int &tpc,
+                        std::vector<long long> &xblk) {
+  long long tiles = 0;
+  for (int m = 0; m < nmol; ++m) tiles += (goff[m + 1] - goff[m] + pt - 1) / pt;
+  // enough CTAs to fill the GPU several times over, each flushing V once
+  tpc = (int)std::max(1ll, std::min(16ll, tiles / (8ll * 148ll)));
+  xblk.assign(nmol + 1, 0);
+  for (int m = 0; m < nmol; ++m) {
+    const long long nt = (goff[m + 1] - goff[m] + pt - 1) / pt;
+    xblk[m + 1] = xblk[m] + (nt + tpc - 1) / tpc;
+  }
+}
+
 int b2_grid_setup(B2PlanDev &P, const long long *grid_off_host) {
   b2_grid_free(P);
   const int nmol = P.h.nmol;
   std::vector<long long> goff(grid_off_host, grid_off_host + nmol + 1), gblk(nmol + 1, 0),
-      vblk(nmol + 1, 0), aoff(nmol + 1, 0);
+      aoff(nmol + 1, 0), x32, x64;
   for (int m = 0; m < nmol; ++m) {
     long long G = goff[m + 1] - goff[m];
     if (G < 0) return B2_ERR_ARG;
     gblk[m + 1] = gblk[m] + (G + 127) / 128;
-    vblk[m + 1] = vblk[m] + (G + B2_VXC_PTS - 1) / B2_VXC_PTS;
     aoff[m + 1] = aoff[m] + 4 * G * P.h.mols[m].nao;
   }
+  b2_xc_split(goff, nmol, 64, P.g.tpc32, x32);
+  b2_xc_split(goff, nmol, 32, P.g.tpc64, x64);
   P.g.n_points = goff[nmol];
   P.g.n_gblk = gblk[nmol];
-  P.g.n_vblk = vblk[nmol];
+  P.g.n_xblk32 = x32[nmol];
+  P.g.n_xblk64 = x64[nmol];
   P.g.n_ao = aoff[nmol];
   P.g.grid_off_h = goff;
   P.g.ao_off_h = aoff;
   size_t nb = sizeof(long long) * (nmol + 1);
   B2_CUDA_TRY(cudaMalloc(&P.g.grid_off, nb));
   B2_CUDA_TRY(cudaMalloc(&P.g.gblk_off, nb));
-  B2_CUDA_TRY(cudaMalloc(&P.g.vblk_off, nb));
+  B2_CUDA_TRY(cudaMalloc(&P.g.xblk32, nb));
+  B2_CUDA_TRY(cudaMalloc(&P.g.xblk64, nb));
   B2_CUDA_TRY(cudaMalloc(&P.g.ao_off, nb));
   B2_CUDA_TRY(cudaMemcpy(P.g.grid_off, goff.data(), nb, cudaMemcpyHostToDevice));
   B2_CUDA_TRY(cudaMemcpy(P.g.gblk_off, gblk.data(), nb, cudaMemcpyHostToDevice));
-  B2_CUDA_TRY(cudaMemcpy(P.g.vblk_off, vblk.data(), nb, cudaMemcpyHostToDevice));
+  B2_CUDA_TRY(cudaMemcpy(P.g.xblk32, x32.data(), nb, cudaMemcpyHostToDevice));
+  B2_CUDA_TRY(cudaMemcpy(P.g.xblk64, x64.data(), nb, cudaMemcpyHostToDevice));
   B2_CUDA_TRY(cudaMemcpy(P.g.ao_off, aoff.data(), nb, cudaMemcpyHostToDevice));
-  // scratch for rt (4 x points) in double (covers both precisions)
-  B2_CUDA_TRY(cudaMalloc(&P.g.rt, sizeof(double) * 4 * std::max<long long>(1, P.g.n_points)));
   return B2_OK;
 }
 
 void b2_grid_free(B2PlanDev &P) {
-  cudaFree(P.g.grid_off); cudaFree(P.g.gblk_off); cudaFree(P.g.vblk_off); cudaFree(P.g.ao_off);
-  cudaFree(P.g.rt);
+  cudaFree(P.g.grid_off); cudaFree(P.g.gblk_off); cudaFree(P.g.xblk32); cudaFree(P.g.xblk64);
+  cudaFree(P.g.ao_off);
+  cudaFree(P.g.tmpl); cudaFree(P.g.tmpl_off); cudaFree(P.g.atom_pt_off);
   P.g = B2GridDev();
 }
 
@@ -217,31 +294,42 @@ int b2_launch_ao_eval(const B2PlanDev &P, int precision, const double *coords, v
   return B2_OK;
 }
 
-template <typename T>
-static int b2_xc_impl(const B2PlanDev &P, const T *ao, const double *w, const double *D, double *V,
-                      double *exc, T *rt, cudaStream_t st) {
-  B2_CUDA_TRY(cudaMemsetAsync(V, 0, sizeof(double) * P.h.n_mat, st));
-  B2_CUDA_TRY(cudaMemsetAsync(exc, 0, sizeof(double) * P.h.nmol, st));
-  if (P.g.n_gblk > 0)
-    k_rho_b3lyp<T><<<(unsigned)P.g.n_gblk, 128, 0, st>>>(P.mols, P.g.gblk_off, P.g.grid_off,
-        P.g.ao_off, P.h.nmol, ao, w, D, rt, exc);
-  const int N = P.h.max_nao;
-  size_t sm = sizeof(T) * 2 * B2_VXC_PTS * N;
-  B2_CUDA_TRY(cudaFuncSetAttribute(k_vxc<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  if (P.g.n_vblk > 0)
-    k_vxc<T><<<(unsigned)P.g.n_vblk, 256, sm, st>>>(P.mols, P.g.vblk_off, P.g.grid_off, P.g.ao_off,
-                                                    P.h.nmol, ao, rt, V);
-  k_sym<<<P.h.nmol, 256, 0, st>>>(P.mols, V);
+__global__ void k_zero_exc(int nmol, const int *__restrict__ active, double *__restrict__ exc) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m < nmol && (!active || active[m])) exc[m] = 0.0;
+}
+
+template <typename T, int PT>
+static int b2_xc_impl(const B2PlanDev &P, const int *active, const T *ao, const double *w,
+                      const double *D, double *V, double *exc, const long long *xblk, long long nblk,
+                      int tpc, cudaStream_t st) {
+  if (active) {
+    int rc = b2_zero_active(P, active, V, nullptr, st);
+    if (rc) return rc;
+  } else {
+    B2_CUDA_TRY(cudaMemsetAsync(V, 0, sizeof(double) * P.h.n_mat, st));
+  }
+  k_zero_exc<<<(P.h.nmol + 255) / 256, 256, 0, st>>>(P.h.nmol, active, exc);
+  const size_t sm = sizeof(T) * (B2_XC_NP * B2_XC_NP + 4 * PT * (B2_XC_NP + 1));
+  B2_CUDA_TRY(cudaFuncSetAttribute(k_xc_fused<T, PT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  if (nblk > 0)
+    k_xc_fused<T, PT><<<(unsigned)nblk, 256, sm, st>>>(P.mols, xblk, P.g.grid_off, P.g.ao_off,
+                                                       P.h.nmol, tpc, active, ao, w, D, V, exc);
+  k_sym<<<P.h.nmol, 256, 0, st>>>(P.mols, active, V);
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }
 
-int b2_launch_xc(const B2PlanDev &P, int precision, const void *ao, const double *w,
-                 const double *D, double *V, double *exc, void *rt_scratch, cudaStream_t st) {
+int b2_launch_xc(const B2PlanDev &P, int precision, const int *active, const void *ao,
+                 const double *w, const double *D, double *V, double *exc, void *rt_scratch,
+                 cudaStream_t st) {
   if (!P.g.grid_off) return B2_ERR_ARG;
+  (void)rt_scratch;
   if (precision == 64)
-    return b2_xc_impl<double>(P, (const double *)ao, w, D, V, exc, (double *)rt_scratch, st);
+    return b2_xc_impl<double, 32>(P, active, (const double *)ao, w, D, V, exc, P.g.xblk64,
+                                  P.g.n_xblk64, P.g.tpc64, st);
   if (precision == 32)
-    return b2_xc_impl<float>(P, (const float *)ao, w, D, V, exc, (float *)rt_scratch, st);
+    return b2_xc_impl<float, 64>(P, active, (const float *)ao, w, D, V, exc, P.g.xblk32,
+                                 P.g.n_xblk32, P.g.tpc32, st);
   return B2_ERR_ARG;
 }

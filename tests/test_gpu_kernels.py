@@ -21,13 +21,17 @@ def _mols():
     return [Mole(str(g["atom"]), unit=str(g["unit"])) for g in gs], gs
 
 
-def _eri(mols, prec, cuda):
+def _eri(mols, prec, cuda, raw=False):
+    """device s8 lists; the plan pads each molecule's list to 32 entries"""
     P = Plan(mols)
     out = torch.full((P.n_eri,), float("nan"), dtype=torch.float64 if prec == 64 else torch.float32,
                      device=cuda)
     check(lib().b2_eri_s8(P.h, prec, ptr(out), stream_handle()), "eri")
     torch.cuda.synchronize()
-    return P, out.double().cpu().numpy()
+    v = out.double().cpu().numpy()
+    if raw:
+        return P, v
+    return P, np.concatenate([v[P.eri_off[i]:P.eri_off[i] + oeri.n_s8(int(P.nao[i]))] for i in range(P.nmol)])
 
 
 def test_eri_s8_fp64_vs_reference(cuda):
@@ -77,7 +81,7 @@ def _sym_random(n, rng):
 @pytest.mark.parametrize("prec", [64, 32])
 def test_jk_parity(cuda, prec):
     mols, gs = _mols()
-    P, v = _eri(mols, prec, cuda)
+    P, v = _eri(mols, prec, cuda, raw=True)
     rng = np.random.default_rng(0)
     Ds = [_sym_random(m.nao, rng) for m in mols]
     eri_t = torch.from_numpy(v).to(cuda).to(torch.float64 if prec == 64 else torch.float32)
@@ -87,7 +91,7 @@ def test_jk_parity(cuda, prec):
     for chunk in (0, 64, 1000):               # several work splits give the same answer
         if chunk:
             P.set_jk_chunk(chunk)
-        check(lib().b2_jk_s8(P.h, prec, ptr(eri_t), ptr(D), ptr(J), ptr(K), stream_handle()), "jk")
+        check(lib().b2_jk_s8(P.h, prec, None, ptr(eri_t), ptr(D), ptr(J), ptr(K), stream_handle()), "jk")
         torch.cuda.synchronize()
         Jh, Kh = J.cpu().numpy(), K.cpu().numpy()
         for mi, (m, g) in enumerate(zip(mols, gs)):
@@ -99,7 +103,7 @@ def test_jk_parity(cuda, prec):
 
 def test_ao_eval_and_xc(cuda):
     mols = [Mole(methane()), Mole("O 0 0 0.1173; H 0 0.7572 -0.4692; H 0 -0.7572 -0.4692")]
-    eng = RKSEngine(mols, level=0, precision="fp64")
+    eng = RKSEngine(mols, level=0, precision="fp64", setups=[HostSetup(m, 0) for m in mols])
     eng.compute_ao()
     torch.cuda.synchronize()
     ao = eng.ao.cpu().numpy()

@@ -40,7 +40,7 @@ def test_scf_batch_uneven_fp64(cuda):
     eng = RKSEngine(mols, level=0, precision="fp64")
     res = eng.run(its=15)
     for mi, m in enumerate(mols):
-        ref = oracle_scf(m, eng.setups[mi], its=15)
+        ref = oracle_scf(m, HostSetup(m, 0), its=15)
         assert np.abs(res["energies"][:, mi, 0] - ref["energies"][:, 0]).max() <= 1e-6
     eng.close()
 
@@ -79,3 +79,48 @@ def test_dft_dropin(cuda):
     e, energy, eigval, eigvec, dms, L_inv = dft.density_functional_theory(None, args)
     assert dms.shape == (10, 3, 9, 9)
     np.testing.assert_allclose(dms[:, 0], np.transpose(dms[:, 0], (0, 2, 1)), atol=1e-12)
+
+
+def test_device_setup_matches_host(cuda):
+    rng = np.random.default_rng(3)
+    mols = [Mole(methane()), Mole(random_molecule(rng, 3)), Mole(random_molecule(rng, 5))]
+    eng = RKSEngine(mols, level=0, precision="fp64")
+    eng.device_setup()
+    torch.cuda.synchronize()
+    P = eng.plan
+    off = P.grid_off
+    coords = eng.coords.cpu().numpy().reshape(-1, 3)
+    w = eng.weights.cpu().numpy()
+    for mi, m in enumerate(mols):
+        hs = HostSetup(m, 0)
+        for name, ref in (("S", hs.S), ("T", hs.T), ("V", hs.V), ("Linv", hs.L_inv), ("D0", hs.D0)):
+            got = P.unpack(getattr(eng, name).cpu().numpy(), mi)
+            np.testing.assert_allclose(got, ref, atol=1e-10, err_msg=name)
+        np.testing.assert_allclose(coords[off[mi]:off[mi + 1]], hs.coords, atol=1e-12)
+        np.testing.assert_allclose(w[off[mi]:off[mi + 1]], hs.weights, rtol=1e-10, atol=1e-14)
+        assert abs(eng.enuc[mi].item() - hs.E_nuc) < 1e-10
+    eng.close()
+
+
+def test_run_converged_batched_mixed_vs_plain(cuda):
+    rng = np.random.default_rng(21)
+    mols = [Mole(random_molecule(rng, int(k))) for k in (1, 2, 4, 6, 3, 9)]
+    eng = RKSEngine(mols, level=0, precision="mixed")
+    res = eng.run_converged(max_its=40)
+    assert bool(res["converged"].all())
+    E = res["energy"].cpu().numpy()
+    for mi, m in enumerate(mols):
+        e1 = RKSEngine([m], level=0, precision="fp64")
+        r1 = e1.run_converged(graph=False)
+        e1.close()
+        assert abs(E[mi] - float(r1["energy"][0])) <= 1e-4          # |dE| <= 0.1 mHa
+    eng.close()
+
+
+def test_converged_graph_equals_eager(cuda):
+    rng = np.random.default_rng(8)
+    mols = [Mole(random_molecule(rng, 3)), Mole(methane())]
+    a = RKSEngine(mols, level=0, precision="fp64").run_converged(graph=True)
+    b = RKSEngine(mols, level=0, precision="fp64").run_converged(graph=False)
+    np.testing.assert_allclose(a["energy"].cpu().numpy(), b["energy"].cpu().numpy(), atol=1e-10)
+    assert (a["iterations"].cpu().numpy() == b["iterations"].cpu().numpy()).all()
