@@ -214,8 +214,6 @@ def main():
         if record:
             ev["eri"][1].record()
             ev["ao"][0].record()
-        eng.compute_ao()
-        if record:
             ev["ao"][1].record()
             ev["scf"][0].record()
         r = eng.run_converged()

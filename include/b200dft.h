@@ -85,6 +85,11 @@ int b2_ao_eval(b2_plan_t plan, int precision, const double *coords, void *ao, vo
 int b2_xc(b2_plan_t plan, int precision, const int *active, const void *ao,
           const double *weights, const double *D, double *Vxc, double *Exc, void *stream);
 
+/* As b2_xc, with AO values and gradients generated on the fly per tile of grid points from
+ * the basis (no stored AO tensor); coords: device float64 (n_points x 3). */
+int b2_xc_direct(b2_plan_t plan, int precision, const int *active, const double *coords,
+                 const double *weights, const double *D, double *Vxc, double *Exc, void *stream);
+
 /* B3LYP at n points: rho (4 x n, device float64, rho[1:4] = half density gradient as the
  * reference forms it) -> e_xc, vrho, vgamma (device float64).  Replaces b3lyp(rho, eps)
  * (exchange_correlation/b3lyp.py:13). */

@@ -33,6 +33,7 @@ SIGNATURES = {
     "b2_grid_ao_offsets": [_P, _P],
     "b2_ao_eval": [_P, _I, _P, _P, _P],
     "b2_xc": [_P, _I, _P, _P, _P, _P, _P, _P, _P],
+    "b2_xc_direct": [_P, _I, _P, _P, _P, _P, _P, _P, _P],
     "b2_b3lyp": [_L, _P, _P, _P, _P, _P],
     "b2_chol_inv": [_P, _P, _P, _P, _P],
     "b2_fock_diis": [_P, _P, _P, _D, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],

@@ -179,7 +179,7 @@ class RKSEngine:
             self._tmpl = (tmpl, toff)
             self._setup_done = False
         self.eri = torch.empty(max(1, P.n_eri), dtype=rdt, device=dev)
-        self.ao = torch.empty(max(1, P.n_ao), dtype=rdt, device=dev)
+        self.ao = None          # (4, G, nao) AO tensor, only for the AO-input XC entry
         self.D, self.J, self.K, self.Vxc = z(nmat), z(nmat), z(nmat), z(nmat)
         self.H, self.diffJK = z(nmat), z(nmat)
         self.ring_err, self.ring_h = z(9 * nmat), z(9 * nmat)
@@ -218,6 +218,10 @@ class RKSEngine:
         self._eri_done = True
 
     def compute_ao(self, stream=None):
+        """Stored AO values + gradients (the reference's grid_AO tensor), for ``xc_from_ao``."""
+        if self.ao is None:
+            rdt = torch.float64 if self.prec == 64 else torch.float32
+            self.ao = torch.empty(max(1, self.plan.n_ao), dtype=rdt, device=self.device)
         check(lib().b2_ao_eval(self.plan.h, self.prec, ptr(self.coords), ptr(self.ao),
                                stream_handle(stream)), "b2_ao_eval")
         self._ao_done = True
@@ -228,6 +232,13 @@ class RKSEngine:
                              ptr(self.K), stream_handle(stream)), "b2_jk_s8")
 
     def xc(self, D=None, active=None, stream=None):
+        """E_xc and V_xc with AO values generated on the fly per grid tile."""
+        D = self.D if D is None else D
+        check(lib().b2_xc_direct(self.plan.h, self.prec, ptr(active), ptr(self.coords), ptr(self.weights),
+                                 ptr(D), ptr(self.Vxc), ptr(self.exc), stream_handle(stream)), "b2_xc_direct")
+
+    def xc_from_ao(self, D=None, active=None, stream=None):
+        """E_xc and V_xc from the stored AO tensor (compute_ao first)."""
         D = self.D if D is None else D
         check(lib().b2_xc(self.plan.h, self.prec, ptr(active), ptr(self.ao), ptr(self.weights), ptr(D),
                           ptr(self.Vxc), ptr(self.exc), stream_handle(stream)), "b2_xc")
@@ -254,8 +265,6 @@ class RKSEngine:
         self.device_setup()
         if not self._eri_done:
             self.compute_eri()
-        if not self._ao_done:
-            self.compute_ao()
 
     def initial(self):
         """D <- D0, then XC and J/K of D0 (nanoDFT.py:146-148)."""

@@ -33,6 +33,7 @@ static void b2_plan_free(B2PlanDev *P) {
   cudaFree(P->pp64); cudaFree(P->pp32); cudaFree(P->ao2sh); cudaFree(P->cls_list);
   cudaFree(P->cls_cnt); cudaFree(P->atom_xyz); cudaFree(P->atom_z); cudaFree(P->boys);
   cudaFree(P->jk_chunk_off);
+  cudaFree(P->eri_tasks32); cudaFree(P->eri_tasks64);
   delete P;
 }
 
@@ -155,6 +156,13 @@ int b2_xc(void *plan, int precision, const int *active, const void *ao, const do
   if (!plan || !ao || !weights || !D || !Vxc || !Exc) return B2_ERR_ARG;
   B2PlanDev *P = (B2PlanDev *)plan;
   return b2_launch_xc(*P, precision, active, ao, weights, D, Vxc, Exc, nullptr, (cudaStream_t)stream);
+}
+
+int b2_xc_direct(void *plan, int precision, const int *active, const double *coords,
+                 const double *weights, const double *D, double *Vxc, double *Exc, void *stream) {
+  if (!plan || !coords || !weights || !D || !Vxc || !Exc) return B2_ERR_ARG;
+  return b2_launch_xc_direct(*(B2PlanDev *)plan, precision, active, coords, weights, D, Vxc, Exc,
+                             (cudaStream_t)stream);
 }
 
 __global__ void k_b3lyp_points(long long n, const double *__restrict__ rho, double *exc,

@@ -2,6 +2,7 @@
 #pragma once
 #include "plan_host.hpp"
 #include "boys.cuh"
+#include "eri_sq.cuh"
 
 struct B2GridDev {             // grid layout registered with b2_grid_set
   long long n_points = 0, n_gblk = 0, n_xblk32 = 0, n_xblk64 = 0, n_ao = 0;
@@ -33,9 +34,11 @@ struct B2PlanDev {
   long long jk_nchunks = 0;
   int device = 0;
   B2GridDev g;
+  B2EriTask *eri_tasks32 = nullptr, *eri_tasks64 = nullptr;
+  std::vector<long long> eri_goff32, eri_goff64;   // task group (class combination) starts
 };
 
-int b2_launch_eri_s8(const B2PlanDev &P, int precision, void *out, cudaStream_t st);
+int b2_launch_eri_s8(B2PlanDev &P, int precision, void *out, cudaStream_t st);
 int b2_launch_jk_s8(const B2PlanDev &P, int precision, const int *active, const void *eri,
                     const double *D, double *J, double *K, cudaStream_t st);
 int b2_zero_active(const B2PlanDev &P, const int *active, double *A, double *B, cudaStream_t st);

@@ -3,6 +3,7 @@
 // the CPU test suite can check the kernel arithmetic against the oracle without a GPU.
 // It is never loaded by the product path (libb200dft.so has no CPU fallback).
 #include "eri_row.cuh"
+#include "eri_sq.cuh"
 #include "xc_math.cuh"
 #include <vector>
 
@@ -31,41 +32,35 @@ int b2hc_eri_s8(int nmol, const int *natm, const int *nbas, const int *atm, cons
   std::vector<double> tab(B2_BOYS_NT * B2_BOYS_NM);
   b2_boys_fill_table(tab.data());
   long long packed = 0;                     // output: molecules' s8 lists back to back
-  for (int m = 0; m < nmol; ++m) {
-    const B2MolDev &md = P.mols[m];
-    long long n2 = (long long)md.nao * (md.nao + 1) / 2;
-    double *om = out + packed;
-    packed += md.n4;
-    for (long long ij = 0; ij < n2; ++ij) {
-      B2RowInfo r = b2_row_info(md, ij, P.ao2sh.data(), P.pinfo.data());
-      int cnt[4];
-      for (int c = 0; c < 4; ++c) cnt[c] = P.cls_cnt[4ll * md.sp_off + (long long)c * md.nsp + r.spcut];
+  std::vector<long long> base(nmol);
+  for (int m = 0; m < nmol; ++m) { base[m] = packed; packed += P.mols[m].n4; }
+  std::vector<B2EriTask> tasks;
+  b2_eri_tasks(P, 128, precision == 64, tasks);
+  for (const B2EriTask &tk : tasks) {
+    const B2MolDev &md = P.mols[tk.mol];
+    const B2PairInfo &bp = P.pinfo[md.sp_off + tk.IJ];
+    double *om = out + base[tk.mol];
+    for (int t = 0; t < tk.count; ++t) {
+      const int KL = P.cls_list[md.sp_off + md.cls_start[tk.cls] + tk.start + t];
+      const B2PairInfo &kp = P.pinfo[md.sp_off + KL];
       if (precision == 64) {
-        B2BraPrim<double> bra[9];
+        B2PairPrim<double> bra[9];
         int nb = 0;
-        const B2PairPrim<double> *bp = &P.pp64[(size_t)(md.sp_off + r.sp) * B2_MAXPP];
-        for (int x = 0; x < 9; ++x) if (bp[x].K != 0) b2_make_bra_dispatch<double>(r.bcls, bp[x], r.ci, r.cj, bra[nb++]);
-        for (int c = 0; c < 4; ++c)
-          for (int e = 0; e < cnt[c]; ++e) {
-            int KL = P.cls_list[md.sp_off + md.cls_start[c] + e];
-            const B2PairInfo &kp = P.pinfo[md.sp_off + KL];
-            double acc[3][3];
-            b2_eri_dispatch<double>(r.bcls, c, bra, nb, &P.pp64[(size_t)(md.sp_off + KL) * 9], r.ci, r.cj, tab.data(), acc);
-            b2_eri_store<double, double>(om, ij, kp, kp.I == kp.J, acc);
-          }
+        for (int x = 0; x < 9; ++x) {
+          const B2PairPrim<double> &q = P.pp64[(size_t)(md.sp_off + tk.IJ) * 9 + x];
+          if (q.K != 0) bra[nb++] = q;
+        }
+        b2_sq_dispatch<double, double>(bp.lI + 2 * bp.lJ, tk.cls, tk.sub, bra, nb,
+                                       &P.pp64[(size_t)(md.sp_off + KL) * 9], tab.data(), om, bp, kp);
       } else {
-        B2BraPrim<float> bra[9];
+        B2PairPrim<float> bra[9];
         int nb = 0;
-        const B2PairPrim<float> *bp = &P.pp32[(size_t)(md.sp_off + r.sp) * B2_MAXPP];
-        for (int x = 0; x < 9; ++x) if (bp[x].K != 0) b2_make_bra_dispatch<float>(r.bcls, bp[x], r.ci, r.cj, bra[nb++]);
-        for (int c = 0; c < 4; ++c)
-          for (int e = 0; e < cnt[c]; ++e) {
-            int KL = P.cls_list[md.sp_off + md.cls_start[c] + e];
-            const B2PairInfo &kp = P.pinfo[md.sp_off + KL];
-            float acc[3][3];
-            b2_eri_dispatch<float>(r.bcls, c, bra, nb, &P.pp32[(size_t)(md.sp_off + KL) * 9], r.ci, r.cj, tab.data(), acc);
-            b2_eri_store<float, double>(om, ij, kp, kp.I == kp.J, acc);
-          }
+        for (int x = 0; x < 9; ++x) {
+          const B2PairPrim<float> &q = P.pp32[(size_t)(md.sp_off + tk.IJ) * 9 + x];
+          if (q.K != 0) bra[nb++] = q;
+        }
+        b2_sq_dispatch<float, double>(bp.lI + 2 * bp.lJ, tk.cls, tk.sub, bra, nb,
+                                      &P.pp32[(size_t)(md.sp_off + KL) * 9], tab.data(), om, bp, kp);
       }
     }
   }

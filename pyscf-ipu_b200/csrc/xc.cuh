@@ -6,3 +6,5 @@ int b2_launch_ao_eval(const B2PlanDev &P, int precision, const double *coords, v
 int b2_launch_xc(const B2PlanDev &P, int precision, const int *active, const void *ao,
                  const double *w, const double *D, double *V, double *exc, void *rt_scratch,
                  cudaStream_t st);
+int b2_launch_xc_direct(const B2PlanDev &P, int precision, const int *active, const double *coords,
+                        const double *w, const double *D, double *V, double *exc, cudaStream_t st);

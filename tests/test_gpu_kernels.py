@@ -112,12 +112,32 @@ def test_ao_eval_and_xc(cuda):
         a = ao[eng.plan.ao_off[mi]:eng.plan.ao_off[mi] + 4 * G * N].reshape(4, G, N)
         np.testing.assert_allclose(a, rks.ao_values(m, s.coords), atol=1e-12)
     eng.D.copy_(eng.D0)
+    for fn in (eng.xc_from_ao, eng.xc):          # stored-AO and on-the-fly-AO paths
+        eng.Vxc.zero_()
+        fn()
+        torch.cuda.synchronize()
+        for mi, (m, s) in enumerate(zip(mols, eng.setups)):
+            exc, V, _ = rks.exchange_correlation(s.D0, rks.ao_values(m, s.coords), s.weights)
+            assert abs(eng.exc[mi].item() - exc) < 1e-10
+            np.testing.assert_allclose(eng.plan.unpack(eng.Vxc.cpu().numpy(), mi), V, atol=1e-10)
+    eng.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_xc_direct_sizes(cuda, prec):
+    # molecules in every orbital bucket (nao 5..65) through the on-the-fly AO path
+    rng = np.random.default_rng(4)
+    mols = [Mole(random_molecule(rng, k)) for k in (1, 3, 5, 7, 9)]
+    setups = [HostSetup(m, 0) for m in mols]
+    eng = RKSEngine(mols, level=0, precision=prec, setups=setups)
+    eng.D.copy_(eng.D0)
     eng.xc()
     torch.cuda.synchronize()
-    for mi, (m, s) in enumerate(zip(mols, eng.setups)):
+    tol = 1e-9 if prec == "fp64" else 2e-5
+    for mi, (m, s) in enumerate(zip(mols, setups)):
         exc, V, _ = rks.exchange_correlation(s.D0, rks.ao_values(m, s.coords), s.weights)
-        assert abs(eng.exc[mi].item() - exc) < 1e-10
-        np.testing.assert_allclose(eng.plan.unpack(eng.Vxc.cpu().numpy(), mi), V, atol=1e-10)
+        assert abs(eng.exc[mi].item() - exc) < tol * max(1, abs(exc))
+        np.testing.assert_allclose(eng.plan.unpack(eng.Vxc.cpu().numpy(), mi), V, atol=tol * 10)
     eng.close()
 
 
