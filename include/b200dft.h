@@ -142,6 +142,17 @@ int b2_enuc(b2_plan_t plan, double *enuc, void *stream);
 int b2_int2e_sph_s8(const int *atm, int natm, const int *bas, int nbas, const double *env,
                     int n_env, int precision, void *eri_out, void *stream);
 
+/* Allocation-free variant of b2_int2e_sph_s8 (no counterpart in the reference).  For callers
+ * that cannot allocate device memory -- work being captured into a CUDA graph, processes whose
+ * device memory belongs to another allocator or a fixed-budget pool, loops that must not block
+ * in an allocator.  Its tables live in a 2.5 MiB static device array that every GPU loading the
+ * library keeps until exit.  Limits: nbas <= 48 shells, nao <= 70 (B2_ERR_SIZE beyond).  All
+ * calls share that array, so calls that overlap on the GPU (other streams, other host threads)
+ * race; calls on one stream are ordered.  The first call on a device must be made with that
+ * device current and, if graph capture is used, before capture begins. */
+int b2_int2e_sph_s8_noalloc(const int *atm, int natm, const int *bas, int nbas, const double *env,
+                            int n_env, int precision, void *eri_out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

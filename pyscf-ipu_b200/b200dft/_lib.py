@@ -40,6 +40,7 @@ SIGNATURES = {
     "b2_eigh_density": [_P, _P, _P, _P, _P, _P, _P, _P, _P],
     "b2_energy": [_P, _P, _P, _P, _P, _P, _P, _P, _P],
     "b2_int2e_sph_s8": [_P, _I, _P, _I, _P, _I, _I, _P, _P],
+    "b2_int2e_sph_s8_noalloc": [_P, _I, _P, _I, _P, _I, _I, _P, _P],
     "b2_int1e": [_P, _P, _P, _P, _P],
     "b2_grid_build": [_P, _I, _P, _P, _P, _P, _P],
     "b2_guess": [_P, _P, _P],

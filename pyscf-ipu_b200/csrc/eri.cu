@@ -82,3 +82,181 @@ int b2_launch_eri_s8(B2PlanDev &P, int precision, void *out, cudaStream_t st) {
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }
+
+// ============================================================================================
+// Allocation-free single-molecule ERI entry (b2_int2e_sph_s8_noalloc).
+//
+// For callers that cannot allocate device memory: code running while a CUDA stream is being
+// captured into a graph (allocation is not a capturable operation), processes whose device
+// memory is entirely owned by another allocator or memory pool with a fixed budget, and
+// latency-critical loops that must not block in the allocator.  The per-molecule tables the
+// ERI kernels read (molecule descriptor, shell-pair primitive data, class lists, work list,
+// Boys table) live in one file-scope __device__ array of B2_NOALLOC_BYTES (2.5 MiB) that every
+// GPU loading this library keeps until the process exits; host staging uses a static buffer of
+// the same size.  Limits: nbas <= 48 shells, nao <= 70, s/p shells with <= 3 primitives.
+// The s8 output is written completely, so no part of the array has to start at zero.  All calls
+// share the array: calls whose work overlaps on the GPU (different streams, or different host
+// threads) race; calls on one stream are ordered.  The first call on a device looks up the
+// array's device address (cudaGetSymbolAddress) with that device current.
+#define B2_NOALLOC_MAXBAS 48
+#define B2_NOALLOC_MAXSP (B2_NOALLOC_MAXBAS * (B2_NOALLOC_MAXBAS + 1) / 2)
+#define B2_NOALLOC_MAXTASK (B2_NOALLOC_MAXSP * 42)
+#define B2_NOALLOC_BYTES (2621440)
+
+static __device__ __align__(256) unsigned char g_b2_noalloc_scratch[B2_NOALLOC_BYTES];
+static __align__(256) unsigned char g_b2_noalloc_stage[B2_NOALLOC_BYTES];
+static unsigned char *g_b2_noalloc_dev[128];     // device address of the array, per device
+
+static size_t b2_na_align(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// class-group launch over a fixed-size group table (no container)
+template <typename T>
+static void b2_eri_all_na(const B2PlanDev &P, const B2EriTask *tasks, const long long *g,
+                          const B2PairPrim<T> *pp, T *out, cudaStream_t st) {
+#define B2_G(grp, LI, LJ, LK, LL)                                                            \
+  if (g[grp + 1] > g[grp])                                                                   \
+    b2_eri_group<T, LI, LJ, LK, LL>(P, tasks + g[grp], g[grp + 1] - g[grp], pp, out, st);
+  B2_G(0, 0, 0, 0, 0) B2_G(1, 0, 0, 1, 0) B2_G(2, 0, 0, 0, 1) B2_G(3, 0, 0, 1, 1)
+  B2_G(4, 1, 0, 0, 0) B2_G(5, 1, 0, 1, 0) B2_G(6, 1, 0, 0, 1) B2_G(7, 1, 0, 1, 1)
+  B2_G(8, 0, 1, 0, 0) B2_G(9, 0, 1, 1, 0) B2_G(10, 0, 1, 0, 1) B2_G(11, 0, 1, 1, 1)
+  B2_G(12, 1, 1, 0, 0) B2_G(13, 1, 1, 1, 0) B2_G(14, 1, 1, 0, 1) B2_G(15, 1, 1, 1, 1)
+#undef B2_G
+}
+
+extern "C" int b2_int2e_sph_s8_noalloc(const int *atm, int natm, const int *bas, int nbas,
+                                       const double *env, int n_env, int precision, void *eri_out,
+                                       void *stream) {
+  if (!atm || !bas || !env || !eri_out || natm <= 0 || nbas <= 0 || n_env <= 0) return B2_ERR_ARG;
+  if (precision != 64 && precision != 32) return B2_ERR_ARG;
+  if (nbas > B2_NOALLOC_MAXBAS) return B2_ERR_SIZE;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return B2_ERR_CUDA;
+  if (!g_b2_noalloc_dev[dev]) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_b2_noalloc_scratch) != cudaSuccess || !p) return B2_ERR_CUDA;
+    g_b2_noalloc_dev[dev] = (unsigned char *)p;
+  }
+  unsigned char *H = g_b2_noalloc_stage;
+  // ---- host tables in the static staging buffer (same layout as the device array) ----
+  const size_t o_mol = 0;
+  const size_t o_pi = b2_na_align(o_mol + sizeof(B2MolDev));
+  const size_t o_pp = b2_na_align(o_pi + sizeof(B2PairInfo) * B2_NOALLOC_MAXSP);
+  const size_t pp_bytes = (precision == 64 ? sizeof(B2PairPrim<double>) : sizeof(B2PairPrim<float>)) *
+                          B2_NOALLOC_MAXSP * B2_MAXPP;
+  const size_t o_cls = b2_na_align(o_pp + pp_bytes);
+  const size_t o_task = b2_na_align(o_cls + sizeof(int) * B2_NOALLOC_MAXSP);
+  const size_t o_boys = b2_na_align(o_task + sizeof(B2EriTask) * B2_NOALLOC_MAXTASK);
+  const size_t total = b2_na_align(o_boys + sizeof(double) * B2_BOYS_NT * B2_BOYS_NM);
+  if (total > B2_NOALLOC_BYTES) return B2_ERR_SIZE;
+  B2Shell S[B2_NOALLOC_MAXBAS];
+  int nao = 0;
+  for (int s = 0; s < nbas; ++s) {
+    const int *b = bas + s * B2_BAS_SLOTS;
+    const int l = b[B2_ANG_OF], np = b[B2_NPRIM_OF], ia = b[B2_ATOM_OF];
+    if (l > B2_MAXL || np < 1 || np > B2_MAXPRIM || b[B2_NCTR_OF] != 1) return B2_ERR_UNSUPPORTED;
+    if (ia < 0 || ia >= natm) return B2_ERR_ARG;
+    const int pc = atm[ia * B2_ATM_SLOTS + B2_PTR_COORD];
+    if (pc < 0 || pc + 3 > n_env || b[B2_PTR_EXP] + np > n_env || b[B2_PTR_COEFF] + np > n_env)
+      return B2_ERR_ARG;
+    memset(&S[s], 0, sizeof(B2Shell));
+    for (int d = 0; d < 3; ++d) S[s].R[d] = env[pc + d];
+    const double fac = l == 0 ? B2_FAC_S : B2_FAC_P;
+    for (int k = 0; k < np; ++k) {
+      S[s].exp[k] = env[b[B2_PTR_EXP] + k];
+      S[s].coef[k] = env[b[B2_PTR_COEFF] + k] * fac;
+    }
+    S[s].l = l; S[s].ao0 = nao; S[s].nprim = np; S[s].atom = ia;
+    nao += 2 * l + 1;
+  }
+  if (nao > B2_MAXNAO - 2) return B2_ERR_SIZE;
+  const int nsp = nbas * (nbas + 1) / 2;
+  B2MolDev *md = (B2MolDev *)(H + o_mol);
+  memset(md, 0, sizeof(B2MolDev));
+  md->nao = nao; md->nbas = nbas; md->natm = natm; md->nsp = nsp;
+  const long long n2 = (long long)nao * (nao + 1) / 2;
+  md->n4 = n2 * (n2 + 1) / 2;
+  B2PairInfo *PI = (B2PairInfo *)(H + o_pi);
+  static int cls[B2_NOALLOC_MAXSP];
+  const double k0 = sqrt(2.0) * pow(M_PI, 1.25);
+  for (int I = 0; I < nbas; ++I)
+    for (int J = 0; J <= I; ++J) {
+      const int sp = (int)b2_tri(I) + J;
+      const B2Shell &a = S[I], &b = S[J];
+      PI[sp] = B2PairInfo{I, J, a.l, b.l, a.ao0, b.ao0, a.nprim * b.nprim, 0};
+      cls[sp] = a.l + 2 * b.l;
+      double AB2 = 0;
+      for (int d = 0; d < 3; ++d) AB2 += (a.R[d] - b.R[d]) * (a.R[d] - b.R[d]);
+      for (int x = 0; x < B2_MAXPP; ++x) {
+        B2PairPrim<double> q;
+        memset(&q, 0, sizeof(q));
+        q.zeta = 1.0;
+        const int pa = x / B2_MAXPRIM, pb = x % B2_MAXPRIM;
+        if (pa < a.nprim && pb < b.nprim) {
+          const double al = a.exp[pa], be = b.exp[pb], z = al + be;
+          double Pc[3];
+          for (int d = 0; d < 3; ++d) Pc[d] = (al * a.R[d] + be * b.R[d]) / z;
+          double K = a.coef[pa] * b.coef[pb] * exp(-al * be / z * AB2) * k0 / z;
+          if (fabs(K) < 1e-300) K = 0;
+          q.zeta = z; q.Px = Pc[0]; q.Py = Pc[1]; q.Pz = Pc[2]; q.K = K;
+          q.PAx = Pc[0] - a.R[0]; q.PAy = Pc[1] - a.R[1]; q.PAz = Pc[2] - a.R[2];
+          q.PBx = Pc[0] - b.R[0]; q.PBy = Pc[1] - b.R[1]; q.PBz = Pc[2] - b.R[2];
+        }
+        if (precision == 64) {
+          ((B2PairPrim<double> *)(H + o_pp))[(size_t)sp * B2_MAXPP + x] = q;
+        } else {
+          B2PairPrim<float> f;
+          f.zeta = (float)q.zeta; f.Px = (float)q.Px; f.Py = (float)q.Py; f.Pz = (float)q.Pz;
+          f.K = (float)q.K; f.PAx = (float)q.PAx; f.PAy = (float)q.PAy; f.PAz = (float)q.PAz;
+          f.PBx = (float)q.PBx; f.PBy = (float)q.PBy; f.PBz = (float)q.PBz; f.pad = 0.f;
+          ((B2PairPrim<float> *)(H + o_pp))[(size_t)sp * B2_MAXPP + x] = f;
+        }
+      }
+    }
+  int *CL = (int *)(H + o_cls);
+  int start = 0;
+  for (int c = 0; c < 4; ++c) {
+    md->cls_start[c] = start;
+    for (int sp = 0; sp < nsp; ++sp)
+      if (cls[sp] == c) CL[start++] = sp;
+  }
+  md->cls_start[4] = start;
+  // work list grouped by class combination, kets in chunks of 128 (as b2_eri_tasks)
+  B2EriTask *TK = (B2EriTask *)(H + o_task);
+  long long goff[17];
+  long long nt = 0;
+  for (int grp = 0; grp < 16; ++grp) {
+    goff[grp] = nt;
+    const int bc = grp / 4, c = grp % 4;
+    for (int IJ = 0; IJ < nsp; ++IJ) {
+      if (PI[IJ].lI + 2 * PI[IJ].lJ != bc) continue;
+      const int spcut = (int)b2_tri(PI[IJ].I) + PI[IJ].I;
+      int cnt = 0;                                      // class-c members KL <= spcut
+      for (int e = md->cls_start[c]; e < md->cls_start[c + 1]; ++e) cnt += (CL[e] <= spcut);
+      const int nsub = (precision == 64 && PI[IJ].lI) ? 3 : 1;
+      for (int s0 = 0; s0 < cnt; s0 += 128)
+        for (int sub = 0; sub < nsub; ++sub) {
+          if (nt >= B2_NOALLOC_MAXTASK) return B2_ERR_SIZE;
+          TK[nt++] = B2EriTask{0, IJ, c, s0, cnt - s0 < 128 ? cnt - s0 : 128, nsub > 1 ? sub : -1};
+        }
+    }
+  }
+  goff[16] = nt;
+  b2_boys_fill_table((double *)(H + o_boys));
+  // ---- stage to the device array and launch (no device allocation anywhere) ----
+  unsigned char *Dv = g_b2_noalloc_dev[dev];
+  cudaStream_t st = (cudaStream_t)stream;
+  if (cudaMemcpyAsync(Dv, H, total, cudaMemcpyHostToDevice, st) != cudaSuccess) return B2_ERR_CUDA;
+  B2PlanDev P;                                           // view onto the static array
+  P.mols = (B2MolDev *)(Dv + o_mol);
+  P.pinfo = (B2PairInfo *)(Dv + o_pi);
+  P.cls_list = (int *)(Dv + o_cls);
+  P.boys = (double *)(Dv + o_boys);
+  B2EriTask *tasks = (B2EriTask *)(Dv + o_task);
+  if (precision == 64)
+    b2_eri_all_na<double>(P, tasks, goff, (const B2PairPrim<double> *)(Dv + o_pp), (double *)eri_out, st);
+  else
+    b2_eri_all_na<float>(P, tasks, goff, (const B2PairPrim<float> *)(Dv + o_pp), (float *)eri_out, st);
+  P.mols = nullptr; P.pinfo = nullptr; P.cls_list = nullptr; P.boys = nullptr;
+  if (cudaGetLastError() != cudaSuccess) return B2_ERR_CUDA;
+  return B2_OK;
+}
