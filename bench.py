@@ -166,6 +166,7 @@ def main():
     ap.add_argument("--plain-sample", type=int, default=32)
     ap.add_argument("--cpu-sample", type=int, default=8)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile-mode", action="store_true", help="timed steps only (for ncu captures)")
     a = ap.parse_args()
     if a.impl == "reference":
         return run_reference(a)
@@ -173,6 +174,7 @@ def main():
     import torch
     import torch.distributed as dist
     from b200dft.engine import RKSEngine, Plan
+    from b200dft._lib import launch_count
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -230,6 +232,9 @@ def main():
     t_start = torch.cuda.Event(enable_timing=True)
     t_end = torch.cuda.Event(enable_timing=True)
     barrier()
+    eng.graph_replays = 0
+    eng._captured = 0
+    lc0 = launch_count()
     t_start.record()
     its_total = 0
     for _ in range(a.steps):
@@ -241,6 +246,7 @@ def main():
     t_end.record()
     barrier()
     clocks = clk.stop()
+    gpu_launches = eng.kernels_launched(lc0)
     ms = max_over_ranks(t_start.elapsed_time(t_end)) / a.steps
     value = world * a.nmol / (ms / 1000.0)
     conv = res["converged"].cpu().numpy()
@@ -268,9 +274,12 @@ def main():
                 "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
                 "algorithmic_bytes_per_launch": jk_bytes, "ms_per_launch": jk_ms}
 
+    if a.profile_mode:
+        a.plain_sample = 0
+        a.no_cpu = True
     # e2e: public API from host buffers (plan creation = H2D of the libcint tables), results D2H
     e2e = None
-    if rank == 0:
+    if rank == 0 and not a.profile_mode:
         barrier()
         t0 = time.perf_counter()
         e2 = RKSEngine(mols, level=a.level, precision=a.precision)
@@ -321,7 +330,7 @@ def main():
                        "l2": "inputs (s8 ERIs, AO values) larger than L2 between iterations",
                        "convergence": "|dE|<1e-6 Ha and DIIS err<1e-4, retire converged"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-            "gpu_launches": None,
+            "gpu_launches": gpu_launches,
             "phases_ms_per_step": {k: v / a.steps for k, v in phase.items()},
             "scf": {"converged": int(conv.sum()), "of": int(len(conv)), "mean_its": float(iters[conv].mean()) if conv.any() else None,
                     "p50_its": float(np.percentile(iters[conv], 50)) if conv.any() else None,

@@ -35,6 +35,10 @@ typedef void *b2_plan_t;
 /* Library/ABI version (major*10000 + minor*100 + patch). */
 int b2_version(void);
 
+/* Number of kernels the library has launched in this process (monotonic counter; kernels
+ * replayed from a captured CUDA graph are not counted again). */
+int b2_launch_count(int64_t *out);
+
 /* Last CUDA error string seen by the library (for diagnostics). */
 const char *b2_last_error(void);
 
@@ -110,9 +114,12 @@ int b2_fock_diis(b2_plan_t plan, const int *active, const int *iter, double hyb,
                  double *ring_h, double *bmat, double *diis_err, void *stream);
 
 /* C = L^T eigvec(L H L^T), D = 2 C_occ C_occ^T (nanoDFT.py:68-72).  mo_energy: device float64
- * nmol x 72 (ascending, first nao valid); C may be NULL; sweeps (device int[nmol]) may be NULL. */
-int b2_eigh_density(b2_plan_t plan, const int *active, const double *H, const double *Linv,
-                    double *D, double *mo_energy, double *C, int *sweeps, void *stream);
+ * nmol x 72 (ascending, first nao valid); C may be NULL; sweeps (device int[nmol]) may be NULL.
+ * ws (device float64 n_mat, may be NULL): eigenvector basis kept between calls; with iter[m] > 0
+ * the solve starts from it (warm start), with iter NULL or iter[m] == 0 it starts cold. */
+int b2_eigh_density(b2_plan_t plan, const int *active, const int *iter, const double *H,
+                    const double *Linv, double *D, double *mo_energy, double *C, double *ws,
+                    int *sweeps, void *stream);
 
 /* energies (device float64 nmol x 5): [E, E_core, E_J_K/2, E_xc, E_nuc] (nanoDFT.py:20-38) */
 int b2_energy(b2_plan_t plan, const int *active, const double *D, const double *Hcore,

@@ -21,6 +21,7 @@ _D = ctypes.c_double
 # name -> argtypes (all return int status)
 SIGNATURES = {
     "b2_version": [],
+    "b2_launch_count": [_P],
     "b2_plan_create": [_I, _P, _P, _P, _P, _P, _P, _P],
     "b2_plan_destroy": [_P],
     "b2_plan_info": [_P, _P],
@@ -37,7 +38,7 @@ SIGNATURES = {
     "b2_b3lyp": [_L, _P, _P, _P, _P, _P],
     "b2_chol_inv": [_P, _P, _P, _P, _P],
     "b2_fock_diis": [_P, _P, _P, _D, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
-    "b2_eigh_density": [_P, _P, _P, _P, _P, _P, _P, _P, _P],
+    "b2_eigh_density": [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "b2_energy": [_P, _P, _P, _P, _P, _P, _P, _P, _P],
     "b2_int2e_sph_s8": [_P, _I, _P, _I, _P, _I, _I, _P, _P],
     "b2_int2e_sph_s8_noalloc": [_P, _I, _P, _I, _P, _I, _I, _P, _P],
@@ -81,6 +82,13 @@ def check(rc, what):
             pass
         raise B200DFTError(f"{what} failed: {ERRORS.get(rc, rc)} {detail}".strip())
     return rc
+
+
+def launch_count():
+    """kernels launched by libb200dft.so so far in this process"""
+    v = ctypes.c_int64()
+    check(lib().b2_launch_count(ctypes.byref(v)), "b2_launch_count")
+    return v.value
 
 
 def ptr(t):

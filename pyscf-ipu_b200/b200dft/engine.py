@@ -14,7 +14,7 @@ import ctypes
 import numpy as np
 import torch
 
-from ._lib import lib, check, ptr, stream_handle, B200DFTError
+from ._lib import lib, check, ptr, stream_handle, B200DFTError, launch_count
 from .constants import HYB_B3LYP
 from .grids import Grids, atomic_grid
 from .guess import minao
@@ -189,12 +189,16 @@ class RKSEngine:
         self.energy = z(5 * nm)
         self.mo_energy = z(NMO * nm)
         self.C = z(nmat)
+        self.eig_ws = z(nmat)          # eigenvector basis carried between iterations (warm start)
         self.iter = torch.zeros(nm, dtype=torch.int32, device=dev)
         self.active = torch.ones(nm, dtype=torch.int32, device=dev)
         self.sweeps = torch.zeros(nm, dtype=torch.int32, device=dev)
         self._eri_done = False
         self._ao_done = False
         self._graph = None
+        self.graph_replays = 0              # kernels replayed from graphs are not in launch_count()
+        self._captured = 0
+        self.graph_kernels_per_step = 0
 
     # --- setup -------------------------------------------------------------------------
     def device_setup(self, stream=None):
@@ -251,9 +255,9 @@ class RKSEngine:
                                  stream_handle(stream)), "b2_fock_diis")
 
     def eigh_density(self, stream=None):
-        check(lib().b2_eigh_density(self.plan.h, ptr(self.active), ptr(self.H), ptr(self.Linv), ptr(self.D),
-                                    ptr(self.mo_energy), ptr(self.C), ptr(self.sweeps),
-                                    stream_handle(stream)), "b2_eigh_density")
+        check(lib().b2_eigh_density(self.plan.h, ptr(self.active), ptr(self.iter), ptr(self.H), ptr(self.Linv),
+                                    ptr(self.D), ptr(self.mo_energy), ptr(self.C), ptr(self.eig_ws),
+                                    ptr(self.sweeps), stream_handle(stream)), "b2_eigh_density")
 
     def energies(self, stream=None):
         check(lib().b2_energy(self.plan.h, ptr(self.active), ptr(self.D), ptr(self.Hcore), ptr(self.diffJK),
@@ -332,14 +336,18 @@ class RKSEngine:
             st = torch.cuda.Stream()
             st.wait_stream(torch.cuda.current_stream())
             g = torch.cuda.CUDAGraph()
+            c0 = launch_count()
             with torch.cuda.stream(st):
                 with torch.cuda.graph(g, stream=st):
                     self.step(use_diis)
             torch.cuda.current_stream().wait_stream(st)
+            self.graph_kernels_per_step = launch_count() - c0
+            self._captured += self.graph_kernels_per_step
             # the capture did not execute the step: state is unchanged
         for i in range(max_its):
             if g is not None:
                 g.replay()
+                self.graph_replays += 1
             else:
                 self.step(use_diis)
             e = self.energy.view(nm, 5)[:, 0]
@@ -352,6 +360,11 @@ class RKSEngine:
         E = self.energy.view(nm, 5)[:, 0].clone()
         return dict(energy=E, iterations=conv_it, converged=conv_it > 0, mo_energy=self.mo_energy.view(nm, NMO),
                     diis_err=self.diis_err.clone(), its_run=i + 1)
+
+    def kernels_launched(self, since):
+        """library kernels executed since the launch_count() value ``since`` (graph replays included;
+        the capture itself launches nothing)"""
+        return launch_count() - since - self._captured + self.graph_replays * self.graph_kernels_per_step
 
     def close(self):
         self.plan.close()

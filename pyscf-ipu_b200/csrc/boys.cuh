@@ -39,13 +39,13 @@ template <typename T> struct B2BoysTerms;
 template <> struct B2BoysTerms<double> { static constexpr int n = 9; };
 template <> struct B2BoysTerms<float> { static constexpr int n = 6; };
 
-// F[0..L] at T; `table` is the double table (device global or host memory).
-template <typename T, int L>
-B2_HD void b2_boys(T t, const double *__restrict__ table, T *F) {
+// F[0..L] at T; `table` is the table in double (float64 kernels) or float (float32 kernels).
+template <typename T, int L, typename TT>
+B2_HD void b2_boys(T t, const TT *__restrict__ table, T *F) {
   if (t < (T)B2_BOYS_TMAX) {
     int k = (int)(t * (T)B2_BOYS_INV_DT + (T)0.5);
     T dt = (T)(k * B2_BOYS_DT) - t;           // T_k - T
-    const double *row = table + k * B2_BOYS_NM + L;
+    const TT *row = table + k * B2_BOYS_NM + L;
     constexpr int NT = B2BoysTerms<T>::n;
     // Horner: sum_j F_{L+j}(T_k) dt^j / j!
     T acc = (T)row[NT - 1];
@@ -65,3 +65,11 @@ B2_HD void b2_boys(T t, const double *__restrict__ table, T *F) {
     for (int m = 0; m < L; ++m) F[m + 1] = (T)(2 * m + 1) * (T)0.5 * inv * F[m];
   }
 }
+
+// reciprocal / inverse square root: exact for float64, fast hardware forms for float32
+template <typename T> B2_HD T b2_div(T a, T b) { return a / b; }
+template <typename T> B2_HD T b2_rsqrt(T x) { return (T)1 / sqrt(x); }
+#ifdef __CUDA_ARCH__
+template <> __device__ __forceinline__ float b2_div<float>(float a, float b) { return __fdividef(a, b); }
+template <> __device__ __forceinline__ float b2_rsqrt<float>(float x) { return rsqrtf(x); }
+#endif

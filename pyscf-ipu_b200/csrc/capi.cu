@@ -10,6 +10,9 @@
 #include "setup.cuh"
 
 static thread_local std::string g_last_error;
+#include <atomic>
+static std::atomic<long long> g_b2_launches{0};
+void b2_count_launches(long long n) { g_b2_launches += n; }
 
 static int b2_note(cudaError_t e) {
   if (e != cudaSuccess) { g_last_error = cudaGetErrorString(e); return B2_ERR_CUDA; }
@@ -31,7 +34,7 @@ static void b2_plan_free(B2PlanDev *P) {
   b2_grid_free(*P);
   cudaFree(P->mols); cudaFree(P->row_off); cudaFree(P->shells); cudaFree(P->pinfo);
   cudaFree(P->pp64); cudaFree(P->pp32); cudaFree(P->ao2sh); cudaFree(P->cls_list);
-  cudaFree(P->cls_cnt); cudaFree(P->atom_xyz); cudaFree(P->atom_z); cudaFree(P->boys);
+  cudaFree(P->cls_cnt); cudaFree(P->atom_xyz); cudaFree(P->atom_z); cudaFree(P->boys); cudaFree(P->boys32);
   cudaFree(P->jk_chunk_off);
   cudaFree(P->eri_tasks32); cudaFree(P->eri_tasks64);
   delete P;
@@ -56,6 +59,12 @@ extern "C" {
 
 int b2_version(void) { return 100; }
 
+int b2_launch_count(int64_t *out) {
+  if (!out) return B2_ERR_ARG;
+  *out = g_b2_launches.load();
+  return B2_OK;
+}
+
 const char *b2_last_error(void) { return g_last_error.c_str(); }
 
 int b2_plan_create(int nmol, const int *natm, const int *nbas, const int *atm, const int *bas,
@@ -73,6 +82,7 @@ int b2_plan_create(int nmol, const int *natm, const int *nbas, const int *atm, c
       (rc = b2_upload(&P->ao2sh, P->h.ao2sh)) || (rc = b2_upload(&P->cls_list, P->h.cls_list)) ||
       (rc = b2_upload(&P->cls_cnt, P->h.cls_cnt)) || (rc = b2_upload(&P->atom_xyz, P->h.atom_xyz)) ||
       (rc = b2_upload(&P->atom_z, P->h.atom_z)) || (rc = b2_upload(&P->boys, tab)) ||
+      (rc = b2_upload(&P->boys32, std::vector<float>(tab.begin(), tab.end()))) ||
       (rc = b2_set_jk_chunk(P, 0))) {
     b2_plan_free(P);
     return rc;
@@ -177,6 +187,7 @@ int b2_b3lyp(int64_t n, const double *rho, double *exc, double *vrho, double *vg
   if (n < 0 || (n > 0 && (!rho || !exc || !vrho || !vgamma))) return B2_ERR_ARG;
   if (n == 0) return B2_OK;
   k_b3lyp_points<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(n, rho, exc, vrho, vgamma);
+  b2_count_launches(1);
   B2_TRY(cudaGetLastError());
   return B2_OK;
 }
@@ -196,11 +207,12 @@ int b2_fock_diis(void *plan, const int *active, const int *iter, double hyb, int
                              Vxc, H, diffJK, ring_err, ring_h, bmat, diis_err, (cudaStream_t)stream);
 }
 
-int b2_eigh_density(void *plan, const int *active, const double *H, const double *Linv, double *D,
-                    double *mo_energy, double *C, int *sweeps, void *stream) {
+int b2_eigh_density(void *plan, const int *active, const int *iter, const double *H,
+                    const double *Linv, double *D, double *mo_energy, double *C, double *ws,
+                    int *sweeps, void *stream) {
   if (!plan || !H || !Linv || !D || !mo_energy) return B2_ERR_ARG;
-  return b2_launch_eigh_density(*(B2PlanDev *)plan, active, H, Linv, D, mo_energy, C, sweeps,
-                                (cudaStream_t)stream);
+  return b2_launch_eigh_density(*(B2PlanDev *)plan, active, iter, H, Linv, D, mo_energy, C, ws,
+                                sweeps, (cudaStream_t)stream);
 }
 
 int b2_energy(void *plan, const int *active, const double *D, const double *Hcore,

@@ -4,6 +4,9 @@
 #include "boys.cuh"
 #include "eri_sq.cuh"
 
+// number of kernels this library has launched (monotonic; read with b2_launch_count)
+void b2_count_launches(long long n);
+
 struct B2GridDev {             // grid layout registered with b2_grid_set
   long long n_points = 0, n_gblk = 0, n_xblk32 = 0, n_xblk64 = 0, n_ao = 0;
   long long *grid_off = nullptr, *gblk_off = nullptr, *ao_off = nullptr;
@@ -29,6 +32,7 @@ struct B2PlanDev {
   double *atom_xyz = nullptr;
   int *atom_z = nullptr;
   double *boys = nullptr;
+  float *boys32 = nullptr;                // float copy for the float32 kernels
   long long *jk_chunk_off = nullptr;      // nmol + 1 (J/K work split)
   long long jk_chunk = 0;
   long long jk_nchunks = 0;

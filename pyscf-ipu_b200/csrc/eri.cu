@@ -16,7 +16,7 @@ template <typename T, int LI, int LJ, int LK, int LL>
 __global__ void __launch_bounds__(128)
 k_eri_sq(const B2EriTask *__restrict__ tasks, const B2MolDev *__restrict__ mols,
          const B2PairInfo *__restrict__ pinfo, const B2PairPrim<T> *__restrict__ pp,
-         const int *__restrict__ cls_list, const double *__restrict__ btab, T *__restrict__ out) {
+         const int *__restrict__ cls_list, const T *__restrict__ btab, T *__restrict__ out) {
   __shared__ B2PairPrim<T> sbra[B2_MAXPP];
   __shared__ int s_nb;
   const B2EriTask tk = tasks[blockIdx.x];
@@ -37,13 +37,19 @@ k_eri_sq(const B2EriTask *__restrict__ tasks, const B2MolDev *__restrict__ mols,
                                   btab, out + md.eri_off, bp, kp);
 }
 
+template <typename T> static const T *b2_boys_table(const B2PlanDev &P);
+template <> const double *b2_boys_table<double>(const B2PlanDev &P) { return P.boys; }
+template <> const float *b2_boys_table<float>(const B2PlanDev &P) { return P.boys32; }
+
 template <typename T, int LI, int LJ, int LK, int LL>
 static void b2_eri_group(const B2PlanDev &P, const B2EriTask *tasks, long long n,
                          const B2PairPrim<T> *pp, T *out, cudaStream_t st) {
   const long long maxg = (1ll << 31) - 1;
-  for (long long t0 = 0; t0 < n; t0 += maxg)
+  for (long long t0 = 0; t0 < n; t0 += maxg) {
     k_eri_sq<T, LI, LJ, LK, LL><<<(unsigned)std::min(maxg, n - t0), 128, 0, st>>>(
-        tasks + t0, P.mols, P.pinfo, pp, P.cls_list, P.boys, out);
+        tasks + t0, P.mols, P.pinfo, pp, P.cls_list, b2_boys_table<T>(P), out);
+    b2_count_launches(1);
+  }
 }
 
 template <typename T>
@@ -242,6 +248,11 @@ extern "C" int b2_int2e_sph_s8_noalloc(const int *atm, int natm, const int *bas,
   }
   goff[16] = nt;
   b2_boys_fill_table((double *)(H + o_boys));
+  if (precision == 32) {                          // float32 kernels read a float table
+    const double *bd = (const double *)(H + o_boys);
+    float *bf = (float *)(H + o_boys);
+    for (int i = 0; i < B2_BOYS_NT * B2_BOYS_NM; ++i) bf[i] = (float)bd[i];   // in place, ascending
+  }
   // ---- stage to the device array and launch (no device allocation anywhere) ----
   unsigned char *Dv = g_b2_noalloc_dev[dev];
   cudaStream_t st = (cudaStream_t)stream;
@@ -251,12 +262,13 @@ extern "C" int b2_int2e_sph_s8_noalloc(const int *atm, int natm, const int *bas,
   P.pinfo = (B2PairInfo *)(Dv + o_pi);
   P.cls_list = (int *)(Dv + o_cls);
   P.boys = (double *)(Dv + o_boys);
+  P.boys32 = (float *)(Dv + o_boys);
   B2EriTask *tasks = (B2EriTask *)(Dv + o_task);
   if (precision == 64)
     b2_eri_all_na<double>(P, tasks, goff, (const B2PairPrim<double> *)(Dv + o_pp), (double *)eri_out, st);
   else
     b2_eri_all_na<float>(P, tasks, goff, (const B2PairPrim<float> *)(Dv + o_pp), (float *)eri_out, st);
-  P.mols = nullptr; P.pinfo = nullptr; P.cls_list = nullptr; P.boys = nullptr;
+  P.mols = nullptr; P.pinfo = nullptr; P.cls_list = nullptr; P.boys = nullptr; P.boys32 = nullptr;
   if (cudaGetLastError() != cudaSuccess) return B2_ERR_CUDA;
   return B2_OK;
 }

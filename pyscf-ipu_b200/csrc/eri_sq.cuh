@@ -16,7 +16,7 @@ struct B2Sq {
   static constexpr int L = LI + LJ + LK + LL;
 
   B2_HD static void eval(const B2PairPrim<T> *__restrict__ bra, int nb,
-                         const B2PairPrim<T> *__restrict__ ket, const double *__restrict__ btab,
+                         const B2PairPrim<T> *__restrict__ ket, const T *__restrict__ btab,
                          T acc[NI][NJ][NK][NL]) {
 #pragma unroll
     for (int a = 0; a < NI; ++a)
@@ -30,20 +30,20 @@ struct B2Sq {
       const B2PairPrim<T> Q = ket[q];
       if (Q.K == (T)0) continue;
       const T eta = Q.zeta;
-      const T v = (T)0.5 / eta;
+      const T v = b2_div<T>((T)0.5, eta);
       const T QC[3] = {Q.PAx, Q.PAy, Q.PAz};
       const T QD[3] = {Q.PBx, Q.PBy, Q.PBz};
       for (int p = 0; p < nb; ++p) {
         const B2PairPrim<T> &Bp = bra[p];
         const T zeta = Bp.zeta;
-        const T u = (T)0.5 / zeta;
+        const T u = b2_div<T>((T)0.5, zeta);
         const T sig = zeta + eta;
-        const T rho = zeta * eta / sig;
+        const T rho = b2_div<T>(zeta * eta, sig);
         const T X[3] = {Bp.Px - Q.Px, Bp.Py - Q.Py, Bp.Pz - Q.Pz};
         const T tt = rho * (X[0] * X[0] + X[1] * X[1] + X[2] * X[2]);
-        const T pref = Bp.K * Q.K / sqrt(sig);
+        const T pref = Bp.K * Q.K * b2_rsqrt<T>(sig);
         T F[L + 1];
-        b2_boys<T, L>(tt, btab, F);
+        b2_boys<T, L, T>(tt, btab, F);
         T f[L + 3];
         {
           T m2r = (T)-2 * rho, s = pref;
@@ -146,7 +146,7 @@ struct B2Sq {
 
   template <typename TO>
   B2_HD static void run(const B2PairPrim<T> *bra, int nb, const B2PairPrim<T> *ket,
-                        const double *btab, TO *out, const B2PairInfo &bp, const B2PairInfo &kp) {
+                        const T *btab, TO *out, const B2PairInfo &bp, const B2PairInfo &kp) {
     T acc[NI][NJ][NK][NL];
     eval(bra, nb, ket, btab, acc);
     store<TO>(out, bp, kp, acc);
@@ -196,7 +196,7 @@ static void b2_eri_tasks(const B2PlanHost &P, int chunk, bool split_p, std::vect
 // dispatch on (bra class, ket class, sub) to the specialised evaluator
 template <typename T, int LI, int LJ, int LK, int LL, typename TO>
 B2_HD void b2_sq_sub(int sub, const B2PairPrim<T> *bra, int nb, const B2PairPrim<T> *ket,
-                     const double *btab, TO *out, const B2PairInfo &bp, const B2PairInfo &kp) {
+                     const T *btab, TO *out, const B2PairInfo &bp, const B2PairInfo &kp) {
   if (LI && sub >= 0) {
     switch (sub) {
       case 0: B2Sq<T, LI, LJ, LK, LL, 0>::template run<TO>(bra, nb, ket, btab, out, bp, kp); break;
@@ -210,7 +210,7 @@ B2_HD void b2_sq_sub(int sub, const B2PairPrim<T> *bra, int nb, const B2PairPrim
 
 template <typename T, int LI, int LJ, typename TO>
 B2_HD void b2_sq_ket(int cls, int sub, const B2PairPrim<T> *bra, int nb, const B2PairPrim<T> *ket,
-                     const double *btab, TO *out, const B2PairInfo &bp, const B2PairInfo &kp) {
+                     const T *btab, TO *out, const B2PairInfo &bp, const B2PairInfo &kp) {
   switch (cls) {
     case 0: b2_sq_sub<T, LI, LJ, 0, 0, TO>(sub, bra, nb, ket, btab, out, bp, kp); break;
     case 1: b2_sq_sub<T, LI, LJ, 1, 0, TO>(sub, bra, nb, ket, btab, out, bp, kp); break;
@@ -221,7 +221,7 @@ B2_HD void b2_sq_ket(int cls, int sub, const B2PairPrim<T> *bra, int nb, const B
 
 template <typename T, typename TO>
 B2_HD void b2_sq_dispatch(int bcls, int cls, int sub, const B2PairPrim<T> *bra, int nb,
-                          const B2PairPrim<T> *ket, const double *btab, TO *out,
+                          const B2PairPrim<T> *ket, const T *btab, TO *out,
                           const B2PairInfo &bp, const B2PairInfo &kp) {
   switch (bcls) {
     case 0: b2_sq_ket<T, 0, 0, TO>(cls, sub, bra, nb, ket, btab, out, bp, kp); break;

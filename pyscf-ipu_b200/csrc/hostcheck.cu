@@ -34,6 +34,7 @@ int b2hc_eri_s8(int nmol, const int *natm, const int *nbas, const int *atm, cons
   long long packed = 0;                     // output: molecules' s8 lists back to back
   std::vector<long long> base(nmol);
   for (int m = 0; m < nmol; ++m) { base[m] = packed; packed += P.mols[m].n4; }
+  std::vector<float> tab32(tab.begin(), tab.end());
   std::vector<B2EriTask> tasks;
   b2_eri_tasks(P, 128, precision == 64, tasks);
   for (const B2EriTask &tk : tasks) {
@@ -60,7 +61,7 @@ int b2hc_eri_s8(int nmol, const int *natm, const int *nbas, const int *atm, cons
           if (q.K != 0) bra[nb++] = q;
         }
         b2_sq_dispatch<float, double>(bp.lI + 2 * bp.lJ, tk.cls, tk.sub, bra, nb,
-                                      &P.pp32[(size_t)(md.sp_off + KL) * 9], tab.data(), om, bp, kp);
+                                      &P.pp32[(size_t)(md.sp_off + KL) * 9], tab32.data(), om, bp, kp);
       }
     }
   }

@@ -143,6 +143,7 @@ __global__ void k_zero_active(const B2MolDev *__restrict__ mols, const int *__re
 
 int b2_zero_active(const B2PlanDev &P, const int *active, double *A, double *B, cudaStream_t st) {
   k_zero_active<<<P.h.nmol, 256, 0, st>>>(P.mols, active, A, B);
+  b2_count_launches(1);
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }
@@ -171,6 +172,7 @@ int b2_launch_jk_s8(const B2PlanDev &P, int precision, const int *active, const 
   } else {
     return B2_ERR_ARG;
   }
+  b2_count_launches(1);
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }

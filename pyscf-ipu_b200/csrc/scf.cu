@@ -258,11 +258,15 @@ k_fock_diis(const B2MolDev *__restrict__ mols, const int *__restrict__ active,
 }
 
 // ------------------------------------------------------------------ eigensolve + density
+// F' = L H L^T; with a previous eigenvector basis W (ws, per molecule) and iter > 0 the Jacobi
+// sweeps run on W^T F' W, which is nearly diagonal once the SCF settles (2-3 sweeps instead of
+// 6-8); the eigenvectors are W V'.  The result is the same eigen-decomposition up to the sign
+// and order of eigenvectors, which the density does not depend on.
 __global__ void __launch_bounds__(256)
 k_eigh_density(const B2MolDev *__restrict__ mols, const int *__restrict__ active,
-               const double *__restrict__ H, const double *__restrict__ Linv,
-               double *__restrict__ D, double *__restrict__ mo_energy, double *__restrict__ C,
-               int *__restrict__ sweeps) {
+               const int *__restrict__ iter, const double *__restrict__ H,
+               const double *__restrict__ Linv, double *__restrict__ D, double *__restrict__ mo_energy,
+               double *__restrict__ C, double *__restrict__ ws, int *__restrict__ sweeps) {
   const int m = blockIdx.x;
   if (active && !active[m]) return;
   extern __shared__ double sm[];
@@ -270,17 +274,19 @@ k_eigh_density(const B2MolDev *__restrict__ mols, const int *__restrict__ active
   __shared__ double rot[B2_MAXNAO];
   __shared__ int prs[B2_MAXNAO];
   __shared__ int order[B2_MAXNAO];
+  __shared__ double evals[B2_MAXNAO];
   const B2MolDev md = mols[m];
   const int N = md.nao, NN = N * N;
   const int n = (N + 1) & ~1;                     // even size for the round-robin ordering
   const int ld = n + 1;                            // odd leading dimension: no bank conflicts
   const long long mo = md.mat_off;
+  const bool warm = ws && iter && iter[m] > 0;
   double *sL = sm, *sT = sL + NN, *sA = sT + NN, *sV = sA + n * ld;
   for (int e = threadIdx.x; e < NN; e += blockDim.x) { sL[e] = Linv[mo + e]; sA[e] = H[mo + e]; }
   __syncthreads();
   b2_mm(sL, sA, sT, N, false);                    // L H
   __syncthreads();
-  // A = (L H) L^T written with leading dimension n
+  // F' = (L H) L^T into sA (leading dimension ld, padded to n)
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
     const int r = e / n, c = e - (e / n) * n;
     double s = 0;
@@ -291,25 +297,61 @@ k_eigh_density(const B2MolDev *__restrict__ mols, const int *__restrict__ active
     sA[r * ld + c] = s;
   }
   __syncthreads();
+  if (warm) {
+    for (int e = threadIdx.x; e < NN; e += blockDim.x) sT[e] = ws[mo + e];     // W
+    __syncthreads();
+    for (int e = threadIdx.x; e < NN; e += blockDim.x) {                       // F' W -> sV
+      const int r = e / N, c = e - (e / N) * N;
+      double s = 0;
+      for (int k = 0; k < N; ++k) s += sA[r * ld + k] * sT[k * N + c];
+      sV[r * ld + c] = s;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < NN; e += blockDim.x) {                       // W^T (F' W) -> sA
+      const int r = e / N, c = e - (e / N) * N;
+      double s = 0;
+      for (int k = 0; k < N; ++k) s += sT[k * N + r] * sV[k * ld + c];
+      sA[r * ld + c] = s;
+    }
+    __syncthreads();
+  }
   const int sw = b2_jacobi(sA, sV, n, N, rot, prs, red, 30);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) evals[i] = sA[i * ld + i];
+  __syncthreads();
+  if (warm) {                                                                   // W V' -> sA
+    for (int e = threadIdx.x; e < NN; e += blockDim.x) {
+      const int r = e / N, c = e - (e / N) * N;
+      double s = 0;
+      for (int k = 0; k < N; ++k) s += sT[r * N + k] * sV[k * ld + c];
+      sA[r * ld + c] = s;
+    }
+  } else {
+    for (int e = threadIdx.x; e < NN; e += blockDim.x) {
+      const int r = e / N, c = e - (e / N) * N;
+      sA[r * ld + c] = sV[r * ld + c];
+    }
+  }
+  __syncthreads();
+  if (ws)
+    for (int e = threadIdx.x; e < NN; e += blockDim.x) ws[mo + e] = sA[(e / N) * ld + e % N];
   // ascending order of eigenvalues
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const double li = sA[i * ld + i];
+    const double li = evals[i];
     int rank = 0;
     for (int j = 0; j < n; ++j) {
-      const double lj = sA[j * ld + j];
+      const double lj = evals[j];
       rank += (lj < li) || (lj == li && j < i);
     }
     order[rank] = i;
   }
   __syncthreads();
-  for (int k = threadIdx.x; k < N; k += blockDim.x) mo_energy[(long long)m * B2_MAXNAO + k] = sA[order[k] * ld + order[k]];
+  for (int k = threadIdx.x; k < N; k += blockDim.x) mo_energy[(long long)m * B2_MAXNAO + k] = evals[order[k]];
   // C[:, k] = L^T V[:, order[k]]  (all N columns, into sT)
   for (int e = threadIdx.x; e < NN; e += blockDim.x) {
     const int r = e / N, k = e - (e / N) * N;
     const int col = order[k];
     double s = 0;
-    for (int a = 0; a < N; ++a) s += sL[a * N + r] * sV[a * ld + col];
+    for (int a = 0; a < N; ++a) s += sL[a * N + r] * sA[a * ld + col];
     sT[e] = s;
   }
   __syncthreads();
@@ -406,16 +448,18 @@ int b2_launch_fock_diis(const B2PlanDev &P, const int *active, const int *iter, 
   B2_CUDA_TRY(cudaFuncSetAttribute(k_fock_diis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   k_fock_diis<<<P.h.nmol, 256, sm, st>>>(P.mols, active, iter, hyb, use_diis, Hcore, S, D, J, K,
                                           Vxc, H, diffJK, ring_err, ring_h, Bmat, diis_err);
+                                          b2_count_launches(1);
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }
 
-int b2_launch_eigh_density(const B2PlanDev &P, const int *active, const double *H,
-                           const double *Linv, double *D, double *mo_energy, double *C,
+int b2_launch_eigh_density(const B2PlanDev &P, const int *active, const int *iter, const double *H,
+                           const double *Linv, double *D, double *mo_energy, double *C, double *ws,
                            int *sweeps, cudaStream_t st) {
   size_t sm = b2_eigh_smem(P.h.max_nao);
   B2_CUDA_TRY(cudaFuncSetAttribute(k_eigh_density, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  k_eigh_density<<<P.h.nmol, 256, sm, st>>>(P.mols, active, H, Linv, D, mo_energy, C, sweeps);
+  k_eigh_density<<<P.h.nmol, 256, sm, st>>>(P.mols, active, iter, H, Linv, D, mo_energy, C, ws, sweeps);
+  b2_count_launches(1);
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }
@@ -424,6 +468,7 @@ int b2_launch_energy(const B2PlanDev &P, const int *active, const double *D, con
                      const double *diffJK, const double *exc, const double *enuc, double *out,
                      cudaStream_t st) {
   k_energy<<<P.h.nmol, 256, 0, st>>>(P.mols, active, D, Hcore, diffJK, exc, enuc, out);
+  b2_count_launches(1);
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }
@@ -433,6 +478,7 @@ int b2_launch_chol_inv(const B2PlanDev &P, const double *S, double *Linv, int *s
   size_t sm = sizeof(double) * 2 * P.h.max_nao * P.h.max_nao;
   B2_CUDA_TRY(cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   k_chol_inv<<<P.h.nmol, 128, sm, st>>>(P.mols, S, Linv, status);
+  b2_count_launches(1);
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }

@@ -187,6 +187,7 @@ __global__ void k_add(long long n, const double *__restrict__ a, const double *_
 
 int b2_launch_int1e(const B2PlanDev &P, double *S, double *T, double *V, cudaStream_t st) {
   k_int1e<<<P.h.nmol, 256, 0, st>>>(P.mols, P.shells, P.ao2sh, P.atom_xyz, P.atom_z, P.boys, S, T, V);
+  b2_count_launches(1);
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }
@@ -223,27 +224,34 @@ int b2_launch_grid_build(B2PlanDev &P, int nz, const double *tmpl_host, const lo
   double brs[10];
   for (int i = 0; i < 10; ++i) brs[i] = br[i] > 0 ? sqrt(br[i]) : 1.0;
   B2_CUDA_TRY(cudaMemcpyToSymbol(c_bragg_sqrt, brs, sizeof(brs)));
-  if (P.g.n_points > 0)
+  if (P.g.n_points > 0) {
     k_grid<<<(unsigned)((P.g.n_points + 127) / 128), 128, 0, st>>>(P.mols, P.h.nmol, P.g.grid_off,
         P.g.atom_pt_off, P.atom_xyz, P.atom_z, P.g.tmpl, P.g.tmpl_off, P.g.n_points, coords, weights);
+    b2_count_launches(1);
+  }
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }
 
 int b2_launch_guess(const B2PlanDev &P, double *D, cudaStream_t st) {
   k_guess<<<P.h.nmol, 256, 0, st>>>(P.mols, P.shells, P.ao2sh, P.atom_z, D);
+  b2_count_launches(1);
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }
 
 int b2_launch_enuc(const B2PlanDev &P, double *enuc, cudaStream_t st) {
   k_enuc<<<(P.h.nmol + 127) / 128, 128, 0, st>>>(P.mols, P.h.nmol, P.atom_xyz, P.atom_z, enuc);
+  b2_count_launches(1);
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }
 
 int b2_launch_add(long long n, const double *a, const double *b, double *c, cudaStream_t st) {
-  if (n > 0) k_add<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, a, b, c);
+  if (n > 0) {
+    k_add<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, a, b, c);
+    b2_count_launches(1);
+  }
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }

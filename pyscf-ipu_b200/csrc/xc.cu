@@ -290,6 +290,7 @@ int b2_launch_ao_eval(const B2PlanDev &P, int precision, const double *coords, v
     k_ao_eval<float><<<(unsigned)P.g.n_gblk, 128, 0, st>>>(P.mols, P.shells, P.g.gblk_off,
         P.g.grid_off, P.g.ao_off, P.h.nmol, coords, (float *)ao);
   else return B2_ERR_ARG;
+  b2_count_launches(1);
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }
@@ -310,12 +311,16 @@ static int b2_xc_impl(const B2PlanDev &P, const int *active, const T *ao, const 
     B2_CUDA_TRY(cudaMemsetAsync(V, 0, sizeof(double) * P.h.n_mat, st));
   }
   k_zero_exc<<<(P.h.nmol + 255) / 256, 256, 0, st>>>(P.h.nmol, active, exc);
+  b2_count_launches(1);
   const size_t sm = sizeof(T) * (B2_XC_NP * B2_XC_NP + 4 * PT * (B2_XC_NP + 1));
   B2_CUDA_TRY(cudaFuncSetAttribute(k_xc_fused<T, PT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  if (nblk > 0)
+  if (nblk > 0) {
     k_xc_fused<T, PT><<<(unsigned)nblk, 256, sm, st>>>(P.mols, xblk, P.g.grid_off, P.g.ao_off,
                                                        P.h.nmol, tpc, active, ao, w, D, V, exc);
+    b2_count_launches(1);
+  }
   k_sym<<<P.h.nmol, 256, 0, st>>>(P.mols, active, V);
+  b2_count_launches(1);
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }

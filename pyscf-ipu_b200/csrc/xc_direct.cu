@@ -240,13 +240,17 @@ static int b2_xcd_impl(const B2PlanDev &P, const int *active, const double *coor
     B2_CUDA_TRY(cudaMemsetAsync(V, 0, sizeof(double) * P.h.n_mat, st));
   }
   k_zero_exc2<<<(P.h.nmol + 255) / 256, 256, 0, st>>>(P.h.nmol, active, exc);
+  b2_count_launches(1);
   const int NBmax = 80;
   const size_t sm = sizeof(T) * (NBmax * NBmax + 4 * PT * (NBmax + 1));
   B2_CUDA_TRY(cudaFuncSetAttribute(k_xc_direct<T, PT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  if (nblk > 0)
+  if (nblk > 0) {
     k_xc_direct<T, PT><<<(unsigned)nblk, 256, sm, st>>>(P.mols, P.shells, xblk, P.g.grid_off, P.h.nmol,
                                                          tpc, active, coords, w, D, V, exc);
+    b2_count_launches(1);
+  }
   k_sym2<<<P.h.nmol, 256, 0, st>>>(P.mols, active, V);
+  b2_count_launches(1);
   B2_CUDA_TRY(cudaGetLastError());
   return B2_OK;
 }
