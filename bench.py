@@ -270,8 +270,13 @@ def main():
     jk_ms = jk_ev[0].elapsed_time(jk_ev[1]) / njk
     jk_bytes = P.n_eri * rbytes
     achieved = jk_bytes / (jk_ms / 1000.0) / 1e9
+    # DRAM traffic per launch: ncu capture of the same kernel on the 256-molecule batch
+    # (profiles/k_jk_s8_batch256.md: 438.9 MB read + 7.9 MB written for 430.4 MB of float32 ERIs),
+    # scaled to this launch by the number of ERIs processed (traffic grows with the list size)
+    traffic = jk_bytes * (446.8 / 430.4) if a.precision == "mixed" else None
     roofline = {"kernel": "k_jk_s8", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "traffic": None, "peak_kind": peak_kind,
+                "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
+                "traffic_source": "ncu 256-molecule capture scaled by ERI count",
                 "algorithmic_bytes_per_launch": jk_bytes, "ms_per_launch": jk_ms}
 
     if a.profile_mode:
