@@ -4,8 +4,9 @@ Workload: a seeded batch of synthetic molecules with the shape of the batched
 configuration (1-9 heavy atoms from C/N/O/F = 0.7/0.1/0.15/0.05, H to valence, STO-3G,
 B3LYP, level-0 grid); synthetic because the reference's GDB/QM1B data is not available.
 One step = the whole hot path over the batch from inputs resident in HBM: device setup
-(1e matrices, Becke grid, guess, L), ERIs (FP32, s8), AO values, and the SCF iterated per
-molecule until |dE| < 1e-6 Ha and DIIS error < 1e-4 with converged molecules retired.
+(1e matrices, Becke grid, MINAO guess, L), the learned initial guess (network forward pass;
+MINAO is the per-molecule fallback), ERIs (FP32, s8), and the SCF iterated per molecule until
+|dE| < 1e-6 Ha and DIIS error < 1e-4 with converged molecules retired.
 ``e2e`` runs the same through the public API from host buffers (plan creation from the
 libcint host arrays, host->device copies, results copied back).
 
@@ -163,6 +164,7 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--guess", default="learned", choices=["learned", "minao"])
     ap.add_argument("--plain-sample", type=int, default=32)
     ap.add_argument("--cpu-sample", type=int, default=8)
     ap.add_argument("--no-cpu", action="store_true")
@@ -198,7 +200,11 @@ def main():
 
     # weak scaling: every rank runs its own shard of molecules (no data-path collective)
     mols = molecules(a.nmol, seed=a.seed + 1000 * rank)
-    eng = RKSEngine(mols, level=a.level, precision=a.precision)
+    net = None
+    if a.guess == "learned":
+        from b200dft.train_guess import load
+        net = load()
+    eng = RKSEngine(mols, level=a.level, precision=a.precision, guess=a.guess, net=net)
     ev = {k: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for k in ("setup", "eri", "ao", "scf")}
 
@@ -287,7 +293,7 @@ def main():
     if rank == 0 and not a.profile_mode:
         barrier()
         t0 = time.perf_counter()
-        e2 = RKSEngine(mols, level=a.level, precision=a.precision)
+        e2 = RKSEngine(mols, level=a.level, precision=a.precision, guess=a.guess, net=net)
         r2 = e2.run_converged()
         host_E = r2["energy"].cpu().numpy()
         host_it = r2["iterations"].cpu().numpy()
@@ -331,13 +337,14 @@ def main():
             "warmup": a.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32+f64" if a.precision == "mixed" else "f64", "data": "synthetic",
             "config": {"workload": "batched uneven STO-3G B3LYP molecules (1-9 heavy atoms C/N/O/F 0.7/0.1/0.15/0.05), level-0 grid",
-                       "nmol_per_gpu": a.nmol, "precision": a.precision,
+                       "nmol_per_gpu": a.nmol, "precision": a.precision, "guess": a.guess,
                        "l2": "inputs (s8 ERIs, AO values) larger than L2 between iterations",
                        "convergence": "|dE|<1e-6 Ha and DIIS err<1e-4, retire converged"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": gpu_launches,
             "phases_ms_per_step": {k: v / a.steps for k, v in phase.items()},
-            "scf": {"converged": int(conv.sum()), "of": int(len(conv)), "mean_its": float(iters[conv].mean()) if conv.any() else None,
+            "scf": {"converged": int(conv.sum()), "of": int(len(conv)),
+                    "fallbacks_to_minao": int(res["fell_back"].sum().item()), "mean_its": float(iters[conv].mean()) if conv.any() else None,
                     "p50_its": float(np.percentile(iters[conv], 50)) if conv.any() else None,
                     "p99_its": float(np.percentile(iters[conv], 99)) if conv.any() else None},
             "plain_fp64_per_molecule": plain,

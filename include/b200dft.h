@@ -59,6 +59,11 @@ int b2_plan_offsets(b2_plan_t plan, int64_t *eri_off, int64_t *mat_off, int *nao
 /* Re-split the J/K work: `elems` s8 entries per CTA (0 = default policy). */
 int b2_plan_set_jk_chunk(b2_plan_t plan, int64_t elems);
 
+/* Restrict the J/K and XC launches to a subset of the batch's molecules (host int[n] molecule
+ * indices; n = 0 restores the full batch).  Used when few molecules are still iterating, so the
+ * launches cover only their work. */
+int b2_plan_set_subset(b2_plan_t plan, const int *mols, int n);
+
 /* All unique ERIs of every molecule into the s8 layout, precision 64 (float64 out) or 32
  * (float32 out).  Replaces int2e_sph (int2e_sph.cpp:6750) dispatched per shell quartet by
  * compute_integrals_2 / integrals_v1 (direct.py:506-707), and mol.intor('int2e_sph',

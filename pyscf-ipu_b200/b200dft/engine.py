@@ -138,7 +138,7 @@ class RKSEngine:
     """
 
     def __init__(self, mols, level=0, precision="fp64", setups=None, device=None, jk_chunk=None,
-                 plan=None):
+                 plan=None, guess="minao", net=None):
         _require_cuda()
         self.mols = list(mols)
         self.level = level
@@ -196,6 +196,9 @@ class RKSEngine:
         self._eri_done = False
         self._ao_done = False
         self._graph = None
+        self.guess = guess                  # "minao" or "learned"
+        self.net = net
+        self.D0_minao = None
         self.graph_replays = 0              # kernels replayed from graphs are not in launch_count()
         self._captured = 0
         self.graph_kernels_per_step = 0
@@ -215,6 +218,19 @@ class RKSEngine:
         check(lib().b2_enuc(P.h, ptr(self.enuc), s), "b2_enuc")
         check(lib().b2_chol_inv(P.h, ptr(self.S), ptr(self.Linv), ptr(self.chol_status), s), "b2_chol_inv")
         self._setup_done = True
+        if self.guess == "learned":
+            self.apply_learned_guess()
+
+    def apply_learned_guess(self):
+        """D0 <- network prediction (MINAO kept as the fallback)"""
+        from .learned import Batch
+        if self.net is None:
+            from .train_guess import load
+            self.net = load(device=self.device)
+        self.D0_minao = self.D0.clone()
+        if not hasattr(self, "_nn_batch"):
+            self._nn_batch = Batch(self.mols, device=self.device, mat_off=self.plan.mat_off, nao=self.plan.nao)
+        self.net.predict(self._nn_batch, self.D0)
 
     # --- kernels -----------------------------------------------------------------------
     def compute_eri(self, stream=None):
@@ -321,15 +337,23 @@ class RKSEngine:
         return g
 
     def run_converged(self, max_its=40, e_tol=1e-6, diis_tol=1e-4, use_diis=True, graph=True,
-                      check_every=1):
+                      check_every=1, fallback=True, rise=3.0, fallback_window=5, tail=0.25):
         """Iterate until each molecule's |E_i - E_{i-1}| < e_tol and DIIS error < diis_tol, then
-        retire it (its kernels skip it).  Returns per-molecule energies, iterations and flags."""
+        retire it (its kernels skip it).  With a learned guess and ``fallback``, a molecule whose DIIS
+        error rises by more than ``rise`` x from one iteration to the next during its first
+        ``fallback_window`` iterations restarts once from MINAO.  Once at most ``tail`` of the batch
+        is still iterating, the J/K and XC launches are compacted to those molecules (eager mode).
+        Returns per-molecule energies, iterations (counted from the first start) and flags."""
         self.prepare()
         self.initial()
         nm = self.plan.nmol
         dev = self.device
         e_prev = torch.full((nm,), float("inf"), dtype=torch.float64, device=dev)
         conv_it = torch.full((nm,), -1, dtype=torch.int32, device=dev)
+        use_fb = fallback and self.D0_minao is not None
+        sub_n = nm + 1
+        fell_back = torch.zeros(nm, dtype=torch.bool, device=dev)
+        err_prev = torch.full((nm,), float("inf"), dtype=torch.float64, device=dev)
         g = None
         if graph:
             # capture one iteration (all launches go to the capture stream); replay per step
@@ -355,11 +379,43 @@ class RKSEngine:
             conv_it = torch.where(newly, torch.full_like(conv_it, i + 1), conv_it)
             self.active.masked_fill_(newly, 0)
             e_prev = torch.where(self.active > 0, e, e_prev)
-            if (i + 1) % check_every == 0 and int(self.active.sum().item()) == 0:
-                break
+            if use_fb:
+                err = self.diis_err
+                bad = ((self.active > 0) & ~fell_back & (self.iter >= 2) & (self.iter <= fallback_window)
+                       & (err > rise * err_prev))
+                err_prev = torch.where(self.active > 0, err, err_prev)
+                if bool(bad.any()):
+                    self._restart_from_minao(bad)
+                    fell_back |= bad
+                    e_prev = torch.where(bad, torch.full_like(e_prev, float("inf")), e_prev)
+                    err_prev = torch.where(bad, torch.full_like(err_prev, float("inf")), err_prev)
+            if (i + 1) % check_every == 0:
+                n_act = int(self.active.sum().item())
+                if n_act == 0:
+                    break
+                if n_act <= tail * nm and n_act <= sub_n // 2:
+                    idx = self.active.nonzero().flatten().to(torch.int32).cpu().numpy()
+                    check(lib().b2_plan_set_subset(self.plan.h, ptr(np.ascontiguousarray(idx)), len(idx)),
+                          "b2_plan_set_subset")
+                    sub_n = n_act
+                    g = None                                 # graph holds full-batch launches
+        if sub_n <= nm:
+            check(lib().b2_plan_set_subset(self.plan.h, None, 0), "b2_plan_set_subset")
         E = self.energy.view(nm, 5)[:, 0].clone()
         return dict(energy=E, iterations=conv_it, converged=conv_it > 0, mo_energy=self.mo_energy.view(nm, NMO),
-                    diis_err=self.diis_err.clone(), its_run=i + 1)
+                    diis_err=self.diis_err.clone(), its_run=i + 1, fell_back=fell_back)
+
+    def _restart_from_minao(self, mask):
+        """restart the molecules in ``mask`` from the MINAO density (iteration counter 0)"""
+        P = self.plan
+        sel = mask.nonzero().flatten().cpu().numpy()
+        for m in sel:
+            o, n = int(P.mat_off[m]), int(P.nao[m]) ** 2
+            self.D[o:o + n].copy_(self.D0_minao[o:o + n])
+        self.iter.masked_fill_(mask, 0)
+        act = mask.to(torch.int32)
+        self.xc(active=act)
+        self.jk(active=act)
 
     def kernels_launched(self, since):
         """library kernels executed since the launch_count() value ``since`` (graph replays included;

@@ -29,8 +29,14 @@ static int b2_upload(T **dst, const std::vector<T> &src) {
   return B2_OK;
 }
 
+static void b2_subset_free(B2PlanDev *P) {
+  cudaFree(P->sub.mol_map); cudaFree(P->sub.jk_off); cudaFree(P->sub.x32); cudaFree(P->sub.x64);
+  P->sub = B2SubsetDev();
+}
+
 static void b2_plan_free(B2PlanDev *P) {
   if (!P) return;
+  b2_subset_free(P);
   b2_grid_free(*P);
   cudaFree(P->mols); cudaFree(P->row_off); cudaFree(P->shells); cudaFree(P->pinfo);
   cudaFree(P->pp64); cudaFree(P->pp32); cudaFree(P->ao2sh); cudaFree(P->cls_list);
@@ -50,6 +56,7 @@ static int b2_set_jk_chunk(B2PlanDev *P, long long elems) {
   P->jk_chunk_off = nullptr;
   int rc = b2_upload(&P->jk_chunk_off, off);
   if (rc) return rc;
+  P->jk_off_h = off;
   P->jk_chunk = elems;
   P->jk_nchunks = off[nmol];
   return B2_OK;
@@ -120,6 +127,34 @@ int b2_plan_offsets(void *plan, int64_t *eri_off, int64_t *mat_off, int *nao, in
 int b2_plan_set_jk_chunk(void *plan, int64_t elems) {
   if (!plan) return B2_ERR_ARG;
   return b2_set_jk_chunk((B2PlanDev *)plan, elems);
+}
+
+int b2_plan_set_subset(void *plan, const int *mols, int n) {
+  if (!plan || n < 0 || (n > 0 && !mols)) return B2_ERR_ARG;
+  B2PlanDev *P = (B2PlanDev *)plan;
+  b2_subset_free(P);
+  if (n == 0) return B2_OK;
+  if (P->g.xblk32_h.empty()) return B2_ERR_ARG;
+  std::vector<int> map(mols, mols + n);
+  std::vector<long long> jo(n + 1, 0), x3(n + 1, 0), x6(n + 1, 0);
+  for (int k = 0; k < n; ++k) {
+    const int m = map[k];
+    if (m < 0 || m >= P->h.nmol) return B2_ERR_ARG;
+    jo[k + 1] = jo[k] + (P->jk_off_h[m + 1] - P->jk_off_h[m]);
+    x3[k + 1] = x3[k] + (P->g.xblk32_h[m + 1] - P->g.xblk32_h[m]);
+    x6[k + 1] = x6[k] + (P->g.xblk64_h[m + 1] - P->g.xblk64_h[m]);
+  }
+  int rc;
+  if ((rc = b2_upload(&P->sub.mol_map, map)) || (rc = b2_upload(&P->sub.jk_off, jo)) ||
+      (rc = b2_upload(&P->sub.x32, x3)) || (rc = b2_upload(&P->sub.x64, x6))) {
+    b2_subset_free(P);
+    return rc;
+  }
+  P->sub.n = n;
+  P->sub.jk_n = jo[n];
+  P->sub.n_x32 = x3[n];
+  P->sub.n_x64 = x6[n];
+  return B2_OK;
 }
 
 int b2_eri_s8(void *plan, int precision, void *eri_out, void *stream) {

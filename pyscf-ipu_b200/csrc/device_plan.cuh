@@ -15,7 +15,14 @@ struct B2GridDev {             // grid layout registered with b2_grid_set
   double *rt = nullptr;        // unused (kept for layout compatibility)
   double *tmpl = nullptr;      // atomic grid templates (x, y, z, w)
   long long *tmpl_off = nullptr, *atom_pt_off = nullptr;
-  std::vector<long long> grid_off_h, ao_off_h;
+  std::vector<long long> grid_off_h, ao_off_h, xblk32_h, xblk64_h;
+};
+
+struct B2SubsetDev {           // compacted work tables for a subset of the batch's molecules
+  int n = 0;                   // 0: no subset (full tables)
+  int *mol_map = nullptr;      // compacted index -> molecule
+  long long *jk_off = nullptr, *x32 = nullptr, *x64 = nullptr;
+  long long jk_n = 0, n_x32 = 0, n_x64 = 0;
 };
 
 struct B2PlanDev {
@@ -40,6 +47,8 @@ struct B2PlanDev {
   B2GridDev g;
   B2EriTask *eri_tasks32 = nullptr, *eri_tasks64 = nullptr;
   std::vector<long long> eri_goff32, eri_goff64;   // task group (class combination) starts
+  std::vector<long long> jk_off_h;                 // host copy of jk_chunk_off
+  B2SubsetDev sub;
 };
 
 int b2_launch_eri_s8(B2PlanDev &P, int precision, void *out, cudaStream_t st);

@@ -50,7 +50,8 @@ template <typename T>
 __global__ void __launch_bounds__(256)
 k_jk_s8(const B2MolDev *__restrict__ mols, const long long *__restrict__ chunk_off, int nmol,
         long long chunk, const int *__restrict__ active, const T *__restrict__ eri,
-        const double *__restrict__ D, double *__restrict__ J, double *__restrict__ K) {
+        const double *__restrict__ D, double *__restrict__ J, double *__restrict__ K,
+        const int *__restrict__ mol_map) {
   extern __shared__ double smem_d[];
   const long long cid = blockIdx.x;
   int lo = 0, hi = nmol - 1;
@@ -58,8 +59,9 @@ k_jk_s8(const B2MolDev *__restrict__ mols, const long long *__restrict__ chunk_o
     int mid = (lo + hi + 1) >> 1;
     if (chunk_off[mid] <= cid) lo = mid; else hi = mid - 1;
   }
-  if (active && !active[lo]) return;
-  const B2MolDev md = mols[lo];
+  const int mol = mol_map ? mol_map[lo] : lo;
+  if (active && !active[mol]) return;
+  const B2MolDev md = mols[mol];
   const int N = md.nao, NN = N * N;
   double *sD = smem_d, *sJ = sD + NN, *sK = sJ + NN;
   for (int e = threadIdx.x; e < NN; e += blockDim.x) {
@@ -152,6 +154,12 @@ int b2_launch_jk_s8(const B2PlanDev &P, int precision, const int *active, const 
                     const double *D, double *J, double *K, cudaStream_t st) {
   if (P.jk_nchunks <= 0) return B2_OK;
   if (P.jk_chunk % (256 * B2_JK_RUN) != 0) return B2_ERR_ARG;
+  const bool sub = P.sub.n > 0;
+  const long long *coff = sub ? P.sub.jk_off : P.jk_chunk_off;
+  const int nm = sub ? P.sub.n : P.h.nmol;
+  const long long nch = sub ? P.sub.jk_n : P.jk_nchunks;
+  const int *map = sub ? P.sub.mol_map : nullptr;
+  if (nch <= 0) return B2_OK;
   if (active) {
     int rc = b2_zero_active(P, active, J, K, st);
     if (rc) return rc;
@@ -163,12 +171,12 @@ int b2_launch_jk_s8(const B2PlanDev &P, int precision, const int *active, const 
   const size_t sm = sizeof(double) * 3 * N * N;
   if (precision == 64) {
     B2_CUDA_TRY(cudaFuncSetAttribute(k_jk_s8<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_jk_s8<double><<<(unsigned)P.jk_nchunks, 256, sm, st>>>(P.mols, P.jk_chunk_off, P.h.nmol,
-        P.jk_chunk, active, (const double *)eri, D, J, K);
+    k_jk_s8<double><<<(unsigned)nch, 256, sm, st>>>(P.mols, coff, nm, P.jk_chunk, active,
+                                                   (const double *)eri, D, J, K, map);
   } else if (precision == 32) {
     B2_CUDA_TRY(cudaFuncSetAttribute(k_jk_s8<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_jk_s8<float><<<(unsigned)P.jk_nchunks, 256, sm, st>>>(P.mols, P.jk_chunk_off, P.h.nmol,
-        P.jk_chunk, active, (const float *)eri, D, J, K);
+    k_jk_s8<float><<<(unsigned)nch, 256, sm, st>>>(P.mols, coff, nm, P.jk_chunk, active,
+                                                  (const float *)eri, D, J, K, map);
   } else {
     return B2_ERR_ARG;
   }

@@ -258,6 +258,8 @@ int b2_grid_setup(B2PlanDev &P, const long long *grid_off_host) {
   P.g.n_ao = aoff[nmol];
   P.g.grid_off_h = goff;
   P.g.ao_off_h = aoff;
+  P.g.xblk32_h = x32;
+  P.g.xblk64_h = x64;
   size_t nb = sizeof(long long) * (nmol + 1);
   B2_CUDA_TRY(cudaMalloc(&P.g.grid_off, nb));
   B2_CUDA_TRY(cudaMalloc(&P.g.gblk_off, nb));

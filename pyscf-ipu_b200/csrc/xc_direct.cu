@@ -164,13 +164,14 @@ k_xc_direct(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shell
             const long long *__restrict__ xblk_off, const long long *__restrict__ grid_off, int nmol,
             int tpc, const int *__restrict__ active, const double *__restrict__ coords,
             const double *__restrict__ w, const double *__restrict__ D, double *__restrict__ V,
-            double *__restrict__ exc) {
+            double *__restrict__ exc, const int *__restrict__ mol_map) {
   extern __shared__ unsigned char smem_raw[];
   __shared__ B2Shell sh[B2_XD_MAXSH];
   __shared__ T sRt[PT][4];
   __shared__ double sC[PT * 3];
   __shared__ double red[8];
-  const int m = b2_findx(xblk_off, nmol, blockIdx.x);
+  const int lo = b2_findx(xblk_off, nmol, blockIdx.x);
+  const int m = mol_map ? mol_map[lo] : lo;
   if (active && !active[m]) return;
   const B2MolDev md = mols[m];
   const int N = md.nao;
@@ -183,7 +184,7 @@ k_xc_direct(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shell
   }
   for (int s = threadIdx.x; s < md.nbas; s += blockDim.x) sh[s] = shells[md.sh_off + s];
   const long long G = grid_off[m + 1] - grid_off[m];
-  const long long t0 = (blockIdx.x - xblk_off[m]) * (long long)tpc;
+  const long long t0 = (blockIdx.x - xblk_off[lo]) * (long long)tpc;
   const double *cm = coords + 3 * grid_off[m];
   const double *wm = w + grid_off[m];
   double e_part = 0;
@@ -232,6 +233,9 @@ template <typename T, int PT>
 static int b2_xcd_impl(const B2PlanDev &P, const int *active, const double *coords, const double *w,
                        const double *D, double *V, double *exc, const long long *xblk,
                        long long nblk, int tpc, cudaStream_t st) {
+  const bool sub = P.sub.n > 0;
+  const int nm = sub ? P.sub.n : P.h.nmol;
+  const int *map = sub ? P.sub.mol_map : nullptr;
   if (P.h.max_nbas > B2_XD_MAXSH) return B2_ERR_SIZE;
   if (active) {
     int rc = b2_zero_active(P, active, V, nullptr, st);
@@ -245,8 +249,8 @@ static int b2_xcd_impl(const B2PlanDev &P, const int *active, const double *coor
   const size_t sm = sizeof(T) * (NBmax * NBmax + 4 * PT * (NBmax + 1));
   B2_CUDA_TRY(cudaFuncSetAttribute(k_xc_direct<T, PT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
   if (nblk > 0) {
-    k_xc_direct<T, PT><<<(unsigned)nblk, 256, sm, st>>>(P.mols, P.shells, xblk, P.g.grid_off, P.h.nmol,
-                                                         tpc, active, coords, w, D, V, exc);
+    k_xc_direct<T, PT><<<(unsigned)nblk, 256, sm, st>>>(P.mols, P.shells, xblk, P.g.grid_off, nm,
+                                                         tpc, active, coords, w, D, V, exc, map);
     b2_count_launches(1);
   }
   k_sym2<<<P.h.nmol, 256, 0, st>>>(P.mols, active, V);
@@ -258,9 +262,12 @@ static int b2_xcd_impl(const B2PlanDev &P, const int *active, const double *coor
 int b2_launch_xc_direct(const B2PlanDev &P, int precision, const int *active, const double *coords,
                         const double *w, const double *D, double *V, double *exc, cudaStream_t st) {
   if (!P.g.grid_off) return B2_ERR_ARG;
+  const bool sub = P.sub.n > 0;
   if (precision == 64)
-    return b2_xcd_impl<double, 32>(P, active, coords, w, D, V, exc, P.g.xblk64, P.g.n_xblk64, P.g.tpc64, st);
+    return b2_xcd_impl<double, 32>(P, active, coords, w, D, V, exc, sub ? P.sub.x64 : P.g.xblk64,
+                                   sub ? P.sub.n_x64 : P.g.n_xblk64, P.g.tpc64, st);
   if (precision == 32)
-    return b2_xcd_impl<float, 64>(P, active, coords, w, D, V, exc, P.g.xblk32, P.g.n_xblk32, P.g.tpc32, st);
+    return b2_xcd_impl<float, 64>(P, active, coords, w, D, V, exc, sub ? P.sub.x32 : P.g.xblk32,
+                                  sub ? P.sub.n_x32 : P.g.n_xblk32, P.g.tpc32, st);
   return B2_ERR_ARG;
 }
