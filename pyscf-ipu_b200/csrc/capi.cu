@@ -47,8 +47,10 @@ static void b2_plan_free(B2PlanDev *P) {
 }
 
 static int b2_set_jk_chunk(B2PlanDev *P, long long elems) {
+  // whole runs of 8 for every thread of a 1024-thread CTA; at most 32768 entries per CTA
+  // keeps the fixed-point J/K accumulators exact
   if (elems <= 0) elems = 32768;
-  elems = (elems + 2047) / 2048 * 2048;          // whole runs of 8 for every thread of a CTA
+  elems = std::min(32768LL, (elems + 8191) / 8192 * 8192);
   const int nmol = P->h.nmol;
   std::vector<long long> off(nmol + 1, 0);
   for (int m = 0; m < nmol; ++m) off[m + 1] = off[m] + (P->h.mols[m].n4 + elems - 1) / elems;
