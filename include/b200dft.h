@@ -58,6 +58,15 @@ int b2_plan_offsets(b2_plan_t plan, int64_t *eri_off, int64_t *mat_off, int *nao
 
 /* Re-split the J/K work: `elems` s8 entries per CTA (0 = default policy). */
 int b2_plan_set_jk_chunk(b2_plan_t plan, int64_t elems);
+/* Float32 exchange-correlation implementation used by b2_xc_direct(precision 32):
+ * 0 = tcgen05 tensor-core kernel with TMEM accumulators (default), 1 = CUDA-core kernel.
+ * No reference counterpart (replaces the XC einsums of nanoDFT.py:105-123). */
+int b2_plan_set_xc_impl(b2_plan_t plan, int impl);
+/* Grid tiles (128 points) per CTA of the tensor-core XC kernel; 0 restores the automatic
+ * choice.  Clears any molecule subset set with b2_plan_set_subset.  No reference counterpart. */
+int b2_plan_set_xc_tiles(b2_plan_t plan, int tiles_per_cta);
+/* Error code of the tensor-core XC kernel's bounded waits (0 = none); reset != 0 clears it. */
+int b2_xc_tc_status(int reset, int *status);
 
 /* Restrict the J/K and XC launches to a subset of the batch's molecules (host int[n] molecule
  * indices; n = 0 restores the full batch).  Used when few molecules are still iterating, so the

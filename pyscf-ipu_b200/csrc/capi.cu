@@ -31,6 +31,7 @@ static int b2_upload(T **dst, const std::vector<T> &src) {
 
 static void b2_subset_free(B2PlanDev *P) {
   cudaFree(P->sub.mol_map); cudaFree(P->sub.jk_off); cudaFree(P->sub.x32); cudaFree(P->sub.x64);
+  cudaFree(P->sub.xtc);
   P->sub = B2SubsetDev();
 }
 
@@ -131,6 +132,27 @@ int b2_plan_set_jk_chunk(void *plan, int64_t elems) {
   return b2_set_jk_chunk((B2PlanDev *)plan, elems);
 }
 
+int b2_plan_set_xc_impl(void *plan, int impl) {
+  if (!plan || impl < 0 || impl > 1) return B2_ERR_ARG;
+  ((B2PlanDev *)plan)->xc_impl = impl;
+  return B2_OK;
+}
+
+int b2_plan_set_xc_tiles(void *plan, int tiles_per_cta) {
+  if (!plan || tiles_per_cta < 0) return B2_ERR_ARG;
+  B2PlanDev *P = (B2PlanDev *)plan;
+  b2_subset_free(P);                  // subset tables derive from the tile split
+  return b2_xc_set_tpc(*P, tiles_per_cta);
+}
+
+int b2_xc_tc_status(int reset, int *status) {
+  if (!status) return B2_ERR_ARG;
+  const int v = b2_xc_tc_status_read(reset);
+  if (v < 0) return B2_ERR_CUDA;
+  *status = v;
+  return B2_OK;
+}
+
 int b2_plan_set_subset(void *plan, const int *mols, int n) {
   if (!plan || n < 0 || (n > 0 && !mols)) return B2_ERR_ARG;
   B2PlanDev *P = (B2PlanDev *)plan;
@@ -138,17 +160,19 @@ int b2_plan_set_subset(void *plan, const int *mols, int n) {
   if (n == 0) return B2_OK;
   if (P->g.xblk32_h.empty()) return B2_ERR_ARG;
   std::vector<int> map(mols, mols + n);
-  std::vector<long long> jo(n + 1, 0), x3(n + 1, 0), x6(n + 1, 0);
+  std::vector<long long> jo(n + 1, 0), x3(n + 1, 0), x6(n + 1, 0), xt(n + 1, 0);
   for (int k = 0; k < n; ++k) {
     const int m = map[k];
     if (m < 0 || m >= P->h.nmol) return B2_ERR_ARG;
     jo[k + 1] = jo[k] + (P->jk_off_h[m + 1] - P->jk_off_h[m]);
     x3[k + 1] = x3[k] + (P->g.xblk32_h[m + 1] - P->g.xblk32_h[m]);
     x6[k + 1] = x6[k] + (P->g.xblk64_h[m + 1] - P->g.xblk64_h[m]);
+    xt[k + 1] = xt[k] + (P->g.xblk_tc_h[m + 1] - P->g.xblk_tc_h[m]);
   }
   int rc;
   if ((rc = b2_upload(&P->sub.mol_map, map)) || (rc = b2_upload(&P->sub.jk_off, jo)) ||
-      (rc = b2_upload(&P->sub.x32, x3)) || (rc = b2_upload(&P->sub.x64, x6))) {
+      (rc = b2_upload(&P->sub.x32, x3)) || (rc = b2_upload(&P->sub.x64, x6)) ||
+      (rc = b2_upload(&P->sub.xtc, xt))) {
     b2_subset_free(P);
     return rc;
   }
@@ -156,6 +180,7 @@ int b2_plan_set_subset(void *plan, const int *mols, int n) {
   P->sub.jk_n = jo[n];
   P->sub.n_x32 = x3[n];
   P->sub.n_x64 = x6[n];
+  P->sub.n_xtc = xt[n];
   return B2_OK;
 }
 

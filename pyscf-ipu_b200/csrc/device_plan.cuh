@@ -8,21 +8,22 @@
 void b2_count_launches(long long n);
 
 struct B2GridDev {             // grid layout registered with b2_grid_set
-  long long n_points = 0, n_gblk = 0, n_xblk32 = 0, n_xblk64 = 0, n_ao = 0;
+  long long n_points = 0, n_gblk = 0, n_xblk32 = 0, n_xblk64 = 0, n_xblk_tc = 0, n_ao = 0;
   long long *grid_off = nullptr, *gblk_off = nullptr, *ao_off = nullptr;
   long long *xblk32 = nullptr, *xblk64 = nullptr;   // fused-XC CTA prefix per precision
-  int tpc32 = 1, tpc64 = 1;                         // tiles per CTA
+  long long *xblk_tc = nullptr;                     // tensor-core XC CTA prefix (128-point tiles)
+  int tpc32 = 1, tpc64 = 1, tpc_tc = 1;             // tiles per CTA
   double *rt = nullptr;        // unused (kept for layout compatibility)
   double *tmpl = nullptr;      // atomic grid templates (x, y, z, w)
   long long *tmpl_off = nullptr, *atom_pt_off = nullptr;
-  std::vector<long long> grid_off_h, ao_off_h, xblk32_h, xblk64_h;
+  std::vector<long long> grid_off_h, ao_off_h, xblk32_h, xblk64_h, xblk_tc_h;
 };
 
 struct B2SubsetDev {           // compacted work tables for a subset of the batch's molecules
   int n = 0;                   // 0: no subset (full tables)
   int *mol_map = nullptr;      // compacted index -> molecule
-  long long *jk_off = nullptr, *x32 = nullptr, *x64 = nullptr;
-  long long jk_n = 0, n_x32 = 0, n_x64 = 0;
+  long long *jk_off = nullptr, *x32 = nullptr, *x64 = nullptr, *xtc = nullptr;
+  long long jk_n = 0, n_x32 = 0, n_x64 = 0, n_xtc = 0;
 };
 
 struct B2PlanDev {
@@ -49,6 +50,7 @@ struct B2PlanDev {
   std::vector<long long> eri_goff32, eri_goff64;   // task group (class combination) starts
   std::vector<long long> jk_off_h;                 // host copy of jk_chunk_off
   B2SubsetDev sub;
+  int xc_impl = 0;             // float32 XC: 0 = tensor-core kernel, 1 = SIMT kernel
 };
 
 int b2_launch_eri_s8(B2PlanDev &P, int precision, void *out, cudaStream_t st);

@@ -226,11 +226,11 @@ __global__ void k_sym(const B2MolDev *__restrict__ mols, const int *__restrict__
 }
 
 static void b2_xc_split(const std::vector<long long> &goff, int nmol, int pt, int &tpc,
-                        std::vector<long long> &xblk) {
+                        std::vector<long long> &xblk, int tpc_fixed = 0) {
   long long tiles = 0;
   for (int m = 0; m < nmol; ++m) tiles += (goff[m + 1] - goff[m] + pt - 1) / pt;
   // enough CTAs to fill the GPU several times over, each flushing V once
-  tpc = (int)std::max(1ll, std::min(16ll, tiles / (8ll * 148ll)));
+  tpc = tpc_fixed > 0 ? tpc_fixed : (int)std::max(1ll, std::min(16ll, tiles / (8ll * 148ll)));
   xblk.assign(nmol + 1, 0);
   for (int m = 0; m < nmol; ++m) {
     const long long nt = (goff[m + 1] - goff[m] + pt - 1) / pt;
@@ -242,7 +242,7 @@ int b2_grid_setup(B2PlanDev &P, const long long *grid_off_host) {
   b2_grid_free(P);
   const int nmol = P.h.nmol;
   std::vector<long long> goff(grid_off_host, grid_off_host + nmol + 1), gblk(nmol + 1, 0),
-      aoff(nmol + 1, 0), x32, x64;
+      aoff(nmol + 1, 0), x32, x64, xtc;
   for (int m = 0; m < nmol; ++m) {
     long long G = goff[m + 1] - goff[m];
     if (G < 0) return B2_ERR_ARG;
@@ -251,31 +251,52 @@ int b2_grid_setup(B2PlanDev &P, const long long *grid_off_host) {
   }
   b2_xc_split(goff, nmol, 64, P.g.tpc32, x32);
   b2_xc_split(goff, nmol, 32, P.g.tpc64, x64);
+  b2_xc_split(goff, nmol, 128, P.g.tpc_tc, xtc);
   P.g.n_points = goff[nmol];
   P.g.n_gblk = gblk[nmol];
   P.g.n_xblk32 = x32[nmol];
   P.g.n_xblk64 = x64[nmol];
+  P.g.n_xblk_tc = xtc[nmol];
   P.g.n_ao = aoff[nmol];
   P.g.grid_off_h = goff;
   P.g.ao_off_h = aoff;
   P.g.xblk32_h = x32;
   P.g.xblk64_h = x64;
+  P.g.xblk_tc_h = xtc;
   size_t nb = sizeof(long long) * (nmol + 1);
   B2_CUDA_TRY(cudaMalloc(&P.g.grid_off, nb));
   B2_CUDA_TRY(cudaMalloc(&P.g.gblk_off, nb));
   B2_CUDA_TRY(cudaMalloc(&P.g.xblk32, nb));
   B2_CUDA_TRY(cudaMalloc(&P.g.xblk64, nb));
+  B2_CUDA_TRY(cudaMalloc(&P.g.xblk_tc, nb));
   B2_CUDA_TRY(cudaMalloc(&P.g.ao_off, nb));
   B2_CUDA_TRY(cudaMemcpy(P.g.grid_off, goff.data(), nb, cudaMemcpyHostToDevice));
   B2_CUDA_TRY(cudaMemcpy(P.g.gblk_off, gblk.data(), nb, cudaMemcpyHostToDevice));
   B2_CUDA_TRY(cudaMemcpy(P.g.xblk32, x32.data(), nb, cudaMemcpyHostToDevice));
   B2_CUDA_TRY(cudaMemcpy(P.g.xblk64, x64.data(), nb, cudaMemcpyHostToDevice));
+  B2_CUDA_TRY(cudaMemcpy(P.g.xblk_tc, xtc.data(), nb, cudaMemcpyHostToDevice));
   B2_CUDA_TRY(cudaMemcpy(P.g.ao_off, aoff.data(), nb, cudaMemcpyHostToDevice));
+  return B2_OK;
+}
+
+int b2_xc_set_tpc(B2PlanDev &P, int tpc) {
+  if (!P.g.grid_off || tpc < 0) return B2_ERR_ARG;
+  std::vector<long long> xtc;
+  b2_xc_split(P.g.grid_off_h, P.h.nmol, 128, P.g.tpc_tc, xtc, tpc);
+  long long *d = nullptr;
+  const size_t nb = sizeof(long long) * (P.h.nmol + 1);
+  B2_CUDA_TRY(cudaMalloc(&d, nb));
+  B2_CUDA_TRY(cudaMemcpy(d, xtc.data(), nb, cudaMemcpyHostToDevice));
+  cudaFree(P.g.xblk_tc);
+  P.g.xblk_tc = d;
+  P.g.xblk_tc_h = xtc;
+  P.g.n_xblk_tc = xtc[P.h.nmol];
   return B2_OK;
 }
 
 void b2_grid_free(B2PlanDev &P) {
   cudaFree(P.g.grid_off); cudaFree(P.g.gblk_off); cudaFree(P.g.xblk32); cudaFree(P.g.xblk64);
+  cudaFree(P.g.xblk_tc);
   cudaFree(P.g.ao_off);
   cudaFree(P.g.tmpl); cudaFree(P.g.tmpl_off); cudaFree(P.g.atom_pt_off);
   P.g = B2GridDev();

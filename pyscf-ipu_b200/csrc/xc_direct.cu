@@ -229,6 +229,20 @@ __global__ void k_sym2(const B2MolDev *__restrict__ mols, const int *__restrict_
   }
 }
 
+int b2_zero_exc(const B2PlanDev &P, const int *active, double *exc, cudaStream_t st) {
+  k_zero_exc2<<<(P.h.nmol + 255) / 256, 256, 0, st>>>(P.h.nmol, active, exc);
+  b2_count_launches(1);
+  B2_CUDA_TRY(cudaGetLastError());
+  return B2_OK;
+}
+
+int b2_sym_v(const B2PlanDev &P, const int *active, double *V, cudaStream_t st) {
+  k_sym2<<<P.h.nmol, 256, 0, st>>>(P.mols, active, V);
+  b2_count_launches(1);
+  B2_CUDA_TRY(cudaGetLastError());
+  return B2_OK;
+}
+
 template <typename T, int PT>
 static int b2_xcd_impl(const B2PlanDev &P, const int *active, const double *coords, const double *w,
                        const double *D, double *V, double *exc, const long long *xblk,
@@ -266,6 +280,8 @@ int b2_launch_xc_direct(const B2PlanDev &P, int precision, const int *active, co
   if (precision == 64)
     return b2_xcd_impl<double, 32>(P, active, coords, w, D, V, exc, sub ? P.sub.x64 : P.g.xblk64,
                                    sub ? P.sub.n_x64 : P.g.n_xblk64, P.g.tpc64, st);
+  if (precision == 32 && P.xc_impl == 0)
+    return b2_launch_xc_tc(P, active, coords, w, D, V, exc, st);
   if (precision == 32)
     return b2_xcd_impl<float, 64>(P, active, coords, w, D, V, exc, sub ? P.sub.x32 : P.g.xblk32,
                                   sub ? P.sub.n_x32 : P.g.n_xblk32, P.g.tpc32, st);

@@ -12,37 +12,19 @@
 template <typename T>
 struct B2XcPoint { T exc, vrho, vgamma; };
 
+// Exchange part (0.08 Slater + 0.72 B88) and correlation parts (0.19 VWN, 0.81 LYP);
+// b2_b3lyp_point is their sum.  The split lets several threads share one grid point.
 template <typename T>
-B2_HD B2XcPoint<T> b2_b3lyp_point(T r0, T r1, T r2, T r3) {
+B2_HD B2XcPoint<T> b2_b3lyp_x(T r0, T r1, T r2, T r3) {
   const T rho = r0 < (T)1e-9 ? (T)1e-9 : (r0 > (T)1e12 ? (T)1e12 : r0);
   const T gx = r1 + r1, gy = r2 + r2, gz = r3 + r3;
   const T sig = gx * gx + gy * gy + gz * gz + (T)1e-20;
   const T lr = log(rho);
-  const T rho13 = exp(lr * (T)(1.0 / 3.0));
   const T inv_rho = (T)1 / rho;
 
   // --- Slater * 0.08: e = -exp(log(rho)/3 - 0.30305460484554375); d(rho e)/drho = 4/3 e
   const T e_lda = (T)-0.08 * exp(lr * (T)(1.0 / 3.0) - (T)0.30305460484554375);
   const T v_lda = (T)(4.0 / 3.0) * e_lda;
-
-  // --- VWN * 0.19: vwn(n) = n p1 G(s), s = (3/(4 pi n))^{1/6}
-  //     G = log s + f [ log(s^2+p2 s+p3)/2 - (1/f+1) log(s-p0) ] + pre atan(c/(2s+p2))
-  //     d vwn/dn = p1 [G - (s/6) G'(s)]
-  const T p0 = (T)-0.10498, p1 = (T)0.0621813817393097900698817274255, p2 = (T)3.72744,
-          p3 = (T)12.9352;
-  const T f = (T)-1.0311676086789439;                // p0 p2 / (p0^2 + p0 p2 + p3) - 1
-  const T c = (T)6.15199081975908;                    // sqrt(4 p3 - p2^2)
-  const T pre = (T)0.6237121531215607;                 // p2 (1/c - p0 / ((p0^2+p0 p2+p3) c / (p2 + 2 p0)))
-  const T log_s = -lr / (T)6 + (T)-0.2387353263835302;    // log(3/(4pi))/6
-  const T s = exp(log_s);
-  const T X = s * s + p2 * s + p3;
-  const T den = (T)2 * s + p2;
-  const T z = c / den;
-  const T G = log_s + f * ((T)0.5 * log(X) - ((T)1 / f + (T)1) * log(s - p0)) + pre * atan(z);
-  const T Gp = (T)1 / s + f * (den / ((T)2 * X) - ((T)1 / f + (T)1) / (s - p0)) +
-               pre * ((T)-2 * c / (den * den)) / ((T)1 + z * z);
-  const T e_vwn = (T)0.19 * rho * p1 * G;                      // per volume
-  const T v_vwn = (T)0.19 * p1 * (G - s / (T)6 * Gp);
 
   // --- B88 * 0.72 (per volume, includes its Slater part): n = rho/2,
   //     x^2 = (sigma/4) n^{-8/3}, E = c3 n^{4/3} - 2 d n^{4/3} h(x), h = x^2 / Dn,
@@ -70,6 +52,57 @@ B2_HD B2XcPoint<T> b2_b3lyp_point(T r0, T r1, T r2, T r3) {
   const T v_b88 = (T)0.72 * (T)0.5 * dEdn;
   const T g_b88 = (T)0.72 * (-d * (T)0.25 * hpx / n43);
 
+  B2XcPoint<T> o;
+  o.exc = e_lda + e_b88 * inv_rho;
+  o.vrho = v_lda + v_b88;
+  o.vgamma = g_b88;
+  return o;
+}
+
+template <typename T>
+B2_HD B2XcPoint<T> b2_b3lyp_vwn(T r0, T r1, T r2, T r3) {
+  const T rho = r0 < (T)1e-9 ? (T)1e-9 : (r0 > (T)1e12 ? (T)1e12 : r0);
+  const T gx = r1 + r1, gy = r2 + r2, gz = r3 + r3;
+  const T sig = gx * gx + gy * gy + gz * gz + (T)1e-20;
+  const T lr = log(rho);
+  const T rho13 = exp(lr * (T)(1.0 / 3.0));
+  const T inv_rho = (T)1 / rho;
+
+  // --- VWN * 0.19: vwn(n) = n p1 G(s), s = (3/(4 pi n))^{1/6}
+  //     G = log s + f [ log(s^2+p2 s+p3)/2 - (1/f+1) log(s-p0) ] + pre atan(c/(2s+p2))
+  //     d vwn/dn = p1 [G - (s/6) G'(s)]
+  const T p0 = (T)-0.10498, p1 = (T)0.0621813817393097900698817274255, p2 = (T)3.72744,
+          p3 = (T)12.9352;
+  const T f = (T)-1.0311676086789439;                // p0 p2 / (p0^2 + p0 p2 + p3) - 1
+  const T c = (T)6.15199081975908;                    // sqrt(4 p3 - p2^2)
+  const T pre = (T)0.6237121531215607;                 // p2 (1/c - p0 / ((p0^2+p0 p2+p3) c / (p2 + 2 p0)))
+  const T log_s = -lr / (T)6 + (T)-0.2387353263835302;    // log(3/(4pi))/6
+  const T s = exp(log_s);
+  const T X = s * s + p2 * s + p3;
+  const T den = (T)2 * s + p2;
+  const T z = c / den;
+  const T G = log_s + f * ((T)0.5 * log(X) - ((T)1 / f + (T)1) * log(s - p0)) + pre * atan(z);
+  const T Gp = (T)1 / s + f * (den / ((T)2 * X) - ((T)1 / f + (T)1) / (s - p0)) +
+               pre * ((T)-2 * c / (den * den)) / ((T)1 + z * z);
+  const T e_vwn = (T)0.19 * rho * p1 * G;                      // per volume
+  const T v_vwn = (T)0.19 * p1 * (G - s / (T)6 * Gp);
+
+  B2XcPoint<T> o;
+  o.exc = e_vwn * inv_rho;
+  o.vrho = v_vwn;
+  o.vgamma = (T)0;
+  return o;
+}
+
+template <typename T>
+B2_HD B2XcPoint<T> b2_b3lyp_lyp(T r0, T r1, T r2, T r3) {
+  const T rho = r0 < (T)1e-9 ? (T)1e-9 : (r0 > (T)1e12 ? (T)1e12 : r0);
+  const T gx = r1 + r1, gy = r2 + r2, gz = r3 + r3;
+  const T sig = gx * gx + gy * gy + gz * gz + (T)1e-20;
+  const T lr = log(rho);
+  const T rho13 = exp(lr * (T)(1.0 / 3.0));
+  const T inv_rho = (T)1 / rho;
+
   // --- LYP * 0.81: t = n^{-1/3}, P = 1/(1 + D t), w = exp(-C t) P, dl = t (C + D P)
   //     R = -A n P - A B CF w n + (A B / 72) w sigma n^{-5/3} (3 + 7 dl)
   //     P' = D P^2 t/(3n), w' = w dl/(3n), dl' = (D^2 P^2 t^2 - dl)/(3n)
@@ -95,8 +128,28 @@ B2_HD B2XcPoint<T> b2_b3lyp_point(T r0, T r1, T r2, T r3) {
   const T g_lyp = (T)0.81 * dRdg;
 
   B2XcPoint<T> o;
-  o.exc = e_lda + (e_vwn + e_b88 + e_lyp) * inv_rho;
-  o.vrho = v_lda + v_vwn + v_b88 + v_lyp;
-  o.vgamma = g_b88 + g_lyp;
+  o.exc = e_lyp * inv_rho;
+  o.vrho = v_lyp;
+  o.vgamma = g_lyp;
+  return o;
+}
+
+template <typename T>
+B2_HD B2XcPoint<T> b2_b3lyp_c(T r0, T r1, T r2, T r3) {
+  const B2XcPoint<T> a = b2_b3lyp_vwn<T>(r0, r1, r2, r3), b = b2_b3lyp_lyp<T>(r0, r1, r2, r3);
+  B2XcPoint<T> o;
+  o.exc = a.exc + b.exc;
+  o.vrho = a.vrho + b.vrho;
+  o.vgamma = a.vgamma + b.vgamma;
+  return o;
+}
+
+template <typename T>
+B2_HD B2XcPoint<T> b2_b3lyp_point(T r0, T r1, T r2, T r3) {
+  const B2XcPoint<T> x = b2_b3lyp_x<T>(r0, r1, r2, r3), c = b2_b3lyp_c<T>(r0, r1, r2, r3);
+  B2XcPoint<T> o;
+  o.exc = x.exc + c.exc;
+  o.vrho = x.vrho + c.vrho;
+  o.vgamma = x.vgamma + c.vgamma;
   return o;
 }

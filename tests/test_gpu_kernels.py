@@ -141,6 +141,35 @@ def test_xc_direct_sizes(cuda, prec):
     eng.close()
 
 
+def test_xc_tensor_core_vs_cuda_core(cuda):
+    # tcgen05 split-TF32 kernel against the float32 CUDA-core kernel and the float64 oracle,
+    # every orbital bucket (nao 5..65), several 128-point tiles per CTA, a converged-like D
+    rng = np.random.default_rng(11)
+    mols = [Mole(random_molecule(rng, k)) for k in (1, 2, 4, 6, 8, 9)]
+    setups = [HostSetup(m, 0) for m in mols]
+    eng = RKSEngine(mols, level=0, precision="mixed", setups=setups)
+    eng.D.copy_(eng.D0)
+    got = {}
+    for impl in (1, 0):
+        check(lib().b2_plan_set_xc_impl(eng.plan.h, impl), "b2_plan_set_xc_impl")
+        eng.xc()
+        torch.cuda.synchronize()
+        got[impl] = (eng.exc.cpu().numpy().copy(), eng.Vxc.cpu().numpy().copy())
+    st = ctypes.c_int(-1)
+    check(lib().b2_xc_tc_status(1, ctypes.byref(st)), "b2_xc_tc_status")
+    assert st.value == 0
+    for mi, (m, s) in enumerate(zip(mols, setups)):
+        exc, V, _ = rks.exchange_correlation(s.D0, rks.ao_values(m, s.coords), s.weights)
+        Vt = eng.plan.unpack(got[0][1], mi)
+        Vs = eng.plan.unpack(got[1][1], mi)
+        # float32 quality: relative 2e-6 on E_xc, 2e-5 * max|V| on V
+        assert abs(got[0][0][mi] - exc) < 2e-6 * abs(exc)
+        np.testing.assert_allclose(Vt, V, atol=2e-5 * np.abs(V).max())
+        np.testing.assert_allclose(Vt, Vs, atol=2e-5 * np.abs(V).max())
+        np.testing.assert_allclose(Vt, Vt.T, atol=1e-12)
+    eng.close()
+
+
 def test_b3lyp_entry(cuda):
     rng = np.random.default_rng(0)
     n = 10000
