@@ -362,8 +362,13 @@ class RKSEngine:
             g = torch.cuda.CUDAGraph()
             c0 = launch_count()
             with torch.cuda.stream(st):
-                with torch.cuda.graph(g, stream=st):
+                # explicit capture: torch.cuda.graph() would also run gc.collect() and release
+                # the allocator cache (both slow for large batches, neither needed here)
+                g.capture_begin()
+                try:
                     self.step(use_diis)
+                finally:
+                    g.capture_end()
             torch.cuda.current_stream().wait_stream(st)
             self.graph_kernels_per_step = launch_count() - c0
             self._captured += self.graph_kernels_per_step

@@ -90,29 +90,41 @@ class Batch:
     """Graph of a list of molecules (host arrays + device copies)."""
 
     def __init__(self, mols, device="cuda", mat_off=None, nao=None):
-        types, mol_of, ao0, heavy, xyz = [], [], [], [], []
-        src, dst, rr = [], [], []
-        pa, pb, pr, pu = [], [], [], []
-        base = 0
-        self.n_atoms = []
-        for mi, m in enumerate(mols):
-            n = m.natm
-            c = m.coords
-            d = np.sqrt(((c[:, None] - c[None]) ** 2).sum(-1))
-            s, t = np.where((d < RC) & ~np.eye(n, dtype=bool))
-            order = np.argsort(t, kind="stable")
-            src.append(s[order] + base); dst.append(t[order] + base); rr.append(d[s[order], t[order]])
-            a, b = np.where(np.triu(d < RC, 1))
-            pa.append(a + base); pb.append(b + base); pr.append(d[a, b])
-            u = c[b] - c[a]
-            pu.append(u / np.maximum(np.linalg.norm(u, axis=1, keepdims=True), 1e-30))
-            o = 0
-            for k in range(n):
-                z = int(m.charges[k])
-                types.append(TYPE[z]); mol_of.append(mi); ao0.append(o); heavy.append(1 if z > 2 else 0)
-                o += 1 if z <= 2 else 5
-            base += n
-            self.n_atoms.append(n)
+        # all molecules at once on a padded (molecule, atom, atom) grid, on ``device``; edge order
+        # per molecule is by receiving atom then sending atom, pair order by (a, b) with a < b
+        nat = np.array([m.natm for m in mols], np.int64)
+        self.n_atoms = [int(n) for n in nat]
+        nm, amax = len(mols), int(nat.max()) if len(mols) else 0
+        valid_h = np.arange(amax)[None, :] < nat[:, None]
+        Ch = np.zeros((nm, amax, 3))
+        Zh = np.zeros((nm, amax), np.int64)
+        if nm:
+            Ch[valid_h] = np.concatenate([m.coords for m in mols])
+            Zh[valid_h] = np.concatenate([m.charges for m in mols])
+        dev = torch.device(device)
+        C = torch.from_numpy(Ch).to(dev)
+        valid = torch.from_numpy(valid_h).to(dev)
+        base = torch.from_numpy(np.concatenate([[0], np.cumsum(nat)[:-1]]).astype(np.int64) if nm
+                                else np.zeros(0, np.int64)).to(dev)
+        d = torch.sqrt(((C[:, :, None] - C[:, None]) ** 2).sum(-1))
+        close = (d < RC) & valid[:, :, None] & valid[:, None, :]
+        edge = close & ~torch.eye(amax, dtype=torch.bool, device=dev)[None]
+        em, et, es = torch.nonzero(edge.transpose(1, 2), as_tuple=True)   # (molecule, receiver, sender)
+        host = lambda x: x.cpu().numpy()
+        src, dst, rr = [host(es + base[em])], [host(et + base[em])], [host(d[em, es, et])]
+        pm, a, b = torch.nonzero(torch.triu(close, 1) if amax else close, as_tuple=True)
+        pa, pb, pr = [host(a + base[pm])], [host(b + base[pm])], [host(d[pm, a, b])]
+        u = C[pm, b] - C[pm, a]
+        pu = [host(u / torch.clamp(torch.linalg.norm(u, dim=1, keepdim=True), min=1e-30))]
+        zf = Zh[valid_h]
+        mol_of = np.repeat(np.arange(nm), nat)
+        width = np.where(Zh <= 2, 1, 5) * valid_h
+        ao0 = (np.cumsum(width, 1) - width)[valid_h]
+        tmap = np.zeros(max(TYPE) + 1 if TYPE else 1, np.int32)
+        for zz, tt in TYPE.items():
+            tmap[zz] = tt
+        types = tmap[zf]
+        heavy = (zf > 2).astype(np.int64)
         cat = lambda xs, dt: np.ascontiguousarray(np.concatenate(xs) if xs else np.zeros(0), dtype=dt)
         self.src, self.dst, self.r = cat(src, np.int32), cat(dst, np.int32), cat(rr, np.float32)
         self.pa, self.pb, self.pr = cat(pa, np.int32), cat(pb, np.int32), cat(pr, np.float32)

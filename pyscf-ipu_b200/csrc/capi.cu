@@ -88,12 +88,11 @@ int b2_plan_create(int nmol, const int *natm, const int *nbas, const int *atm, c
   std::vector<B2MolDev> mols = P->h.mols;
   if ((rc = b2_upload(&P->mols, mols)) || (rc = b2_upload(&P->row_off, P->h.row_off)) ||
       (rc = b2_upload(&P->shells, P->h.shells)) || (rc = b2_upload(&P->pinfo, P->h.pinfo)) ||
-      (rc = b2_upload(&P->pp64, P->h.pp64)) || (rc = b2_upload(&P->pp32, P->h.pp32)) ||
       (rc = b2_upload(&P->ao2sh, P->h.ao2sh)) || (rc = b2_upload(&P->cls_list, P->h.cls_list)) ||
       (rc = b2_upload(&P->cls_cnt, P->h.cls_cnt)) || (rc = b2_upload(&P->atom_xyz, P->h.atom_xyz)) ||
       (rc = b2_upload(&P->atom_z, P->h.atom_z)) || (rc = b2_upload(&P->boys, tab)) ||
       (rc = b2_upload(&P->boys32, std::vector<float>(tab.begin(), tab.end()))) ||
-      (rc = b2_set_jk_chunk(P, 0))) {
+      (rc = b2_set_jk_chunk(P, 0)) || (rc = b2_build_pairs(*P))) {
     b2_plan_free(P);
     return rc;
   }

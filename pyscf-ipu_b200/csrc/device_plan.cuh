@@ -54,6 +54,7 @@ struct B2PlanDev {
 };
 
 int b2_launch_eri_s8(B2PlanDev &P, int precision, void *out, cudaStream_t st);
+int b2_build_pairs(B2PlanDev &P);
 int b2_launch_jk_s8(const B2PlanDev &P, int precision, const int *active, const void *eri,
                     const double *D, double *J, double *K, cudaStream_t st);
 int b2_zero_active(const B2PlanDev &P, const int *active, double *A, double *B, cudaStream_t st);

@@ -272,3 +272,40 @@ extern "C" int b2_int2e_sph_s8_noalloc(const int *atm, int natm, const int *bas,
   if (cudaGetLastError() != cudaSuccess) return B2_ERR_CUDA;
   return B2_OK;
 }
+
+// primitive-pair tables of every shell pair of the batch (float64 and float32 copies), one
+// thread per (shell pair, primitive pair); same formula as the host test build
+__global__ void k_pair_prims(const B2MolDev *__restrict__ mols, int nmol, const B2Shell *__restrict__ shells,
+                             const B2PairInfo *__restrict__ pinfo, long long n_sp,
+                             B2PairPrim<double> *__restrict__ pp64, B2PairPrim<float> *__restrict__ pp32) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n_sp * B2_MAXPP) return;
+  const long long gp = t / B2_MAXPP;
+  const int x = (int)(t - gp * B2_MAXPP);
+  int lo = 0, hi = nmol - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (mols[mid].sp_off <= gp) lo = mid; else hi = mid - 1;
+  }
+  const B2PairInfo pi = pinfo[gp];
+  const int sh = mols[lo].sh_off;
+  B2PairPrim<double> q;
+  b2_pair_prim(shells[sh + pi.I], shells[sh + pi.J], x, q);
+  B2PairPrim<float> f;
+  b2_pair_prim32(q, f);
+  pp64[t] = q;
+  pp32[t] = f;
+}
+
+int b2_build_pairs(B2PlanDev &P) {
+  const long long n = (long long)P.h.n_sp * B2_MAXPP;
+  B2_CUDA_TRY(cudaMalloc(&P.pp64, sizeof(B2PairPrim<double>) * (size_t)std::max(1ll, n)));
+  B2_CUDA_TRY(cudaMalloc(&P.pp32, sizeof(B2PairPrim<float>) * (size_t)std::max(1ll, n)));
+  if (n > 0) {
+    k_pair_prims<<<(unsigned)((n + 255) / 256), 256>>>(P.mols, P.h.nmol, P.shells, P.pinfo, P.h.n_sp,
+                                                       P.pp64, P.pp32);
+    b2_count_launches(1);
+    B2_CUDA_TRY(cudaGetLastError());
+  }
+  return B2_OK;
+}

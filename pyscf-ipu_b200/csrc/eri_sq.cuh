@@ -163,33 +163,34 @@ struct B2EriTask {
 // grouped by class combination g = bra class * 4 + ket class; goff (17 entries) = group starts
 static void b2_eri_tasks(const B2PlanHost &P, int chunk, bool split_p, std::vector<B2EriTask> &out,
                          std::vector<long long> *goff = nullptr) {
-  out.clear();
-  for (int m = 0; m < P.nmol; ++m) {
-    const B2MolDev &md = P.mols[m];
-    for (int IJ = 0; IJ < md.nsp; ++IJ) {
-      const B2PairInfo &pi = P.pinfo[md.sp_off + IJ];
-      const int spcut = (int)b2_tri(pi.I) + pi.I;
-      const int nsub = (split_p && pi.lI) ? 3 : 1;
-      for (int c = 0; c < 4; ++c) {
-        const int cnt = P.cls_cnt[4ll * md.sp_off + (long long)c * md.nsp + spcut];
-        for (int s0 = 0; s0 < cnt; s0 += chunk)
-          for (int sub = 0; sub < nsub; ++sub)
-            out.push_back(B2EriTask{m, IJ, c, s0, std::min(chunk, cnt - s0), nsub > 1 ? sub : -1});
+  // two passes over (molecule, bra pair, ket class): count tasks per group, then place them
+  std::vector<long long> g(17, 0);
+  for (int pass = 0; pass < 2; ++pass) {
+    std::vector<long long> pos(g.begin(), g.end() - 1);
+    for (int m = 0; m < P.nmol; ++m) {
+      const B2MolDev &md = P.mols[m];
+      for (int IJ = 0; IJ < md.nsp; ++IJ) {
+        const B2PairInfo &pi = P.pinfo[md.sp_off + IJ];
+        const int spcut = (int)b2_tri(pi.I) + pi.I;
+        const int nsub = (split_p && pi.lI) ? 3 : 1;
+        for (int c = 0; c < 4; ++c) {
+          const int cnt = P.cls_cnt[4ll * md.sp_off + (long long)c * md.nsp + spcut];
+          const int grp = (pi.lI + 2 * pi.lJ) * 4 + c;
+          if (pass == 0) {
+            g[grp + 1] += (long long)((cnt + chunk - 1) / chunk) * nsub;
+            continue;
+          }
+          for (int s0 = 0; s0 < cnt; s0 += chunk)
+            for (int sub = 0; sub < nsub; ++sub)
+              out[pos[grp]++] = B2EriTask{m, IJ, c, s0, std::min(chunk, cnt - s0), nsub > 1 ? sub : -1};
+        }
       }
     }
-  }
-  std::vector<B2EriTask> sorted;
-  sorted.reserve(out.size());
-  std::vector<long long> g(17, 0);
-  for (int grp = 0; grp < 16; ++grp) {
-    g[grp] = (long long)sorted.size();
-    for (const B2EriTask &t : out) {
-      const B2PairInfo &pi = P.pinfo[P.mols[t.mol].sp_off + t.IJ];
-      if ((pi.lI + 2 * pi.lJ) * 4 + t.cls == grp) sorted.push_back(t);
+    if (pass == 0) {
+      for (int k = 0; k < 16; ++k) g[k + 1] += g[k];
+      out.assign((size_t)g[16], B2EriTask{});
     }
   }
-  g[16] = (long long)sorted.size();
-  out.swap(sorted);
   if (goff) *goff = g;
 }
 

@@ -29,6 +29,7 @@ int b2hc_eri_s8(int nmol, const int *natm, const int *nbas, const int *atm, cons
   B2PlanHost P;
   int rc = b2_plan_build(P, nmol, natm, nbas, atm, bas, env, env_off);
   if (rc) return rc;
+  b2_plan_fill_pairs(P);
   std::vector<double> tab(B2_BOYS_NT * B2_BOYS_NM);
   b2_boys_fill_table(tab.data());
   long long packed = 0;                     // output: molecules' s8 lists back to back

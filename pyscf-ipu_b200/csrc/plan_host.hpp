@@ -37,8 +37,8 @@ struct B2PlanHost {
   std::vector<long long> row_off;         // nmol + 1
   std::vector<B2Shell> shells;
   std::vector<B2PairInfo> pinfo;
-  std::vector<B2PairPrim<double>> pp64;
-  std::vector<B2PairPrim<float>> pp32;
+  std::vector<B2PairPrim<double>> pp64;   // filled by b2_plan_fill_pairs (host builds only;
+  std::vector<B2PairPrim<float>> pp32;    // the device plan computes them on the GPU)
   std::vector<int> ao2sh;                 // per AO: local shell index
   std::vector<int> cls_list;              // per molecule nsp entries (offset sp_off)
   std::vector<int> cls_cnt;               // per molecule 4*nsp (offset 4*sp_off)
@@ -48,6 +48,33 @@ struct B2PlanHost {
 
 static inline int b2_class(int lK, int lL) { return lK + 2 * lL; }   // ss=0, ps=1, sp=2, pp=3
 
+// primitive pair x (= ia * B2_MAXPRIM + ib) of shells a, b: zeta, centre P, P-A, P-B and
+// K = c_a c_b exp(-a b / zeta |AB|^2) sqrt(2) pi^{5/4} / zeta; absent primitives give an inert
+// entry (zeta 1, K 0).  Shared by the device plan kernel and the host test build.
+B2_HD void b2_pair_prim(const B2Shell &a, const B2Shell &b, int x, B2PairPrim<double> &q) {
+  q.zeta = 1.0; q.Px = q.Py = q.Pz = 0.0; q.K = 0.0;
+  q.PAx = q.PAy = q.PAz = q.PBx = q.PBy = q.PBz = 0.0; q.pad = 0.0;
+  const int pa = x / B2_MAXPRIM, pb = x % B2_MAXPRIM;
+  if (pa >= a.nprim || pb >= b.nprim) return;
+  const double k0 = 5.914967172795613;           // sqrt(2) pi^(5/4)
+  double AB2 = 0;
+  for (int d = 0; d < 3; ++d) AB2 += (a.R[d] - b.R[d]) * (a.R[d] - b.R[d]);
+  const double al = a.exp[pa], be = b.exp[pb], z = al + be;
+  double Pc[3];
+  for (int d = 0; d < 3; ++d) Pc[d] = (al * a.R[d] + be * b.R[d]) / z;
+  double K = a.coef[pa] * b.coef[pb] * exp(-al * be / z * AB2) * k0 / z;
+  if (fabs(K) < 1e-300) K = 0;
+  q.zeta = z; q.Px = Pc[0]; q.Py = Pc[1]; q.Pz = Pc[2]; q.K = K;
+  q.PAx = Pc[0] - a.R[0]; q.PAy = Pc[1] - a.R[1]; q.PAz = Pc[2] - a.R[2];
+  q.PBx = Pc[0] - b.R[0]; q.PBy = Pc[1] - b.R[1]; q.PBz = Pc[2] - b.R[2];
+}
+
+B2_HD void b2_pair_prim32(const B2PairPrim<double> &q, B2PairPrim<float> &f) {
+  f.zeta = (float)q.zeta; f.Px = (float)q.Px; f.Py = (float)q.Py; f.Pz = (float)q.Pz;
+  f.K = (float)q.K; f.PAx = (float)q.PAx; f.PAy = (float)q.PAy; f.PAz = (float)q.PAz;
+  f.PBx = (float)q.PBx; f.PBy = (float)q.PBy; f.PBz = (float)q.PBz; f.pad = 0.f;
+}
+
 // returns B2_OK or an error code
 static int b2_plan_build(B2PlanHost &P, int nmol, const int *natm, const int *nbas, const int *atm,
                          const int *bas, const double *env, const long long *env_off) {
@@ -55,7 +82,6 @@ static int b2_plan_build(B2PlanHost &P, int nmol, const int *natm, const int *nb
   P.nmol = nmol;
   P.mols.resize(nmol);
   P.row_off.assign(nmol + 1, 0);
-  const double k0 = std::sqrt(2.0) * std::pow(M_PI, 1.25);
   int atm_row = 0, bas_row = 0;
   for (int m = 0; m < nmol; ++m) {
     const int *A = atm + (size_t)atm_row * B2_ATM_SLOTS;
@@ -116,31 +142,6 @@ static int b2_plan_build(B2PlanHost &P, int nmol, const int *natm, const int *nb
         pi.nprim = a.nprim * b.nprim; pi.pad = 0;
         P.pinfo.push_back(pi);
         cls[(int)b2_tri(I) + J] = b2_class(a.l, b.l);
-        double AB2 = 0;
-        for (int d = 0; d < 3; ++d) AB2 += (a.R[d] - b.R[d]) * (a.R[d] - b.R[d]);
-        for (int x = 0; x < B2_MAXPP; ++x) {
-          B2PairPrim<double> q;
-          std::memset(&q, 0, sizeof(q));
-          int pa = x / B2_MAXPRIM, pb = x % B2_MAXPRIM;
-          if (pa < a.nprim && pb < b.nprim) {
-            double al = a.exp[pa], be = b.exp[pb], z = al + be;
-            double Pc[3];
-            for (int d = 0; d < 3; ++d) Pc[d] = (al * a.R[d] + be * b.R[d]) / z;
-            double K = a.coef[pa] * b.coef[pb] * std::exp(-al * be / z * AB2) * k0 / z;
-            if (std::fabs(K) < 1e-300) K = 0;
-            q.zeta = z; q.Px = Pc[0]; q.Py = Pc[1]; q.Pz = Pc[2]; q.K = K;
-            q.PAx = Pc[0] - a.R[0]; q.PAy = Pc[1] - a.R[1]; q.PAz = Pc[2] - a.R[2];
-            q.PBx = Pc[0] - b.R[0]; q.PBy = Pc[1] - b.R[1]; q.PBz = Pc[2] - b.R[2];
-          } else {
-            q.zeta = 1.0;    // inert padding (K = 0)
-          }
-          P.pp64.push_back(q);
-          B2PairPrim<float> f;
-          f.zeta = (float)q.zeta; f.Px = (float)q.Px; f.Py = (float)q.Py; f.Pz = (float)q.Pz;
-          f.K = (float)q.K; f.PAx = (float)q.PAx; f.PAy = (float)q.PAy; f.PAz = (float)q.PAz;
-          f.PBx = (float)q.PBx; f.PBy = (float)q.PBy; f.PBz = (float)q.PBz; f.pad = 0.f;
-          P.pp32.push_back(f);
-        }
       }
     // class lists and prefix counts
     int start = 0;
@@ -174,4 +175,21 @@ static int b2_plan_build(B2PlanHost &P, int nmol, const int *natm, const int *nb
     bas_row += nbas[m];
   }
   return B2_OK;
+}
+
+// host copy of the primitive-pair tables (the device plan builds them with k_pair_prims)
+static void b2_plan_fill_pairs(B2PlanHost &P) {
+  P.pp64.assign((size_t)P.n_sp * B2_MAXPP, B2PairPrim<double>());
+  P.pp32.assign((size_t)P.n_sp * B2_MAXPP, B2PairPrim<float>());
+  for (int m = 0; m < P.nmol; ++m) {
+    const B2MolDev &md = P.mols[m];
+    for (int sp = 0; sp < md.nsp; ++sp) {
+      const B2PairInfo &pi = P.pinfo[md.sp_off + sp];
+      for (int x = 0; x < B2_MAXPP; ++x) {
+        const size_t t = (size_t)(md.sp_off + sp) * B2_MAXPP + x;
+        b2_pair_prim(P.shells[md.sh_off + pi.I], P.shells[md.sh_off + pi.J], x, P.pp64[t]);
+        b2_pair_prim32(P.pp64[t], P.pp32[t]);
+      }
+    }
+  }
 }
