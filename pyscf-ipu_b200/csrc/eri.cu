@@ -183,39 +183,18 @@ extern "C" int b2_int2e_sph_s8_noalloc(const int *atm, int natm, const int *bas,
   md->n4 = n2 * (n2 + 1) / 2;
   B2PairInfo *PI = (B2PairInfo *)(H + o_pi);
   static int cls[B2_NOALLOC_MAXSP];
-  const double k0 = sqrt(2.0) * pow(M_PI, 1.25);
   for (int I = 0; I < nbas; ++I)
     for (int J = 0; J <= I; ++J) {
       const int sp = (int)b2_tri(I) + J;
       const B2Shell &a = S[I], &b = S[J];
       PI[sp] = B2PairInfo{I, J, a.l, b.l, a.ao0, b.ao0, a.nprim * b.nprim, 0};
       cls[sp] = a.l + 2 * b.l;
-      double AB2 = 0;
-      for (int d = 0; d < 3; ++d) AB2 += (a.R[d] - b.R[d]) * (a.R[d] - b.R[d]);
+      B2PairPrim<double> q64[B2_MAXPP];
+      B2PairPrim<float> q32[B2_MAXPP];
+      b2_pair_prims_packed(a, b, q64, q32);              // same screening as the batch plan
       for (int x = 0; x < B2_MAXPP; ++x) {
-        B2PairPrim<double> q;
-        memset(&q, 0, sizeof(q));
-        q.zeta = 1.0;
-        const int pa = x / B2_MAXPRIM, pb = x % B2_MAXPRIM;
-        if (pa < a.nprim && pb < b.nprim) {
-          const double al = a.exp[pa], be = b.exp[pb], z = al + be;
-          double Pc[3];
-          for (int d = 0; d < 3; ++d) Pc[d] = (al * a.R[d] + be * b.R[d]) / z;
-          double K = a.coef[pa] * b.coef[pb] * exp(-al * be / z * AB2) * k0 / z;
-          if (fabs(K) < 1e-300) K = 0;
-          q.zeta = z; q.Px = Pc[0]; q.Py = Pc[1]; q.Pz = Pc[2]; q.K = K;
-          q.PAx = Pc[0] - a.R[0]; q.PAy = Pc[1] - a.R[1]; q.PAz = Pc[2] - a.R[2];
-          q.PBx = Pc[0] - b.R[0]; q.PBy = Pc[1] - b.R[1]; q.PBz = Pc[2] - b.R[2];
-        }
-        if (precision == 64) {
-          ((B2PairPrim<double> *)(H + o_pp))[(size_t)sp * B2_MAXPP + x] = q;
-        } else {
-          B2PairPrim<float> f;
-          f.zeta = (float)q.zeta; f.Px = (float)q.Px; f.Py = (float)q.Py; f.Pz = (float)q.Pz;
-          f.K = (float)q.K; f.PAx = (float)q.PAx; f.PAy = (float)q.PAy; f.PAz = (float)q.PAz;
-          f.PBx = (float)q.PBx; f.PBy = (float)q.PBy; f.PBz = (float)q.PBz; f.pad = 0.f;
-          ((B2PairPrim<float> *)(H + o_pp))[(size_t)sp * B2_MAXPP + x] = f;
-        }
+        if (precision == 64) ((B2PairPrim<double> *)(H + o_pp))[(size_t)sp * B2_MAXPP + x] = q64[x];
+        else ((B2PairPrim<float> *)(H + o_pp))[(size_t)sp * B2_MAXPP + x] = q32[x];
       }
     }
   int *CL = (int *)(H + o_cls);
@@ -273,15 +252,13 @@ extern "C" int b2_int2e_sph_s8_noalloc(const int *atm, int natm, const int *bas,
   return B2_OK;
 }
 
-// primitive-pair tables of every shell pair of the batch (float64 and float32 copies), one
-// thread per (shell pair, primitive pair); same formula as the host test build
+// primitive-pair tables of every shell pair of the batch (float64 and float32 copies, screened
+// and packed), one thread per shell pair; same code as the host test build
 __global__ void k_pair_prims(const B2MolDev *__restrict__ mols, int nmol, const B2Shell *__restrict__ shells,
                              const B2PairInfo *__restrict__ pinfo, long long n_sp,
                              B2PairPrim<double> *__restrict__ pp64, B2PairPrim<float> *__restrict__ pp32) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n_sp * B2_MAXPP) return;
-  const long long gp = t / B2_MAXPP;
-  const int x = (int)(t - gp * B2_MAXPP);
+  const long long gp = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gp >= n_sp) return;
   int lo = 0, hi = nmol - 1;
   while (lo < hi) {
     const int mid = (lo + hi + 1) >> 1;
@@ -289,12 +266,7 @@ __global__ void k_pair_prims(const B2MolDev *__restrict__ mols, int nmol, const 
   }
   const B2PairInfo pi = pinfo[gp];
   const int sh = mols[lo].sh_off;
-  B2PairPrim<double> q;
-  b2_pair_prim(shells[sh + pi.I], shells[sh + pi.J], x, q);
-  B2PairPrim<float> f;
-  b2_pair_prim32(q, f);
-  pp64[t] = q;
-  pp32[t] = f;
+  b2_pair_prims_packed(shells[sh + pi.I], shells[sh + pi.J], pp64 + gp * B2_MAXPP, pp32 + gp * B2_MAXPP);
 }
 
 int b2_build_pairs(B2PlanDev &P) {
@@ -302,8 +274,8 @@ int b2_build_pairs(B2PlanDev &P) {
   B2_CUDA_TRY(cudaMalloc(&P.pp64, sizeof(B2PairPrim<double>) * (size_t)std::max(1ll, n)));
   B2_CUDA_TRY(cudaMalloc(&P.pp32, sizeof(B2PairPrim<float>) * (size_t)std::max(1ll, n)));
   if (n > 0) {
-    k_pair_prims<<<(unsigned)((n + 255) / 256), 256>>>(P.mols, P.h.nmol, P.shells, P.pinfo, P.h.n_sp,
-                                                       P.pp64, P.pp32);
+    k_pair_prims<<<(unsigned)((P.h.n_sp + 127) / 128), 128>>>(P.mols, P.h.nmol, P.shells, P.pinfo,
+                                                              P.h.n_sp, P.pp64, P.pp32);
     b2_count_launches(1);
     B2_CUDA_TRY(cudaGetLastError());
   }

@@ -28,7 +28,7 @@ struct B2Sq {
           for (int d = 0; d < NL; ++d) acc[a][b][c][d] = (T)0;
     for (int q = 0; q < B2_MAXPP; ++q) {
       const B2PairPrim<T> Q = ket[q];
-      if (Q.K == (T)0) continue;
+      if (Q.K == (T)0) break;                 // packed: the rest of the pair is inert
       const T eta = Q.zeta;
       const T v = b2_div<T>((T)0.5, eta);
       const T QC[3] = {Q.PAx, Q.PAy, Q.PAz};

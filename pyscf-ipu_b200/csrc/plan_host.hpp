@@ -75,6 +75,30 @@ B2_HD void b2_pair_prim32(const B2PairPrim<double> &q, B2PairPrim<float> &f) {
   f.PBx = (float)q.PBx; f.PBy = (float)q.PBy; f.PBz = (float)q.PBz; f.pad = 0.f;
 }
 
+// Primitive-pair screening: a primitive pair whose prefactor |K| is below the threshold
+// contributes at most |K| * max|K| / sqrt(zeta + eta) times an angular factor to any ERI of
+// the pair, i.e. < 1e-12 for the float64 tables and < 1e-8 for the float32 ones, below the
+// accuracy of each form (the reference drops primitive pairs below exp(-60), libcint's
+// expcutoff).  Surviving pairs are packed first, so a loop over a pair's primitives can stop
+// at the first inert entry (K = 0).
+#define B2_PP_SCREEN64 1e-15
+#define B2_PP_SCREEN32 1e-11
+B2_HD void b2_pair_prims_packed(const B2Shell &a, const B2Shell &b, B2PairPrim<double> *q64,
+                                B2PairPrim<float> *q32) {
+  B2PairPrim<double> all[B2_MAXPP];
+  for (int x = 0; x < B2_MAXPP; ++x) b2_pair_prim(a, b, x, all[x]);
+  int n64 = 0, n32 = 0;
+  for (int x = 0; x < B2_MAXPP; ++x) {
+    const double k = fabs(all[x].K);
+    if (all[x].K != 0.0 && k >= B2_PP_SCREEN64) q64[n64++] = all[x];
+    if (all[x].K != 0.0 && k >= B2_PP_SCREEN32) b2_pair_prim32(all[x], q32[n32++]);
+  }
+  B2PairPrim<double> inert;
+  b2_pair_prim(a, b, B2_MAXPP * B2_MAXPP, inert);          // out-of-range index: inert entry
+  for (int x = n64; x < B2_MAXPP; ++x) q64[x] = inert;
+  for (int x = n32; x < B2_MAXPP; ++x) b2_pair_prim32(inert, q32[x]);
+}
+
 // returns B2_OK or an error code
 static int b2_plan_build(B2PlanHost &P, int nmol, const int *natm, const int *nbas, const int *atm,
                          const int *bas, const double *env, const long long *env_off) {
@@ -185,11 +209,8 @@ static void b2_plan_fill_pairs(B2PlanHost &P) {
     const B2MolDev &md = P.mols[m];
     for (int sp = 0; sp < md.nsp; ++sp) {
       const B2PairInfo &pi = P.pinfo[md.sp_off + sp];
-      for (int x = 0; x < B2_MAXPP; ++x) {
-        const size_t t = (size_t)(md.sp_off + sp) * B2_MAXPP + x;
-        b2_pair_prim(P.shells[md.sh_off + pi.I], P.shells[md.sh_off + pi.J], x, P.pp64[t]);
-        b2_pair_prim32(P.pp64[t], P.pp32[t]);
-      }
+      const size_t t = (size_t)(md.sp_off + sp) * B2_MAXPP;
+      b2_pair_prims_packed(P.shells[md.sh_off + pi.I], P.shells[md.sh_off + pi.J], &P.pp64[t], &P.pp32[t]);
     }
   }
 }
