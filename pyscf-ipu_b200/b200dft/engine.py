@@ -343,7 +343,8 @@ class RKSEngine:
         error rises by more than ``rise`` x from one iteration to the next during its first
         ``fallback_window`` iterations restarts once from MINAO.  Once at most ``tail`` of the batch
         is still iterating, the J/K and XC launches are compacted to those molecules (eager mode).
-        Returns per-molecule energies, iterations (counted from the first start) and flags."""
+        Returns per-molecule energies, iterations (counted from the first start), flags and
+        the energies of each molecule's last 5 iterations (``last5``, NaN where fewer ran)."""
         self.prepare()
         self.initial()
         nm = self.plan.nmol
@@ -354,6 +355,7 @@ class RKSEngine:
         sub_n = nm + 1
         fell_back = torch.zeros(nm, dtype=torch.bool, device=dev)
         err_prev = torch.full((nm,), float("inf"), dtype=torch.float64, device=dev)
+        hist = torch.full((nm, 5), float("nan"), dtype=torch.float64, device=dev)   # last 5 energies
         g = None
         if graph:
             # capture one iteration (all launches go to the capture stream); replay per step
@@ -380,6 +382,7 @@ class RKSEngine:
             else:
                 self.step(use_diis)
             e = self.energy.view(nm, 5)[:, 0]
+            hist[:, i % 5] = torch.where(self.active > 0, e, hist[:, i % 5])
             newly = (self.active > 0) & ((e - e_prev).abs() < e_tol) & (self.diis_err < diis_tol)
             conv_it = torch.where(newly, torch.full_like(conv_it, i + 1), conv_it)
             self.active.masked_fill_(newly, 0)
@@ -408,7 +411,7 @@ class RKSEngine:
             check(lib().b2_plan_set_subset(self.plan.h, None, 0), "b2_plan_set_subset")
         E = self.energy.view(nm, 5)[:, 0].clone()
         return dict(energy=E, iterations=conv_it, converged=conv_it > 0, mo_energy=self.mo_energy.view(nm, NMO),
-                    diis_err=self.diis_err.clone(), its_run=i + 1, fell_back=fell_back)
+                    diis_err=self.diis_err.clone(), its_run=i + 1, fell_back=fell_back, last5=hist)
 
     def _restart_from_minao(self, mask):
         """restart the molecules in ``mask`` from the MINAO density (iteration counter 0)"""

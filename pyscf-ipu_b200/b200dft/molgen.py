@@ -135,3 +135,23 @@ def config3_batch(n, seed=0, max_heavy=9):
         k = int(rng.integers(1, max_heavy + 1))
         out.append(random_molecule(rng, k))
     return out
+
+
+def stream_molecule(seed, index, max_heavy=9):
+    """Molecule ``index`` of the seeded molecule stream (1..max_heavy heavy atoms, config-3
+    element probabilities); seeded per index, so any chunking gives the same stream."""
+    rng = np.random.default_rng([seed, index])
+    k = int(rng.integers(1, max_heavy + 1))
+    return random_molecule(rng, k)
+
+
+def stream_chunk(args):
+    """(index, atom string, Mole) for molecules [start, start + n) of the stream; run in worker
+    processes (this module imports numpy only)"""
+    from .mole import Mole
+    seed, start, n, max_heavy = args
+    out = []
+    for i in range(start, start + n):
+        s = stream_molecule(seed, i, max_heavy)
+        out.append((i, s, Mole(s)))
+    return out

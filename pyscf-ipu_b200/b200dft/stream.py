@@ -1,0 +1,223 @@
+"""Streaming dataset generation: a molecule stream through the batched B200 SCF into rows.
+
+Restates the reference's generation driver (dft.py:236-691): molecules are taken from a
+stream, each gets a B3LYP/STO-3G SCF, and one row per molecule is appended to the output
+with the energy, HOMO, LUMO and HOMO-LUMO gap in eV, the standard deviation of the energies of
+the last five iterations (the reference's convergence column, dft.py:632) and N = nao.  Two
+output schemas:
+
+* ``parquet``: the QM1B schema (qm1b/README.md:5-19): smile, atoms, z, energy, homo, lumo, N,
+  std, y (= gap), pos (Bohr, flattened), plus ``iterations`` and ``converged``;
+* ``csv``: gzip CSV with the reference's row dictionary (dft.py:629-645) where the data exist
+  here: smile, atoms, atom_positions, energies (last five, eV), std, homo, lumo, hlgap, N, basis.
+
+Molecules come from the seeded synthetic generator (``molgen.random_molecule``, the stand-in for
+the GDB-11 SMILES + RDKit conformers the reference reads, which are not available); the
+``smile`` column therefore holds an identifier ``gen:<seed>:<index>:<formula>``.
+
+Pipelining (the reference overlaps host preparation with device compute the same way): a
+``spawn`` process pool generates and parses molecules in chunks of one batch; a host thread
+keeps the next batch ready while the GPU runs the current one; a writer thread converts and
+appends finished batches.  Each batch is one ``RKSEngine`` run to convergence: molecules retire
+individually as they converge (their kernels skip them, and the J/K and XC launches are
+compacted to the stragglers), so a batch ends when its slowest molecule converges.
+"""
+import argparse
+import json
+import multiprocessing as mp
+import os
+import queue
+import threading
+import time
+from collections import Counter
+
+import numpy as np
+import torch
+
+from .constants import HARTREE_TO_EV
+from .engine import RKSEngine
+from .molgen import stream_chunk
+
+QM1B_COLUMNS = ("smile", "atoms", "z", "energy", "homo", "lumo", "N", "std", "y", "pos")
+
+
+def _formula(symbols):
+    c = Counter(symbols)
+    return "".join(f"{e}{c[e] if c[e] > 1 else ''}" for e in sorted(c, key=lambda e: (e != "C", e != "H", e)))
+
+
+def batch_rows(items, res, seed):
+    """rows (dict of columns) of one finished batch"""
+    E = res["energy"].cpu().numpy() * HARTREE_TO_EV
+    mo = res["mo_energy"].cpu().numpy()
+    last5 = res["last5"].cpu().numpy() * HARTREE_TO_EV
+    its = res["iterations"].cpu().numpy()
+    conv = res["converged"].cpu().numpy()
+    cols = {k: [] for k in QM1B_COLUMNS + ("iterations", "converged", "last5")}
+    for j, (idx, _, m) in enumerate(items):
+        nocc = m.nelectron // 2
+        homo = float(mo[j, nocc - 1]) * HARTREE_TO_EV
+        lumo = float(mo[j, nocc]) * HARTREE_TO_EV if nocc < m.nao else float("nan")
+        l5 = last5[j][np.isfinite(last5[j])]
+        cols["smile"].append(f"gen:{seed}:{idx}:{_formula(m.symbols)}")
+        cols["atoms"].append("".join(m.symbols))
+        cols["z"].append([int(z) for z in m.charges])
+        cols["energy"].append(float(E[j]))
+        cols["homo"].append(homo)
+        cols["lumo"].append(lumo)
+        cols["N"].append(int(m.nao))
+        cols["std"].append(float(np.std(l5)) if len(l5) else float("nan"))
+        cols["y"].append(abs(lumo - homo))
+        cols["pos"].append([float(x) for x in m.coords.reshape(-1)])
+        cols["iterations"].append(int(its[j]))
+        cols["converged"].append(bool(conv[j]))
+        cols["last5"].append([float(x) for x in l5])
+    return cols
+
+
+class RowWriter:
+    """Appends batches of rows to a Parquet file (QM1B schema) or a gzip CSV (reference schema)."""
+
+    def __init__(self, path, fmt="parquet", basis="sto-3g"):
+        self.path, self.fmt, self.basis = path, fmt, basis
+        self._pq = None
+        self._first = True
+
+    def write(self, cols):
+        if self.path is None:
+            return
+        if self.fmt == "parquet":
+            import pyarrow as pa
+            import pyarrow.parquet as pq
+            keep = QM1B_COLUMNS + ("iterations", "converged")
+            t = pa.table({k: cols[k] for k in keep})
+            if self._pq is None:
+                self._pq = pq.ParquetWriter(self.path, t.schema)
+            self._pq.write_table(t)
+        else:
+            import pandas as pd
+            df = pd.DataFrame({
+                "smile": cols["smile"], "atoms": cols["atoms"], "atom_positions": cols["pos"],
+                "energies": cols["last5"], "std": cols["std"], "homo": cols["homo"],
+                "lumo": cols["lumo"], "hlgap": cols["y"], "N": cols["N"],
+                "basis": [self.basis] * len(cols["N"])})
+            df.to_csv(self.path, mode="a", header=self._first, compression="gzip")
+            self._first = False
+
+    def close(self):
+        if self._pq is not None:
+            self._pq.close()
+            self._pq = None
+
+
+def run_stream(n_total, batch=4096, seed=0, level=0, precision="mixed", guess="learned", out=None,
+               fmt="parquet", workers=None, max_heavy=9, net=None, e_tol=1e-6, diis_tol=1e-4):
+    """Generate ``n_total`` molecules and write one row each; returns throughput and iteration
+    statistics (the streaming configuration: molecules/s, p50/p99 iterations)."""
+    if guess == "learned" and net is None:
+        from .train_guess import load
+        net = load()
+    workers = workers or max(1, min(16, (os.cpu_count() or 2) - 1))
+    chunks = [(seed, s, min(batch, n_total - s), max_heavy) for s in range(0, n_total, batch)]
+    ctx = mp.get_context("spawn")
+    pool = ctx.Pool(workers)
+    ready = queue.Queue(maxsize=2)        # generated batches waiting for the GPU
+    done = queue.Queue(maxsize=4)         # finished batches waiting for the writer
+    writer = RowWriter(out, fmt)
+    stats = {"iterations": [], "converged": 0, "batches": 0, "gpu_s": 0.0}
+    err = []
+
+    def submit(c):
+        # one batch split over every worker
+        seed_, start, n, mh = c
+        step = max(1, -(-n // workers))
+        return [pool.apply_async(stream_chunk, ((seed_, s0, min(step, start + n - s0), mh),))
+                for s0 in range(start, start + n, step)]
+
+    def produce():
+        try:
+            pending = [submit(c) for c in chunks[:2]]
+            for k in range(len(chunks)):
+                parts = pending.pop(0)
+                if k + 2 < len(chunks):
+                    pending.append(submit(chunks[k + 2]))
+                items = [x for p in parts for x in p.get()]
+                ready.put(items)
+        except Exception as e:          # surfaced by the main loop
+            err.append(e)
+        ready.put(None)
+
+    def consume():
+        try:
+            while True:
+                got = done.get()
+                if got is None:
+                    break
+                items, res = got
+                writer.write(batch_rows(items, res, seed))
+        except Exception as e:
+            err.append(e)
+
+    tp = threading.Thread(target=produce, daemon=True)
+    tw = threading.Thread(target=consume, daemon=True)
+    t0 = time.perf_counter()
+    tp.start()
+    tw.start()
+    try:
+        while True:
+            items = ready.get()
+            if items is None or err:
+                break
+            g0 = time.perf_counter()
+            eng = RKSEngine([m for _, _, m in items], level=level, precision=precision, guess=guess, net=net)
+            res = eng.run_converged(e_tol=e_tol, diis_tol=diis_tol)
+            res = {k: (v.clone() if torch.is_tensor(v) else v) for k, v in res.items()}
+            torch.cuda.synchronize()
+            eng.close()
+            stats["gpu_s"] += time.perf_counter() - g0
+            its = res["iterations"].cpu().numpy()
+            stats["iterations"].append(its)
+            stats["converged"] += int((its > 0).sum())
+            stats["batches"] += 1
+            done.put((items, res))
+    finally:
+        done.put(None)
+        tw.join()
+        tp.join(timeout=60)
+        pool.terminate()
+        writer.close()
+    if err:
+        raise err[0]
+    wall = time.perf_counter() - t0
+    its = np.concatenate(stats["iterations"]) if stats["iterations"] else np.zeros(0)
+    its_c = its[its > 0]
+    return {"molecules": int(len(its)), "batch": batch, "wall_s": wall, "molecules_per_s": len(its) / wall,
+            "gpu_s": stats["gpu_s"], "gpu_molecules_per_s": len(its) / max(stats["gpu_s"], 1e-9),
+            "converged": stats["converged"],
+            "p50_iterations": float(np.percentile(its_c, 50)) if len(its_c) else None,
+            "p99_iterations": float(np.percentile(its_c, 99)) if len(its_c) else None,
+            "mean_iterations": float(its_c.mean()) if len(its_c) else None,
+            "workers": workers, "out": out, "format": fmt}
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description="stream molecules through the batched B200 SCF")
+    ap.add_argument("--n", type=int, default=200000, help="molecules to generate")
+    ap.add_argument("--batch", type=int, default=4096)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--level", type=int, default=0)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--guess", default="learned", choices=["learned", "minao"])
+    ap.add_argument("--out", default=None, help="output file (.parquet or .csv.gz)")
+    ap.add_argument("--format", default=None, choices=["parquet", "csv"])
+    ap.add_argument("--workers", type=int, default=None)
+    a = ap.parse_args(argv)
+    fmt = a.format or ("csv" if a.out and a.out.endswith((".csv", ".csv.gz", ".gz")) else "parquet")
+    r = run_stream(a.n, batch=a.batch, seed=a.seed, level=a.level, precision=a.precision, guess=a.guess,
+                   out=a.out, fmt=fmt, workers=a.workers)
+    print(json.dumps(r))
+    return r
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,85 @@
+"""Streaming dataset generation: stream determinism, QM1B / reference row schemas, GPU stream."""
+import numpy as np
+import pytest
+import torch
+
+from b200dft.molgen import stream_chunk, stream_molecule
+from b200dft.stream import QM1B_COLUMNS, RowWriter, batch_rows, run_stream
+from b200dft.constants import HARTREE_TO_EV
+
+
+def test_stream_is_chunking_independent():
+    a = stream_chunk((7, 0, 6, 9))
+    b = stream_chunk((7, 0, 3, 9)) + stream_chunk((7, 3, 3, 9))
+    assert [x[1] for x in a] == [x[1] for x in b]
+    assert a[4][1] == stream_molecule(7, 4)
+    assert len({x[1] for x in a}) == 6
+
+
+def _fake_result(items):
+    n = len(items)
+    mo = np.zeros((n, 72))
+    for j, (_, _, m) in enumerate(items):
+        nocc = m.nelectron // 2
+        mo[j, :m.nao] = np.linspace(-10, 1, m.nao)
+        mo[j, nocc - 1], mo[j, nocc] = -0.3, 0.1
+    last5 = np.full((n, 5), np.nan)
+    last5[:, :3] = -40.0 + np.arange(3) * 1e-7
+    return dict(energy=torch.full((n,), -40.0, dtype=torch.float64), mo_energy=torch.from_numpy(mo),
+                last5=torch.from_numpy(last5), iterations=torch.full((n,), 6, dtype=torch.int32),
+                converged=torch.ones(n, dtype=torch.bool))
+
+
+def test_rows_parquet_schema(tmp_path):
+    pq = pytest.importorskip("pyarrow.parquet")
+    items = stream_chunk((1, 0, 5, 4))
+    cols = batch_rows(items, _fake_result(items), seed=1)
+    path = str(tmp_path / "rows.parquet")
+    w = RowWriter(path, "parquet")
+    w.write(cols)
+    w.write(cols)
+    w.close()
+    t = pq.read_table(path)
+    assert t.num_rows == 10
+    for c in QM1B_COLUMNS:
+        assert c in t.column_names
+    r = t.slice(0, 1).to_pylist()[0]
+    m = items[0][2]
+    assert r["atoms"] == "".join(m.symbols) and r["z"] == [int(z) for z in m.charges]
+    assert r["N"] == m.nao and len(r["pos"]) == 3 * m.natm
+    assert abs(r["energy"] - (-40.0 * HARTREE_TO_EV)) < 1e-9
+    assert abs(r["y"] - 0.4 * HARTREE_TO_EV) < 1e-9
+    assert abs(r["std"] - np.std((-40.0 + np.arange(3) * 1e-7) * HARTREE_TO_EV)) < 1e-12
+
+
+def test_rows_csv_schema(tmp_path):
+    import pandas as pd
+    items = stream_chunk((2, 0, 3, 3))
+    cols = batch_rows(items, _fake_result(items), seed=2)
+    path = str(tmp_path / "data.csv")
+    w = RowWriter(path, "csv")
+    w.write(cols)
+    w.write(cols)
+    w.close()
+    df = pd.read_csv(path, compression="gzip")
+    assert len(df) == 6
+    for c in ("smile", "atoms", "atom_positions", "energies", "std", "homo", "lumo", "hlgap", "N", "basis"):
+        assert c in df.columns
+
+
+@pytest.mark.gpu
+def test_stream_gpu_matches_direct_batches(tmp_path):
+    pq = pytest.importorskip("pyarrow.parquet")
+    from b200dft.engine import RKSEngine
+    path = str(tmp_path / "s.parquet")
+    r = run_stream(40, batch=16, seed=3, guess="minao", out=path, workers=2, max_heavy=5)
+    assert r["molecules"] == 40 and r["converged"] == 40
+    assert r["p50_iterations"] is not None and r["p99_iterations"] >= r["p50_iterations"]
+    t = pq.read_table(path).to_pydict()
+    assert len(t["energy"]) == 40
+    # the same molecules in one batch of 40 give the same energies
+    items = stream_chunk((3, 0, 40, 5))
+    eng = RKSEngine([m for _, _, m in items], level=0, precision="mixed", guess="minao")
+    E = eng.run_converged()["energy"].cpu().numpy() * HARTREE_TO_EV
+    eng.close()
+    np.testing.assert_allclose(np.array(t["energy"]), E, atol=2e-3)   # eV, 1e-4 Ha
