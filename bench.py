@@ -177,6 +177,7 @@ def main():
     import torch.distributed as dist
     from b200dft.engine import RKSEngine, Plan
     from b200dft._lib import launch_count
+    from b200dft import shard
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -192,14 +193,10 @@ def main():
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return shard.max_over_ranks(x, world, device="cuda")
 
     # weak scaling: every rank runs its own shard of molecules (no data-path collective)
-    mols = molecules(a.nmol, seed=a.seed + 1000 * rank)
+    mols = molecules(a.nmol, seed=shard.shard_seed(a.seed, rank))
     net = None
     if a.guess == "learned":
         from b200dft.train_guess import load
@@ -254,7 +251,7 @@ def main():
     clocks = clk.stop()
     gpu_launches = eng.kernels_launched(lc0)
     ms = max_over_ranks(t_start.elapsed_time(t_end)) / a.steps
-    value = world * a.nmol / (ms / 1000.0)
+    value = shard.aggregate_rate(a.nmol, world, ms / 1000.0)
     conv = res["converged"].cpu().numpy()
     iters = res["iterations"].cpu().numpy()
 
@@ -277,9 +274,9 @@ def main():
     jk_bytes = P.n_eri * rbytes
     achieved = jk_bytes / (jk_ms / 1000.0) / 1e9
     # DRAM traffic per launch: ncu capture of the same kernel on the 256-molecule batch
-    # (profiles/k_jk_s8_batch256.md: 438.9 MB read + 7.9 MB written for 430.4 MB of float32 ERIs),
+    # (438.9 MB read + 8.7 MB written for 430.4 MB of float32 ERIs),
     # scaled to this launch by the number of ERIs processed (traffic grows with the list size)
-    traffic = jk_bytes * (446.8 / 430.4) if a.precision == "mixed" else None
+    traffic = jk_bytes * (447.6 / 430.4) if a.precision == "mixed" else None
     roofline = {"kernel": "k_jk_s8", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
                 "traffic_source": "ncu 256-molecule capture scaled by ERI count",

@@ -174,6 +174,52 @@ int b2_int2e_sph_s8(const int *atm, int natm, const int *bas, int nbas, const do
 int b2_int2e_sph_s8_noalloc(const int *atm, int natm, const int *bas, int nbas, const double *env,
                             int n_env, int precision, void *eri_out, void *stream);
 
+/* ---- Learned initial guess: kernels of the message-passing network that predicts D0 ----
+ * No counterpart in the reference's code (its nanoDFT README describes the learned guess as
+ * future work; the reference runs minao, pyscf_utils/minao.py:5-123).  Float32 device
+ * buffers; every call takes the stream to launch on and returns B2_OK or an error code.
+ * Forward and backward of one training step and the prediction are compositions of these. */
+
+/* C[M,N] = beta*C + A B (+ bias[N]); A element (i,k) at A[i*sai + k*sak], B (k,j) at
+ * B[k*sbk + j*sbj].  bf16: 0 float32, 1 operands rounded to bfloat16 (CUDA cores),
+ * 2 bfloat16 tensor-core path (float32 accumulation). */
+int b2_nn_gemm(int M, int N, int K, const float *A, int64_t sai, int64_t sak, const float *B,
+               int64_t sbk, int64_t sbj, float *C, int64_t ldc, const float *bias, float beta,
+               int bf16, void *stream);
+/* out[N] (+)= column sums of X[M,N] (row stride ld); accumulate != 0 adds to out. */
+int b2_nn_colsum(int M, int N, const float *X, int64_t ld, float *out, int accumulate, void *stream);
+/* y = x * sigmoid(x) and its backward dx = dy * silu'(x). */
+int b2_nn_silu(int64_t n, const float *x, float *y, void *stream);
+int b2_nn_silu_bwd(int64_t n, const float *x, const float *dy, float *dx, void *stream);
+/* R Gaussian radial basis functions on [0, rc] of P distances r -> out[P,R]. */
+int b2_nn_rbf(int64_t P, int R, float rc, const float *r, float *out, void *stream);
+/* Message passing over a CSR graph (ptr by receiving atom, src = sender): out[a,:] (+)=
+ * sum_e phi[e,:] * h[src[e],:]. */
+int b2_nn_message(int A, int F, const int *ptr, const int *src, const float *phi, const float *h,
+                  float *out, int accumulate, void *stream);
+/* out[e,:] = dm[dst[e],:] * h[src[e],:] (edge gradient of the message). */
+int b2_nn_pairmul(int64_t P, int F, const int *src, const int *dst, const float *dm, const float *h,
+                  float *out, void *stream);
+/* Pair features x[p] = [h[pa[p]], h[pb[p]], rbf[p]] (width 2F+R) and the transpose of the
+ * gather: dh[pa[p]] += dx[p][0:F], dh[pb[p]] += dx[p][F:2F]. */
+int b2_nn_gather(int64_t P, int F, int R, const int *pa, const int *pb, const float *h,
+                 const float *rbf, float *x, void *stream);
+int b2_nn_scatter(int64_t P, int F, int R, const int *pa, const int *pb, const float *dx, float *dh,
+                  void *stream);
+/* Atom-type embedding h[a,:] = E[type[a],:] and its backward dE. */
+int b2_nn_embed(int A, int F, const int *type, const float *E, float *h, void *stream);
+int b2_nn_embed_bwd(int A, int F, const int *type, const float *dh, float *dE, void *stream);
+/* Symmetric density D (float64, per-molecule blocks at mat_off) from the pair scalars z[P,16]
+ * and site scalars y[A,4]; with a target Dt also the mean squared error, the residual R and
+ * the gradients dz, dy (Dt == NULL: prediction only). */
+int b2_nn_assemble(int64_t P, const int *pa, const int *pb, const float *pu, int A,
+                   const void *atoms, const int64_t *mat_off, const int *nao, const float *z,
+                   const float *y, double *D, int64_t n_mat, const double *Dt, double *R,
+                   float *dz, float *dy, double *loss, void *stream);
+/* One Adam step with decoupled weight decay wd (step = 1, 2, ...). */
+int b2_nn_adam(int64_t n, float *p, const float *g, float *m, float *v, float lr, float b1,
+               float b2, float eps, int step, float wd, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

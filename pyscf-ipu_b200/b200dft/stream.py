@@ -111,14 +111,17 @@ class RowWriter:
 
 
 def run_stream(n_total, batch=4096, seed=0, level=0, precision="mixed", guess="learned", out=None,
-               fmt="parquet", workers=None, max_heavy=9, net=None, e_tol=1e-6, diis_tol=1e-4):
+               fmt="parquet", workers=None, max_heavy=9, net=None, e_tol=1e-6, diis_tol=1e-4,
+               rank=0, world=1):
     """Generate ``n_total`` molecules and write one row each; returns throughput and iteration
-    statistics (the streaming configuration: molecules/s, p50/p99 iterations)."""
+    statistics (the streaming configuration: molecules/s, p50/p99 iterations).  With
+    ``world`` > 1 this process handles the stream chunks of ``rank`` (round robin) only."""
     if guess == "learned" and net is None:
         from .train_guess import load
         net = load()
     workers = workers or max(1, min(16, (os.cpu_count() or 2) - 1))
-    chunks = [(seed, s, min(batch, n_total - s), max_heavy) for s in range(0, n_total, batch)]
+    from .shard import shard_indices
+    chunks = [(seed, s, min(batch, n_total - s), max_heavy) for s in shard_indices(n_total, batch, rank, world)]
     ctx = mp.get_context("spawn")
     pool = ctx.Pool(workers)
     ready = queue.Queue(maxsize=2)        # generated batches waiting for the GPU
