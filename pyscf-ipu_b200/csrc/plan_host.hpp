@@ -30,7 +30,7 @@ struct B2MolDev {
 
 struct B2PlanHost {
   int nmol = 0;
-  int max_nao = 0, max_nbas = 0;
+  int max_nao = 0, max_nbas = 0, max_natm = 0;
   long long n_eri = 0, n_rows = 0, n_mat = 0;
   int n_sh = 0, n_sp = 0, n_ao = 0, n_atm = 0;   // n_eri: padded total (see eri_off)
   std::vector<B2MolDev> mols;
@@ -195,6 +195,7 @@ static int b2_plan_build(B2PlanHost &P, int nmol, const int *natm, const int *nb
     P.row_off[m + 1] = P.n_rows;
     P.max_nao = std::max(P.max_nao, nao);
     P.max_nbas = std::max(P.max_nbas, nbas[m]);
+    P.max_natm = std::max(P.max_natm, natm[m]);
     atm_row += natm[m];
     bas_row += nbas[m];
   }

@@ -91,55 +91,78 @@ __device__ __forceinline__ int b2_find_ll(const long long *off, int lo, int hi, 
   return lo;
 }
 
-// one thread per grid point: coordinate from the owning atom's template, weight = template
-// weight * Becke cell function (3-fold polynomial, size-adjusted) normalised over atoms
+// One CTA per block of 128 grid points of one molecule, one thread per point: coordinate from
+// the owning atom's template, weight = template weight * Becke cell function (3-fold
+// polynomial, size-adjusted, build_grid.py:34-100) normalised over atoms.  The CTA tabulates
+// 1/R_ij and the size adjustments a_ij of its molecule in shared memory; each unordered atom
+// pair is evaluated once per point, using a_ji = -a_ij and the odd polynomial, so
+// s(nu_ji) = 1 - s(nu_ij).  Per-point distances and cell products live in shared memory.
+#define B2_GRID_MAXATM 32
 __global__ void __launch_bounds__(128)
-k_grid(const B2MolDev *__restrict__ mols, int nmol, const long long *__restrict__ grid_off,
-       const long long *__restrict__ atom_pt_off, const double *__restrict__ atom_xyz,
-       const int *__restrict__ atom_z, const double *__restrict__ tmpl,
-       const long long *__restrict__ tmpl_off, long long n_points, double *__restrict__ coords,
-       double *__restrict__ weights) {
-  const long long gp = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (gp >= n_points) return;
-  const int m = b2_find_ll(grid_off, 0, nmol - 1, gp);
+k_grid(const B2MolDev *__restrict__ mols, int nmol, const long long *__restrict__ gblk_off,
+       const long long *__restrict__ grid_off, const long long *__restrict__ atom_pt_off,
+       const double *__restrict__ atom_xyz, const int *__restrict__ atom_z,
+       const double *__restrict__ tmpl, const long long *__restrict__ tmpl_off,
+       double *__restrict__ coords, double *__restrict__ weights) {
+  __shared__ double sA[B2_GRID_MAXATM][3];
+  extern __shared__ double sgrid[];                 // [na*na] 1/R, [na*na] a, [na][128] d, p
+  const int m = b2_find_ll(gblk_off, 0, nmol - 1, blockIdx.x);
   const B2MolDev md = mols[m];
-  const int ia = b2_find_ll(atom_pt_off, md.atm_off, md.atm_off + md.natm - 1, gp) - md.atm_off;
+  const int na = md.natm, tid = threadIdx.x;
+  double *sInv = sgrid, *sAij = sInv + na * na;
+  double (*sDist)[128] = reinterpret_cast<double (*)[128]>(sAij + na * na);
+  double (*sP)[128] = sDist + na;
+  for (int e = tid; e < na; e += blockDim.x) {
+    sA[e][0] = atom_xyz[3 * (md.atm_off + e)];
+    sA[e][1] = atom_xyz[3 * (md.atm_off + e) + 1];
+    sA[e][2] = atom_xyz[3 * (md.atm_off + e) + 2];
+  }
+  __syncthreads();
+  for (int e = tid; e < na * na; e += blockDim.x) {
+    const int i = e / na, j = e - (e / na) * na;
+    double inv = 0.0, a = 0.0;
+    if (i != j) {
+      const double rx = sA[i][0] - sA[j][0], ry = sA[i][1] - sA[j][1], rz = sA[i][2] - sA[j][2];
+      inv = 1.0 / sqrt(rx * rx + ry * ry + rz * rz);
+      const double chi = c_bragg_sqrt[atom_z[md.atm_off + i]] / c_bragg_sqrt[atom_z[md.atm_off + j]];
+      const double uu = (chi - 1) / (chi + 1);
+      a = fmin(0.5, fmax(-0.5, uu / (uu * uu - 1)));
+    }
+    sInv[e] = inv;
+    sAij[e] = a;
+  }
+  __syncthreads();
+  const long long G = grid_off[m + 1] - grid_off[m];
+  const long long lp = (blockIdx.x - gblk_off[m]) * 128 + tid;    // point index in the molecule
+  if (lp >= G) return;
+  const long long gp = grid_off[m] + lp;
+  const int ia = b2_find_ll(atom_pt_off, md.atm_off, md.atm_off + na - 1, gp) - md.atm_off;
   const int z = atom_z[md.atm_off + ia];
   const long long t = tmpl_off[z] + (gp - atom_pt_off[md.atm_off + ia]);
-  const double *A = atom_xyz + 3 * md.atm_off;
-  const double x = A[3 * ia] + tmpl[4 * t], y = A[3 * ia + 1] + tmpl[4 * t + 1],
-               zc = A[3 * ia + 2] + tmpl[4 * t + 2];
+  const double x = sA[ia][0] + tmpl[4 * t], y = sA[ia][1] + tmpl[4 * t + 1], zc = sA[ia][2] + tmpl[4 * t + 2];
   coords[3 * gp] = x; coords[3 * gp + 1] = y; coords[3 * gp + 2] = zc;
-  const int na = md.natm;
-  double dist[32];
   for (int i = 0; i < na; ++i) {
-    const double dx = x - A[3 * i], dy = y - A[3 * i + 1], dz = zc - A[3 * i + 2];
-    dist[i] = sqrt(dx * dx + dy * dy + dz * dz);
+    const double dx = x - sA[i][0], dy = y - sA[i][1], dz = zc - sA[i][2];
+    sDist[i][tid] = sqrt(dx * dx + dy * dy + dz * dz);
+    sP[i][tid] = 1.0;
   }
-  double psum = 0, pown = 0;
   for (int i = 0; i < na; ++i) {
-    double p = 1.0;
-    const int zi = atom_z[md.atm_off + i];
-    for (int j = 0; j < na; ++j) {
-      if (j == i) continue;
-      const int zj = atom_z[md.atm_off + j];
-      const double rx = A[3 * i] - A[3 * j], ry = A[3 * i + 1] - A[3 * j + 1], rz = A[3 * i + 2] - A[3 * j + 2];
-      const double rij = sqrt(rx * rx + ry * ry + rz * rz);
-      const double mu = (dist[i] - dist[j]) / rij;
-      const double chi = c_bragg_sqrt[zi] / c_bragg_sqrt[zj];
-      const double uu = (chi - 1) / (chi + 1);
-      double aij = uu / (uu * uu - 1);
-      aij = fmin(0.5, fmax(-0.5, aij));
-      double g = mu + aij * (1 - mu * mu);
+    const double di = sDist[i][tid];
+    double pi = sP[i][tid];
+    for (int j = i + 1; j < na; ++j) {
+      const double mu = (di - sDist[j][tid]) * sInv[i * na + j];
+      double g = mu + sAij[i * na + j] * (1 - mu * mu);
       g = (3 - g * g) * g * 0.5;
       g = (3 - g * g) * g * 0.5;
       g = (3 - g * g) * g * 0.5;
-      p *= 0.5 * (1 - g);
+      pi *= 0.5 * (1 - g);
+      sP[j][tid] *= 0.5 * (1 + g);
     }
-    psum += p;
-    if (i == ia) pown = p;
+    sP[i][tid] = pi;
   }
-  weights[gp] = tmpl[4 * t + 3] * pown / psum;
+  double psum = 0;
+  for (int i = 0; i < na; ++i) psum += sP[i][tid];
+  weights[gp] = tmpl[4 * t + 3] * sP[ia][tid] / psum;
 }
 
 // ------------------------------------------------------------------ guess + E_nuc
@@ -225,8 +248,11 @@ int b2_launch_grid_build(B2PlanDev &P, int nz, const double *tmpl_host, const lo
   for (int i = 0; i < 10; ++i) brs[i] = br[i] > 0 ? sqrt(br[i]) : 1.0;
   B2_CUDA_TRY(cudaMemcpyToSymbol(c_bragg_sqrt, brs, sizeof(brs)));
   if (P.g.n_points > 0) {
-    k_grid<<<(unsigned)((P.g.n_points + 127) / 128), 128, 0, st>>>(P.mols, P.h.nmol, P.g.grid_off,
-        P.g.atom_pt_off, P.atom_xyz, P.atom_z, P.g.tmpl, P.g.tmpl_off, P.g.n_points, coords, weights);
+    if (P.h.max_natm > B2_GRID_MAXATM) return B2_ERR_SIZE;
+    const size_t sm = sizeof(double) * (2 * P.h.max_natm * P.h.max_natm + 2 * 128 * P.h.max_natm);
+    B2_CUDA_TRY(cudaFuncSetAttribute(k_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_grid<<<(unsigned)P.g.n_gblk, 128, sm, st>>>(P.mols, P.h.nmol, P.g.gblk_off, P.g.grid_off,
+        P.g.atom_pt_off, P.atom_xyz, P.atom_z, P.g.tmpl, P.g.tmpl_off, coords, weights);
     b2_count_launches(1);
   }
   B2_CUDA_TRY(cudaGetLastError());
