@@ -3,38 +3,44 @@
 // (direct.py:584-707), and writes straight into the tril-of-tril s8 layout of
 // ``mol.intor('int2e_sph', aosym='s8')`` (nanoDFT.py:285).
 //
-// Decomposition: a host-built task list (plan) assigns each CTA one bra shell pair IJ of one
-// molecule and up to 128 ket shell pairs KL of a single angular class (ss, ps, sp, pp), all
-// with KL <= (I,I); the bra's primitive pairs are staged in shared memory and every thread
-// evaluates all components of one shell quartet (float32 form) or of one bra component
-// (float64 form, p bras split over 3 threads).  Every s8 entry is written exactly once, by the
+// Decomposition: a host-built task list (plan) assigns each warp one bra shell pair IJ of one
+// molecule and a chunk of ket shell pairs KL of a single angular class (ss, ps, sp, pp), all
+// with KL <= (I,I) (32 kets per task for batch plans: warps stay full; 4 tasks per CTA); the
+// bra's primitive pairs are staged in the warp's shared-memory slot and every lane evaluates
+// all components of one shell quartet (float32 form) or of one bra component (float64 form,
+// p bras split over 3 lanes), looping over the chunk's kets.  Every s8 entry is written exactly once, by the
 // CTA whose bra shell pair owns its row ij.
 #include "eri_sq.cuh"
 #include "device_plan.cuh"
 
 template <typename T, int LI, int LJ, int LK, int LL>
 __global__ void __launch_bounds__(128)
-k_eri_sq(const B2EriTask *__restrict__ tasks, const B2MolDev *__restrict__ mols,
+k_eri_sq(const B2EriTask *__restrict__ tasks, long long ntask, const B2MolDev *__restrict__ mols,
          const B2PairInfo *__restrict__ pinfo, const B2PairPrim<T> *__restrict__ pp,
          const int *__restrict__ cls_list, const T *__restrict__ btab, T *__restrict__ out) {
-  __shared__ B2PairPrim<T> sbra[B2_MAXPP];
-  __shared__ int s_nb;
-  const B2EriTask tk = tasks[blockIdx.x];
+  __shared__ B2PairPrim<T> sbra[4][B2_MAXPP];
+  __shared__ int s_nb[4];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long ti = (long long)blockIdx.x * 4 + w;
+  if (ti >= ntask) return;                        // whole warp
+  const B2EriTask tk = tasks[ti];
   const B2MolDev md = mols[tk.mol];
   const B2PairInfo bp = pinfo[md.sp_off + tk.IJ];
-  if (threadIdx.x == 0) {
+  if (lane == 0) {
     const B2PairPrim<T> *src = pp + (size_t)(md.sp_off + tk.IJ) * B2_MAXPP;
     int nb = 0;
     for (int x = 0; x < B2_MAXPP; ++x)
-      if (src[x].K != (T)0) sbra[nb++] = src[x];
-    s_nb = nb;
+      if (src[x].K != (T)0) sbra[w][nb++] = src[x];
+    s_nb[w] = nb;
   }
-  __syncthreads();
-  if ((int)threadIdx.x >= tk.count) return;
-  const int KL = cls_list[md.sp_off + md.cls_start[tk.cls] + tk.start + threadIdx.x];
-  const B2PairInfo kp = pinfo[md.sp_off + KL];
-  b2_sq_sub<T, LI, LJ, LK, LL, T>(tk.sub, sbra, s_nb, pp + (size_t)(md.sp_off + KL) * B2_MAXPP,
-                                  btab, out + md.eri_off, bp, kp);
+  __syncwarp();
+  const int nb = s_nb[w];
+  for (int k = lane; k < tk.count; k += 32) {
+    const int KL = cls_list[md.sp_off + md.cls_start[tk.cls] + tk.start + k];
+    const B2PairInfo kp = pinfo[md.sp_off + KL];
+    b2_sq_sub<T, LI, LJ, LK, LL, T>(tk.sub, sbra[w], nb, pp + (size_t)(md.sp_off + KL) * B2_MAXPP,
+                                    btab, out + md.eri_off, bp, kp);
+  }
 }
 
 template <typename T> static const T *b2_boys_table(const B2PlanDev &P);
@@ -44,10 +50,11 @@ template <> const float *b2_boys_table<float>(const B2PlanDev &P) { return P.boy
 template <typename T, int LI, int LJ, int LK, int LL>
 static void b2_eri_group(const B2PlanDev &P, const B2EriTask *tasks, long long n,
                          const B2PairPrim<T> *pp, T *out, cudaStream_t st) {
-  const long long maxg = (1ll << 31) - 1;
+  const long long maxg = 4 * ((1ll << 31) - 1);    // 4 tasks (one per warp) per CTA
   for (long long t0 = 0; t0 < n; t0 += maxg) {
-    k_eri_sq<T, LI, LJ, LK, LL><<<(unsigned)std::min(maxg, n - t0), 128, 0, st>>>(
-        tasks + t0, P.mols, P.pinfo, pp, P.cls_list, b2_boys_table<T>(P), out);
+    const long long nt = std::min(maxg, n - t0);
+    k_eri_sq<T, LI, LJ, LK, LL><<<(unsigned)((nt + 3) / 4), 128, 0, st>>>(
+        tasks + t0, nt, P.mols, P.pinfo, pp, P.cls_list, b2_boys_table<T>(P), out);
     b2_count_launches(1);
   }
 }
@@ -65,15 +72,79 @@ static void b2_eri_all(const B2PlanDev &P, const B2EriTask *tasks, const std::ve
 #undef B2_G
 }
 
+// Work list on the device: the host makes one counting pass over (shell pair, ket class) and
+// uploads each item's first task index (same grouping and order as b2_eri_tasks); one thread
+// per item then writes its tasks.  A 4096-molecule batch has ~1.7e7 tasks.
+__global__ void k_eri_tasks(const B2MolDev *__restrict__ mols, int nmol, const B2PairInfo *__restrict__ pinfo,
+                            const int *__restrict__ cls_cnt, const int *__restrict__ toff, long long n_sp,
+                            int chunk, int split_p, B2EriTask *__restrict__ tasks) {
+  const long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (it >= 4 * n_sp) return;
+  const long long sp = it >> 2;
+  const int c = (int)(it & 3);
+  int lo = 0, hi = nmol - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (mols[mid].sp_off <= sp) lo = mid; else hi = mid - 1;
+  }
+  const B2MolDev md = mols[lo];
+  const B2PairInfo pi = pinfo[sp];
+  const int IJ = (int)(sp - md.sp_off);
+  const int spcut = (int)b2_tri(pi.I) + pi.I;
+  const int cnt = cls_cnt[4ll * md.sp_off + (long long)c * md.nsp + spcut];
+  const int nsub = (split_p && pi.lI) ? 3 : 1;
+  long long o = toff[it];
+  for (int s0 = 0; s0 < cnt; s0 += chunk)
+    for (int sub = 0; sub < nsub; ++sub)
+      tasks[o++] = B2EriTask{lo, IJ, c, s0, min(chunk, cnt - s0), nsub > 1 ? sub : -1};
+}
+
 static int b2_eri_task_upload(B2PlanDev &P, int precision) {
   B2EriTask *&dst = precision == 64 ? P.eri_tasks64 : P.eri_tasks32;
   std::vector<long long> &goff = precision == 64 ? P.eri_goff64 : P.eri_goff32;
   if (dst) return B2_OK;
-  std::vector<B2EriTask> t;
-  b2_eri_tasks(P.h, 128, precision == 64, t, &goff);
-  B2_CUDA_TRY(cudaMalloc(&dst, sizeof(B2EriTask) * std::max<size_t>(1, t.size())));
-  if (!t.empty())
-    B2_CUDA_TRY(cudaMemcpy(dst, t.data(), sizeof(B2EriTask) * t.size(), cudaMemcpyHostToDevice));
+  const int chunk = 32;                          // kets per warp task
+  const bool split_p = precision == 64;
+  const B2PlanHost &H = P.h;
+  const long long nsp = H.n_sp;
+  std::vector<int> toff((size_t)std::max(1ll, 4 * nsp));
+  std::vector<long long> g(17, 0);
+  for (int pass = 0; pass < 2; ++pass) {
+    std::vector<long long> pos(g.begin(), g.end() - 1);
+    for (int m = 0; m < H.nmol; ++m) {
+      const B2MolDev &md = H.mols[m];
+      for (int IJ = 0; IJ < md.nsp; ++IJ) {
+        const B2PairInfo &pi = H.pinfo[md.sp_off + IJ];
+        const int spcut = (int)b2_tri(pi.I) + pi.I;
+        const int nsub = (split_p && pi.lI) ? 3 : 1;
+        for (int c = 0; c < 4; ++c) {
+          const int cnt = H.cls_cnt[4ll * md.sp_off + (long long)c * md.nsp + spcut];
+          const int grp = (pi.lI + 2 * pi.lJ) * 4 + c;
+          const long long n = (long long)((cnt + chunk - 1) / chunk) * nsub;
+          if (pass == 0) { g[grp + 1] += n; continue; }
+          toff[4 * ((size_t)md.sp_off + IJ) + c] = (int)pos[grp];
+          pos[grp] += n;
+        }
+      }
+    }
+    if (pass == 0) {
+      for (int k = 0; k < 16; ++k) g[k + 1] += g[k];
+      if (g[16] >= (1ll << 31)) return B2_ERR_SIZE;
+    }
+  }
+  goff = g;
+  int *dtoff = nullptr;
+  B2_CUDA_TRY(cudaMalloc(&dst, sizeof(B2EriTask) * std::max<size_t>(1, (size_t)g[16])));
+  B2_CUDA_TRY(cudaMalloc(&dtoff, sizeof(int) * toff.size()));
+  B2_CUDA_TRY(cudaMemcpy(dtoff, toff.data(), sizeof(int) * toff.size(), cudaMemcpyHostToDevice));
+  if (nsp > 0) {
+    k_eri_tasks<<<(unsigned)((4 * nsp + 255) / 256), 256>>>(P.mols, H.nmol, P.pinfo, P.cls_cnt, dtoff, nsp,
+                                                            chunk, split_p ? 1 : 0, dst);
+    b2_count_launches(1);
+  }
+  B2_CUDA_TRY(cudaGetLastError());
+  B2_CUDA_TRY(cudaDeviceSynchronize());
+  cudaFree(dtoff);
   return B2_OK;
 }
 

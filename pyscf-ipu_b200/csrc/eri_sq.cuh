@@ -153,7 +153,7 @@ struct B2Sq {
   }
 };
 
-// work item of the ERI kernel: one CTA = one bra shell pair x <= 128 kets of one class
+// work item of the ERI kernel: one warp = one bra shell pair x a chunk of kets of one class
 struct B2EriTask {
   int mol, IJ, cls, start, count, sub;
 };
