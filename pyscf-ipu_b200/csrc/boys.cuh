@@ -50,13 +50,13 @@ B2_HD void b2_boys(T t, const TT *__restrict__ table, T *F) {
     // Horner: sum_j F_{L+j}(T_k) dt^j / j!
     T acc = (T)row[NT - 1];
 #pragma unroll
-    for (int j = NT - 1; j >= 1; --j) acc = (T)row[j - 1] + acc * dt / (T)j;
+    for (int j = NT - 1; j >= 1; --j) acc = (T)row[j - 1] + acc * dt * (T)(1.0 / j);
     F[L] = acc;
     if (L > 0) {
       T et = exp(-t);
       T t2 = t + t;
 #pragma unroll
-      for (int m = L - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + et) / (T)(2 * m + 1);
+      for (int m = L - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + et) * (T)(1.0 / (2 * m + 1));
     }
   } else {
     T inv = (T)1 / t;

@@ -76,16 +76,16 @@ B2_HD B2XcPoint<T> b2_b3lyp_vwn(T r0, T r1, T r2, T r3) {
   const T f = (T)-1.0311676086789439;                // p0 p2 / (p0^2 + p0 p2 + p3) - 1
   const T c = (T)6.15199081975908;                    // sqrt(4 p3 - p2^2)
   const T pre = (T)0.6237121531215607;                 // p2 (1/c - p0 / ((p0^2+p0 p2+p3) c / (p2 + 2 p0)))
-  const T log_s = -lr / (T)6 + (T)-0.2387353263835302;    // log(3/(4pi))/6
+  const T log_s = -lr * (T)(1.0 / 6.0) + (T)-0.2387353263835302;    // log(3/(4pi))/6
   const T s = exp(log_s);
   const T X = s * s + p2 * s + p3;
   const T den = (T)2 * s + p2;
   const T z = c / den;
-  const T G = log_s + f * ((T)0.5 * log(X) - ((T)1 / f + (T)1) * log(s - p0)) + pre * atan(z);
-  const T Gp = (T)1 / s + f * (den / ((T)2 * X) - ((T)1 / f + (T)1) / (s - p0)) +
+  const T G = log_s + f * ((T)0.5 * log(X) - (T)(1.0 / -1.0311676086789439 + 1.0) * log(s - p0)) + pre * atan(z);
+  const T Gp = (T)1 / s + f * (den / ((T)2 * X) - (T)(1.0 / -1.0311676086789439 + 1.0) / (s - p0)) +
                pre * ((T)-2 * c / (den * den)) / ((T)1 + z * z);
   const T e_vwn = (T)0.19 * rho * p1 * G;                      // per volume
-  const T v_vwn = (T)0.19 * p1 * (G - s / (T)6 * Gp);
+  const T v_vwn = (T)0.19 * p1 * (G - s * (T)(1.0 / 6.0) * Gp);
 
   B2XcPoint<T> o;
   o.exc = e_vwn * inv_rho;
@@ -114,15 +114,15 @@ B2_HD B2XcPoint<T> b2_b3lyp_lyp(T r0, T r1, T r2, T r3) {
   const T dl = t * (C + D * P);
   const T n53 = t * t * t * t * t;                     // rho^{-5/3}
   const T q = (T)3 + (T)7 * dl;
-  const T R = -A * rho * P - A * B * CF * w * rho + A * B / (T)72 * w * sig * n53 * q;
-  const T i3n = inv_rho / (T)3;
+  const T R = -A * rho * P - A * B * CF * w * rho + (T)(0.04918 * 0.132 / 72.0) * w * sig * n53 * q;
+  const T i3n = inv_rho * (T)(1.0 / 3.0);
   const T Pp = D * P * P * t * i3n;
   const T wp = w * dl * i3n;
   const T dlp = (D * D * P * P * t * t - dl) * i3n;
   const T dRdn = -A * (P + rho * Pp) - A * B * CF * (w + rho * wp) +
-                 A * B * sig / (T)72 *
+                 (T)(0.04918 * 0.132 / 72.0) * sig *
                      (wp * n53 * q - (T)(5.0 / 3.0) * w * n53 * inv_rho * q + (T)7 * w * n53 * dlp);
-  const T dRdg = A * B / (T)72 * w * n53 * q;
+  const T dRdg = (T)(0.04918 * 0.132 / 72.0) * w * n53 * q;
   const T e_lyp = (T)0.81 * R;
   const T v_lyp = (T)0.81 * dRdn;
   const T g_lyp = (T)0.81 * dRdg;
