@@ -37,7 +37,14 @@ static void b2_boys_fill_table(double *table) {
 
 template <typename T> struct B2BoysTerms;
 template <> struct B2BoysTerms<double> { static constexpr int n = 9; };
-template <> struct B2BoysTerms<float> { static constexpr int n = 6; };
+template <> struct B2BoysTerms<float> { static constexpr int n = 5; };   // remainder < 1e-8
+
+// e^{-t}: exact for float64; hardware 2^x for float32 (t < 40: relative error < 1e-6 times
+// a term that the downward recursion adds to F values of order >= e^{-t})
+template <typename T> B2_HD T b2_exp_neg(T t) { return exp(-t); }
+#ifdef __CUDA_ARCH__
+template <> __device__ __forceinline__ float b2_exp_neg<float>(float t) { return __expf(-t); }
+#endif
 
 // F[0..L] at T; `table` is the table in double (float64 kernels) or float (float32 kernels).
 template <typename T, int L, typename TT>
@@ -53,7 +60,7 @@ B2_HD void b2_boys(T t, const TT *__restrict__ table, T *F) {
     for (int j = NT - 1; j >= 1; --j) acc = (T)row[j - 1] + acc * dt * (T)(1.0 / j);
     F[L] = acc;
     if (L > 0) {
-      T et = exp(-t);
+      T et = b2_exp_neg<T>(t);
       T t2 = t + t;
 #pragma unroll
       for (int m = L - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + et) * (T)(1.0 / (2 * m + 1));

@@ -47,7 +47,7 @@ struct B2Shell {               // one contracted shell of one molecule
 // primitive-pair data of a shell pair (bra or ket), precision T
 template <typename T>
 struct B2PairPrim {
-  T zeta, Px, Py, Pz, K, PAx, PAy, PAz, PBx, PBy, PBz, pad;
+  T zeta, Px, Py, Pz, K, PAx, PAy, PAz, PBx, PBy, PBz, h2z;   // h2z = 1 / (2 zeta)
 };
 
 struct B2PairInfo {            // per shell pair

@@ -30,13 +30,13 @@ struct B2Sq {
       const B2PairPrim<T> Q = ket[q];
       if (Q.K == (T)0) break;                 // packed: the rest of the pair is inert
       const T eta = Q.zeta;
-      const T v = b2_div<T>((T)0.5, eta);
+      const T v = Q.h2z;
       const T QC[3] = {Q.PAx, Q.PAy, Q.PAz};
       const T QD[3] = {Q.PBx, Q.PBy, Q.PBz};
       for (int p = 0; p < nb; ++p) {
         const B2PairPrim<T> &Bp = bra[p];
         const T zeta = Bp.zeta;
-        const T u = b2_div<T>((T)0.5, zeta);
+        const T u = Bp.h2z;
         const T sig = zeta + eta;
         const T rho = b2_div<T>(zeta * eta, sig);
         const T X[3] = {Bp.Px - Q.Px, Bp.Py - Q.Py, Bp.Pz - Q.Pz};

@@ -53,7 +53,7 @@ static inline int b2_class(int lK, int lL) { return lK + 2 * lL; }   // ss=0, ps
 // entry (zeta 1, K 0).  Shared by the device plan kernel and the host test build.
 B2_HD void b2_pair_prim(const B2Shell &a, const B2Shell &b, int x, B2PairPrim<double> &q) {
   q.zeta = 1.0; q.Px = q.Py = q.Pz = 0.0; q.K = 0.0;
-  q.PAx = q.PAy = q.PAz = q.PBx = q.PBy = q.PBz = 0.0; q.pad = 0.0;
+  q.PAx = q.PAy = q.PAz = q.PBx = q.PBy = q.PBz = 0.0; q.h2z = 0.5;
   const int pa = x / B2_MAXPRIM, pb = x % B2_MAXPRIM;
   if (pa >= a.nprim || pb >= b.nprim) return;
   const double k0 = 5.914967172795613;           // sqrt(2) pi^(5/4)
@@ -64,7 +64,7 @@ B2_HD void b2_pair_prim(const B2Shell &a, const B2Shell &b, int x, B2PairPrim<do
   for (int d = 0; d < 3; ++d) Pc[d] = (al * a.R[d] + be * b.R[d]) / z;
   double K = a.coef[pa] * b.coef[pb] * exp(-al * be / z * AB2) * k0 / z;
   if (fabs(K) < 1e-300) K = 0;
-  q.zeta = z; q.Px = Pc[0]; q.Py = Pc[1]; q.Pz = Pc[2]; q.K = K;
+  q.zeta = z; q.Px = Pc[0]; q.Py = Pc[1]; q.Pz = Pc[2]; q.K = K; q.h2z = 0.5 / z;
   q.PAx = Pc[0] - a.R[0]; q.PAy = Pc[1] - a.R[1]; q.PAz = Pc[2] - a.R[2];
   q.PBx = Pc[0] - b.R[0]; q.PBy = Pc[1] - b.R[1]; q.PBz = Pc[2] - b.R[2];
 }
@@ -72,7 +72,7 @@ B2_HD void b2_pair_prim(const B2Shell &a, const B2Shell &b, int x, B2PairPrim<do
 B2_HD void b2_pair_prim32(const B2PairPrim<double> &q, B2PairPrim<float> &f) {
   f.zeta = (float)q.zeta; f.Px = (float)q.Px; f.Py = (float)q.Py; f.Pz = (float)q.Pz;
   f.K = (float)q.K; f.PAx = (float)q.PAx; f.PAy = (float)q.PAy; f.PAz = (float)q.PAz;
-  f.PBx = (float)q.PBx; f.PBy = (float)q.PBy; f.PBz = (float)q.PBz; f.pad = 0.f;
+  f.PBx = (float)q.PBx; f.PBy = (float)q.PBy; f.PBz = (float)q.PBz; f.h2z = (float)q.h2z;
 }
 
 // Primitive-pair screening: a primitive pair whose prefactor |K| is below the threshold
