@@ -271,15 +271,17 @@ def main():
     jk_ev[1].record()
     torch.cuda.synchronize()
     jk_ms = jk_ev[0].elapsed_time(jk_ev[1]) / njk
-    jk_bytes = P.n_eri * rbytes
+    # J/K reads the s8 list and the exchange list (same size) once per call
+    nlists = 2 if eng.jk_impl == "pairs" else 1
+    jk_bytes = nlists * P.n_eri * rbytes
     achieved = jk_bytes / (jk_ms / 1000.0) / 1e9
     # DRAM traffic per launch: ncu capture of the same kernel on the 256-molecule batch
-    # (438.9 MB read + 8.7 MB written for 430.4 MB of float32 ERIs),
-    # scaled to this launch by the number of ERIs processed (traffic grows with the list size)
-    traffic = jk_bytes * (447.6 / 430.4) if a.precision == "mixed" else None
-    roofline = {"kernel": "k_jk_s8", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
-                "traffic_source": "ncu 256-molecule capture scaled by ERI count",
+    # (k_symv: 868.3 MB read + 6.7 MB written for 860.8 MB of float32 list entries),
+    # scaled to this launch by the number of entries processed (traffic grows with the lists)
+    traffic = jk_bytes * (875.0 / 860.8) if (a.precision == "mixed" and nlists == 2) else None
+    roofline = {"kernel": "k_symv" if nlists == 2 else "k_jk_s8", "bound": "hbm", "achieved": achieved,
+                "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
+                "traffic_source": "ncu 256-molecule capture scaled by list size",
                 "algorithmic_bytes_per_launch": jk_bytes, "ms_per_launch": jk_ms}
 
     if a.profile_mode:

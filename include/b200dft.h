@@ -87,6 +87,17 @@ int b2_eri_s8(b2_plan_t plan, int precision, void *eri_out, void *stream);
 int b2_jk_s8(b2_plan_t plan, int precision, const int *active, const void *eri, const double *D,
              double *J, double *K, void *stream);
 
+/* Exchange list of a batch's s8 ERI list: H[(il),(jk)] = (ij|kl) + (ik|jl) for pairs i >= l,
+ * j >= k, packed like the s8 list (same offsets and size; precision 64: double, 32: float).
+ * Build once per ERI list; b2_jk_pairs reads both lists.  No counterpart in the reference
+ * (an equivalent regrouping of the sums of sparse_symmetric_ERI.py:86-137). */
+int b2_jk_exchange(b2_plan_t plan, int precision, const void *eri, void *exch, void *stream);
+/* J and K as b2_jk_s8, computed as two symmetric matrix-vector products over the s8 list and
+ * the exchange list (float64 arithmetic, no shared-memory atomics).  Uses a plan-owned
+ * workspace: one call at a time per plan. */
+int b2_jk_pairs(b2_plan_t plan, int precision, const int *active, const void *eri,
+                const void *exch, const double *D, double *J, double *K, void *stream);
+
 /* Register the grid layout: grid_off (host, nmol+1 prefix of per-molecule point counts).
  * Allocates the plan's grid tables and XC scratch on the device. */
 int b2_grid_set(b2_plan_t plan, const int64_t *grid_off);

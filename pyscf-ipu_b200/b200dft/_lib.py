@@ -33,6 +33,8 @@ SIGNATURES = {
     "b2_plan_set_subset": [_P, _P, _I],
     "b2_eri_s8": [_P, _I, _P, _P],
     "b2_jk_s8": [_P, _I, _P, _P, _P, _P, _P, _P],
+    "b2_jk_exchange": [_P, _I, _P, _P, _P],
+    "b2_jk_pairs": [_P, _I, _P, _P, _P, _P, _P, _P, _P],
     "b2_grid_set": [_P, _P],
     "b2_grid_info": [_P, _P, _P],
     "b2_grid_ao_offsets": [_P, _P],

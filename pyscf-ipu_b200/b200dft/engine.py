@@ -179,6 +179,8 @@ class RKSEngine:
             self._tmpl = (tmpl, toff)
             self._setup_done = False
         self.eri = torch.empty(max(1, P.n_eri), dtype=rdt, device=dev)
+        self.eri_x = torch.empty(max(1, P.n_eri), dtype=rdt, device=dev)   # exchange list for J/K
+        self.jk_impl = "pairs"      # "pairs": two products over the s8 and exchange lists; "s8"
         self.ao = None          # (4, G, nao) AO tensor, only for the AO-input XC entry
         self.D, self.J, self.K, self.Vxc = z(nmat), z(nmat), z(nmat), z(nmat)
         self.H, self.diffJK = z(nmat), z(nmat)
@@ -235,6 +237,8 @@ class RKSEngine:
     # --- kernels -----------------------------------------------------------------------
     def compute_eri(self, stream=None):
         check(lib().b2_eri_s8(self.plan.h, self.prec, ptr(self.eri), stream_handle(stream)), "b2_eri_s8")
+        check(lib().b2_jk_exchange(self.plan.h, self.prec, ptr(self.eri), ptr(self.eri_x), stream_handle(stream)),
+              "b2_jk_exchange")
         self._eri_done = True
 
     def compute_ao(self, stream=None):
@@ -248,8 +252,12 @@ class RKSEngine:
 
     def jk(self, D=None, active=None, stream=None):
         D = self.D if D is None else D
-        check(lib().b2_jk_s8(self.plan.h, self.prec, ptr(active), ptr(self.eri), ptr(D), ptr(self.J),
-                             ptr(self.K), stream_handle(stream)), "b2_jk_s8")
+        if self.jk_impl == "s8":
+            check(lib().b2_jk_s8(self.plan.h, self.prec, ptr(active), ptr(self.eri), ptr(D), ptr(self.J),
+                                 ptr(self.K), stream_handle(stream)), "b2_jk_s8")
+        else:
+            check(lib().b2_jk_pairs(self.plan.h, self.prec, ptr(active), ptr(self.eri), ptr(self.eri_x), ptr(D),
+                                    ptr(self.J), ptr(self.K), stream_handle(stream)), "b2_jk_pairs")
 
     def xc(self, D=None, active=None, stream=None):
         """E_xc and V_xc with AO values generated on the fly per grid tile."""

@@ -31,7 +31,7 @@ static int b2_upload(T **dst, const std::vector<T> &src) {
 
 static void b2_subset_free(B2PlanDev *P) {
   cudaFree(P->sub.mol_map); cudaFree(P->sub.jk_off); cudaFree(P->sub.x32); cudaFree(P->sub.x64);
-  cudaFree(P->sub.xtc);
+  cudaFree(P->sub.xtc); cudaFree(P->sub.sv_off);
   P->sub = B2SubsetDev();
 }
 
@@ -44,6 +44,7 @@ static void b2_plan_free(B2PlanDev *P) {
   cudaFree(P->cls_cnt); cudaFree(P->atom_xyz); cudaFree(P->atom_z); cudaFree(P->boys); cudaFree(P->boys32);
   cudaFree(P->jk_chunk_off);
   cudaFree(P->eri_tasks32); cudaFree(P->eri_tasks64);
+  cudaFree(P->sv_off); cudaFree(P->sv_work);
   delete P;
 }
 
@@ -62,6 +63,22 @@ static int b2_set_jk_chunk(B2PlanDev *P, long long elems) {
   P->jk_off_h = off;
   P->jk_chunk = elems;
   P->jk_nchunks = off[nmol];
+  return B2_OK;
+}
+
+// warp-task table of the J/K products and their pair-vector workspace
+static int b2_set_sv(B2PlanDev *P) {
+  const int nmol = P->h.nmol;
+  std::vector<long long> off(nmol + 1, 0);
+  for (int m = 0; m < nmol; ++m) {
+    const long long N = P->h.mols[m].nao;
+    off[m + 1] = off[m] + b2_sv_tasks_host(N * (N + 1) / 2);
+  }
+  int rc = b2_upload(&P->sv_off, off);
+  if (rc) return rc;
+  P->sv_off_h = off;
+  P->sv_ntask = off[nmol];
+  B2_TRY(cudaMalloc(&P->sv_work, sizeof(double) * 4 * (size_t)std::max(1ll, P->h.n_rows)));
   return B2_OK;
 }
 
@@ -92,7 +109,7 @@ int b2_plan_create(int nmol, const int *natm, const int *nbas, const int *atm, c
       (rc = b2_upload(&P->cls_cnt, P->h.cls_cnt)) || (rc = b2_upload(&P->atom_xyz, P->h.atom_xyz)) ||
       (rc = b2_upload(&P->atom_z, P->h.atom_z)) || (rc = b2_upload(&P->boys, tab)) ||
       (rc = b2_upload(&P->boys32, std::vector<float>(tab.begin(), tab.end()))) ||
-      (rc = b2_set_jk_chunk(P, 0)) || (rc = b2_build_pairs(*P))) {
+      (rc = b2_set_jk_chunk(P, 0)) || (rc = b2_build_pairs(*P)) || (rc = b2_set_sv(P))) {
     b2_plan_free(P);
     return rc;
   }
@@ -159,7 +176,7 @@ int b2_plan_set_subset(void *plan, const int *mols, int n) {
   if (n == 0) return B2_OK;
   if (P->g.xblk32_h.empty()) return B2_ERR_ARG;
   std::vector<int> map(mols, mols + n);
-  std::vector<long long> jo(n + 1, 0), x3(n + 1, 0), x6(n + 1, 0), xt(n + 1, 0);
+  std::vector<long long> jo(n + 1, 0), x3(n + 1, 0), x6(n + 1, 0), xt(n + 1, 0), so(n + 1, 0);
   for (int k = 0; k < n; ++k) {
     const int m = map[k];
     if (m < 0 || m >= P->h.nmol) return B2_ERR_ARG;
@@ -167,11 +184,12 @@ int b2_plan_set_subset(void *plan, const int *mols, int n) {
     x3[k + 1] = x3[k] + (P->g.xblk32_h[m + 1] - P->g.xblk32_h[m]);
     x6[k + 1] = x6[k] + (P->g.xblk64_h[m + 1] - P->g.xblk64_h[m]);
     xt[k + 1] = xt[k] + (P->g.xblk_tc_h[m + 1] - P->g.xblk_tc_h[m]);
+    so[k + 1] = so[k] + (P->sv_off_h[m + 1] - P->sv_off_h[m]);
   }
   int rc;
   if ((rc = b2_upload(&P->sub.mol_map, map)) || (rc = b2_upload(&P->sub.jk_off, jo)) ||
       (rc = b2_upload(&P->sub.x32, x3)) || (rc = b2_upload(&P->sub.x64, x6)) ||
-      (rc = b2_upload(&P->sub.xtc, xt))) {
+      (rc = b2_upload(&P->sub.xtc, xt)) || (rc = b2_upload(&P->sub.sv_off, so))) {
     b2_subset_free(P);
     return rc;
   }
@@ -180,6 +198,7 @@ int b2_plan_set_subset(void *plan, const int *mols, int n) {
   P->sub.n_x32 = x3[n];
   P->sub.n_x64 = x6[n];
   P->sub.n_xtc = xt[n];
+  P->sub.sv_n = so[n];
   return B2_OK;
 }
 
@@ -188,6 +207,18 @@ int b2_eri_s8(void *plan, int precision, void *eri_out, void *stream) {
   int rc = b2_launch_eri_s8(*(B2PlanDev *)plan, precision, eri_out, (cudaStream_t)stream);
   if (rc == B2_ERR_CUDA) b2_note(cudaGetLastError());
   return rc;
+}
+
+int b2_jk_exchange(void *plan, int precision, const void *eri, void *exch, void *stream) {
+  if (!plan || !eri || !exch) return B2_ERR_ARG;
+  return b2_launch_exch_build(*(B2PlanDev *)plan, precision, eri, exch, (cudaStream_t)stream);
+}
+
+int b2_jk_pairs(void *plan, int precision, const int *active, const void *eri, const void *exch,
+                const double *D, double *J, double *K, void *stream) {
+  if (!plan || !eri || !exch || !D || !J || !K) return B2_ERR_ARG;
+  B2PlanDev *P = (B2PlanDev *)plan;
+  return b2_launch_jk_symv(*P, precision, active, eri, exch, D, J, K, P->sv_work, (cudaStream_t)stream);
 }
 
 int b2_jk_s8(void *plan, int precision, const int *active, const void *eri, const double *D,

@@ -22,8 +22,8 @@ struct B2GridDev {             // grid layout registered with b2_grid_set
 struct B2SubsetDev {           // compacted work tables for a subset of the batch's molecules
   int n = 0;                   // 0: no subset (full tables)
   int *mol_map = nullptr;      // compacted index -> molecule
-  long long *jk_off = nullptr, *x32 = nullptr, *x64 = nullptr, *xtc = nullptr;
-  long long jk_n = 0, n_x32 = 0, n_x64 = 0, n_xtc = 0;
+  long long *jk_off = nullptr, *x32 = nullptr, *x64 = nullptr, *xtc = nullptr, *sv_off = nullptr;
+  long long jk_n = 0, n_x32 = 0, n_x64 = 0, n_xtc = 0, sv_n = 0;
 };
 
 struct B2PlanDev {
@@ -51,10 +51,19 @@ struct B2PlanDev {
   std::vector<long long> jk_off_h;                 // host copy of jk_chunk_off
   B2SubsetDev sub;
   int xc_impl = 0;             // float32 XC: 0 = tensor-core kernel, 1 = SIMT kernel
+  long long *sv_off = nullptr;            // nmol + 1: warp tasks of the J/K products per molecule
+  std::vector<long long> sv_off_h;
+  long long sv_ntask = 0;
+  double *sv_work = nullptr;              // 4 x n_rows: x_J, x_K, y_J, y_K
 };
 
 int b2_launch_eri_s8(B2PlanDev &P, int precision, void *out, cudaStream_t st);
 int b2_build_pairs(B2PlanDev &P);
+int b2_launch_exch_build(const B2PlanDev &P, int precision, const void *eri, void *exch, cudaStream_t st);
+int b2_launch_jk_symv(const B2PlanDev &P, int precision, const int *active, const void *eri,
+                      const void *exch, const double *D, double *J, double *K, double *work,
+                      cudaStream_t st);
+long long b2_sv_tasks_host(long long n2);
 int b2_launch_jk_s8(const B2PlanDev &P, int precision, const int *active, const void *eri,
                     const double *D, double *J, double *K, cudaStream_t st);
 int b2_zero_active(const B2PlanDev &P, const int *active, double *A, double *B, cudaStream_t st);

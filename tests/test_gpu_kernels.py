@@ -101,6 +101,49 @@ def test_jk_parity(cuda, prec):
             np.testing.assert_allclose(P.unpack(Kh, mi), Kr, atol=tol)
 
 
+@pytest.mark.parametrize("prec", [64, 32])
+def test_jk_pairs_parity(cuda, prec):
+    # J/K as two products over the s8 list and the exchange list, vs the s8 semantics oracle;
+    # inactive molecules keep their previous J/K
+    mols, gs = _mols()
+    P, v = _eri(mols, prec, cuda, raw=True)
+    dt = torch.float64 if prec == 64 else torch.float32
+    eri_t = torch.from_numpy(v).to(cuda).to(dt)
+    exch = torch.full_like(eri_t, float("nan"))
+    check(lib().b2_jk_exchange(P.h, prec, ptr(eri_t), ptr(exch), stream_handle()), "exchange")
+    rng = np.random.default_rng(1)
+    Ds = [_sym_random(m.nao, rng) for m in mols]
+    D = torch.from_numpy(P.pack(Ds)).to(cuda)
+    J = torch.full((P.n_mat,), 7.0, dtype=torch.float64, device=cuda)
+    K = torch.full_like(J, 7.0)
+    active = torch.tensor([1, 0, 1, 1], dtype=torch.int32, device=cuda)
+    check(lib().b2_jk_pairs(P.h, prec, ptr(active), ptr(eri_t), ptr(exch), ptr(D), ptr(J), ptr(K),
+                            stream_handle()), "jk_pairs")
+    torch.cuda.synchronize()
+    Jh, Kh = J.cpu().numpy(), K.cpu().numpy()
+    for mi, (m, g) in enumerate(zip(mols, gs)):
+        if mi == 1:
+            assert np.all(P.unpack(Jh, mi) == 7.0) and np.all(P.unpack(Kh, mi) == 7.0)
+            continue
+        _, Jr, Kr = rks.jk_from_s8(Ds[mi], g["s8"], m.nao)
+        tol = 1e-10 if prec == 64 else 2e-5 * max(1.0, np.abs(Jr).max())
+        np.testing.assert_allclose(P.unpack(Jh, mi), Jr, atol=tol)
+        np.testing.assert_allclose(P.unpack(Kh, mi), Kr, atol=tol)
+    # exchange list entries: H[(il),(jk)] = (ij|kl) + (ik|jl)
+    m, g = mols[2], gs[2]
+    N = m.nao
+    full = oeri.unpack_s8(g["s8"], N)
+    o = int(P.eri_off[2])
+    X = exch[o:o + oeri.n_s8(N)].double().cpu().numpy()
+    pr = [(i, l) for i in range(N) for l in range(i + 1)]
+    e = 0
+    for a, (i, l) in enumerate(pr):
+        for (j, k) in pr[:a + 1]:
+            ref = full[i, j, k, l] + full[i, k, j, l]
+            assert abs(X[e] - ref) <= (1e-12 if prec == 64 else 1e-6) * max(1.0, abs(ref))
+            e += 1
+
+
 def test_ao_eval_and_xc(cuda):
     mols = [Mole(methane()), Mole("O 0 0 0.1173; H 0 0.7572 -0.4692; H 0 -0.7572 -0.4692")]
     eng = RKSEngine(mols, level=0, precision="fp64", setups=[HostSetup(m, 0) for m in mols])
