@@ -25,9 +25,8 @@
 //   * D: [k chunk][row group][row % 8][k % 4]; SBO 128 B, LBO (NB/8)*128 B.
 //   * T tile (K = points): AO0^T and Y^T for V = AO0^T Y, [point chunk p/4][row group r/8]
 //     [r % 8][p % 4]; SBO 128 B between row groups, LBO = (rows/8)*128 + 16 B between point
-//     chunks (the extra 16 B staggers the chunks across shared-memory banks).  Threads hold
-//     a point's orbitals, so a 4 x 4 shuffle transpose between the lanes of 4 consecutive
-//     points turns 4 orbitals x 1 point into 1 orbital x 4 points before each 16-byte store.
+//     chunks (the extra 16 B staggers the chunks across shared-memory banks, so the 32 lanes
+//     of a warp -- 32 consecutive points -- storing one orbital hit 32 different banks).
 // Y^T reuses the N tile's bytes once X has been read back.
 //
 // Thread layout: 512 threads = 4 per grid point.  Warp w reads TMEM lanes 32*(w%4)..+31
@@ -142,22 +141,6 @@ __device__ __forceinline__ int b2_tile_idx(int p, int n) {
 __host__ __device__ constexpr int b2_lt(int R) { return (R / 8) * 128 + 16; }
 __device__ __forceinline__ int b2_tt_idx(int R, int r, int pc) {
   return (pc * b2_lt(R) + (r >> 3) * 128 + (r & 7) * 16) >> 2;
-}
-// 4 x 4 transpose among the 4 lanes of a point quad: in v[j] = orbital j of this lane's point,
-// out v[j] = this lane's orbital (lane % 4) at point (quad base + j)
-__device__ __forceinline__ void b2_quad_transpose(float *v) {
-  const int i = threadIdx.x & 3;
-  float o[4] = {v[0], v[1], v[2], v[3]};           // o[i] keeps this lane's own value
-#pragma unroll
-  for (int r = 1; r < 4; ++r) {
-    const int send = (i - r) & 3;                  // receiver (i + r) & 3 wants our v[its i]
-    const float x = send == 0 ? v[0] : send == 1 ? v[1] : send == 2 ? v[2] : v[3];
-    const float got = __shfl_sync(0xffffffffu, x, (threadIdx.x & ~3) | ((i + r) & 3));
-    const int j = (i + r) & 3;
-    if (j == 0) o[0] = got; else if (j == 1) o[1] = got; else if (j == 2) o[2] = got; else o[3] = got;
-  }
-#pragma unroll
-  for (int j = 0; j < 4; ++j) v[j] = o[j];
 }
 
 // 4-register TMEM load (this thread's lane, 4 consecutive columns)
@@ -285,13 +268,11 @@ __device__ void b2_xt_body(const B2MolDev &md, const B2XtOrb *sOrb, const double
       for (int u = 0; u < 4; ++u) b2_split_rn(a0[u], hi[u], lo[u]);
       b2_st4(sAh + b2_tile_idx(p, n0), hi[0], hi[1], hi[2], hi[3]);
       b2_st4(sAl + b2_tile_idx(p, n0), lo[0], lo[1], lo[2], lo[3]);
-      b2_quad_transpose(a0);                        // a0[j] = orbital n0 + p%4 at point 4(p/4)+j
 #pragma unroll
-      for (int u = 0; u < 4; ++u) b2_split_rn(a0[u], hi[u], lo[u]);
-      {
-        const int it = b2_tt_idx(OB, n0 + (p & 3), p >> 2);
-        b2_st4(sTh + it, hi[0], hi[1], hi[2], hi[3]);
-        b2_st4(sTl + it, lo[0], lo[1], lo[2], lo[3]);
+      for (int u = 0; u < 4; ++u) {                 // T tile: one float per orbital (conflict-free)
+        const int it = b2_tt_idx(OB, n0 + u, p >> 2) + (p & 3);
+        sTh[it] = hi[u];
+        sTl[it] = lo[u];
       }
       b2_tmem_st4(tl + colA + n0, a1[0], a1[1], a1[2], a1[3]);
       b2_tmem_st4(tl + colA + NB + n0, a2[0], a2[1], a2[2], a2[3]);
@@ -395,12 +376,13 @@ __device__ void b2_xt_body(const B2MolDev &md, const B2XtOrb *sOrb, const double
       for (int u = 0; u < 4; ++u)
         y[u] = av[u] * rt0 + __uint_as_float(b1[u]) * rt1 + __uint_as_float(b2[u]) * rt2 +
                __uint_as_float(b3[u]) * rt3;
-      b2_quad_transpose(y);
 #pragma unroll
-      for (int u = 0; u < 4; ++u) b2_split_rn(y[u], yh[u], yl[u]);
-      const int it = b2_tt_idx(NB, n0 + (p & 3), p >> 2);
-      b2_st4(sYh + it, yh[0], yh[1], yh[2], yh[3]);
-      b2_st4(sYl + it, yl[0], yl[1], yl[2], yl[3]);
+      for (int u = 0; u < 4; ++u) {
+        b2_split_rn(y[u], yh[u], yl[u]);
+        const int it = b2_tt_idx(NB, n0 + u, p >> 2) + (p & 3);
+        sYh[it] = yh[u];
+        sYl[it] = yl[u];
+      }
     }
     b2_fence_async_smem();
     b2_fence_before();
