@@ -31,7 +31,7 @@ static int b2_upload(T **dst, const std::vector<T> &src) {
 
 static void b2_subset_free(B2PlanDev *P) {
   cudaFree(P->sub.mol_map); cudaFree(P->sub.jk_off); cudaFree(P->sub.x32); cudaFree(P->sub.x64);
-  cudaFree(P->sub.xtc); cudaFree(P->sub.sv_off);
+  cudaFree(P->sub.xtc); cudaFree(P->sub.sv_off); cudaFree(P->sub.bkt_map);
   P->sub = B2SubsetDev();
 }
 
@@ -44,7 +44,9 @@ static void b2_plan_free(B2PlanDev *P) {
   cudaFree(P->cls_cnt); cudaFree(P->atom_xyz); cudaFree(P->atom_z); cudaFree(P->boys); cudaFree(P->boys32);
   cudaFree(P->jk_chunk_off);
   cudaFree(P->eri_tasks32); cudaFree(P->eri_tasks64);
-  cudaFree(P->sv_off); cudaFree(P->sv_work);
+  cudaFree(P->sv_off); cudaFree(P->sv_work); cudaFree(P->bkt_map);
+  for (int b = 0; b < B2_NBKT; ++b) if (P->bkt_stream[b]) cudaStreamDestroy(P->bkt_stream[b]);
+  for (int b = 0; b <= B2_NBKT; ++b) if (P->bkt_ev[b]) cudaEventDestroy(P->bkt_ev[b]);
   delete P;
 }
 
@@ -66,6 +68,18 @@ static int b2_set_jk_chunk(B2PlanDev *P, long long elems) {
   return B2_OK;
 }
 
+// molecules (a list of indices) grouped by orbital bucket, order kept within a bucket
+static void b2_buckets(const B2PlanDev *P, const std::vector<int> &mols, std::vector<int> &map,
+                       std::vector<int> &off) {
+  off.assign(B2_NBKT + 1, 0);
+  auto bkt = [&](int m) { return std::min(B2_NBKT - 1, (P->h.mols[m].nao - 1) / 16); };
+  for (int m : mols) ++off[bkt(m) + 1];
+  for (int b = 0; b < B2_NBKT; ++b) off[b + 1] += off[b];
+  map.assign(mols.size(), 0);
+  std::vector<int> pos(off.begin(), off.end() - 1);
+  for (int m : mols) map[pos[bkt(m)]++] = m;
+}
+
 // warp-task table of the J/K products and their pair-vector workspace
 static int b2_set_sv(B2PlanDev *P) {
   const int nmol = P->h.nmol;
@@ -79,7 +93,12 @@ static int b2_set_sv(B2PlanDev *P) {
   P->sv_off_h = off;
   P->sv_ntask = off[nmol];
   B2_TRY(cudaMalloc(&P->sv_work, sizeof(double) * 4 * (size_t)std::max(1ll, P->h.n_rows)));
-  return B2_OK;
+  std::vector<int> all(nmol), map;
+  for (int m = 0; m < nmol; ++m) all[m] = m;
+  b2_buckets(P, all, map, P->bkt_off_h);
+  for (int b = 0; b < B2_NBKT; ++b) B2_TRY(cudaStreamCreateWithFlags(&P->bkt_stream[b], cudaStreamNonBlocking));
+  for (int b = 0; b <= B2_NBKT; ++b) B2_TRY(cudaEventCreateWithFlags(&P->bkt_ev[b], cudaEventDisableTiming));
+  return b2_upload(&P->bkt_map, map);
 }
 
 extern "C" {
@@ -199,6 +218,12 @@ int b2_plan_set_subset(void *plan, const int *mols, int n) {
   P->sub.n_x64 = x6[n];
   P->sub.n_xtc = xt[n];
   P->sub.sv_n = so[n];
+  std::vector<int> bmap;
+  b2_buckets(P, map, bmap, P->sub.bkt_off_h);
+  if ((rc = b2_upload(&P->sub.bkt_map, bmap))) {
+    b2_subset_free(P);
+    return rc;
+  }
   return B2_OK;
 }
 

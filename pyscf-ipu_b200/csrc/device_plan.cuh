@@ -19,9 +19,13 @@ struct B2GridDev {             // grid layout registered with b2_grid_set
   std::vector<long long> grid_off_h, ao_off_h, xblk32_h, xblk64_h, xblk_tc_h;
 };
 
+#define B2_NBKT 5              // orbital buckets nao <= 16, 32, 48, 64, more
+
 struct B2SubsetDev {           // compacted work tables for a subset of the batch's molecules
   int n = 0;                   // 0: no subset (full tables)
   int *mol_map = nullptr;      // compacted index -> molecule
+  int *bkt_map = nullptr;      // the subset's molecules by orbital bucket
+  std::vector<int> bkt_off_h;  // B2_NBKT + 1
   long long *jk_off = nullptr, *x32 = nullptr, *x64 = nullptr, *xtc = nullptr, *sv_off = nullptr;
   long long jk_n = 0, n_x32 = 0, n_x64 = 0, n_xtc = 0, sv_n = 0;
 };
@@ -55,6 +59,10 @@ struct B2PlanDev {
   std::vector<long long> sv_off_h;
   long long sv_ntask = 0;
   double *sv_work = nullptr;              // 4 x n_rows: x_J, x_K, y_J, y_K
+  int *bkt_map = nullptr;                 // molecules ordered by orbital bucket
+  std::vector<int> bkt_off_h;             // B2_NBKT + 1 bucket starts in bkt_map
+  cudaStream_t bkt_stream[B2_NBKT] = {};  // per-bucket streams (forked from / joined to the caller's)
+  cudaEvent_t bkt_ev[B2_NBKT + 1] = {};
 };
 
 int b2_launch_eri_s8(B2PlanDev &P, int precision, void *out, cudaStream_t st);

@@ -133,26 +133,40 @@ __device__ int b2_jacobi(double *A, double *V, int n, int nreal, double *rot, in
   return sweep;
 }
 
-// serial Jacobi for the small DIIS matrix (n <= 10), thread-local
-__device__ void b2_jacobi_small(double *A, double *V, int n) {
-  for (int i = 0; i < n * n; ++i) V[i] = (i / n == i % n) ? 1.0 : 0.0;
+// cyclic Jacobi on the 10 x 10 DIIS matrix A (shared memory, row-major) run by one warp; V <- the
+// eigenvectors.  Each rotation (p, q) is a row phase (rows p, q) then a column phase (columns
+// p, q, and V); both are independent across k, so lane k < 10 does element k of each phase with
+// the arithmetic of the one-thread loop: the result is identical to the serial sweep order.
+// The convergence norm is summed serially by lane 0 (same order) and broadcast.
+__device__ void b2_jacobi_small_warp(double *A, double *V) {
+  constexpr int n = 10;
+  const int k = threadIdx.x & 31;
+  if (k < n)
+    for (int j = 0; j < n; ++j) V[k * n + j] = (k == j) ? 1.0 : 0.0;
+  __syncwarp();
   for (int sweep = 0; sweep < 50; ++sweep) {
-    double off = 0, tot = 0;
-    for (int i = 0; i < n * n; ++i) { tot += A[i] * A[i]; if (i / n != i % n) off += A[i] * A[i]; }
-    if (off <= 1e-28 * tot || off < 1e-300) break;
+    int done = 0;
+    if (k == 0) {
+      double off = 0, tot = 0;
+      for (int i = 0; i < n * n; ++i) { tot += A[i] * A[i]; if (i / n != i % n) off += A[i] * A[i]; }
+      done = (off <= 1e-28 * tot || off < 1e-300);
+    }
+    if (__shfl_sync(0xffffffffu, done, 0)) break;
     for (int p = 0; p < n - 1; ++p)
       for (int q = p + 1; q < n; ++q) {
-        const double apq = A[p * n + q];
-        if (fabs(apq) <= 1e-300 || fabs(apq) < 1e-18 * sqrt(fabs(A[p * n + p] * A[q * n + q]))) continue;
+        const double apq = A[p * n + q], app = A[p * n + p], aqq = A[q * n + q];
+        if (fabs(apq) <= 1e-300 || fabs(apq) < 1e-18 * sqrt(fabs(app * aqq))) continue;
         double c, s;
-        b2_schur2(A[p * n + p], A[q * n + q], apq, c, s);
+        b2_schur2(app, aqq, apq, c, s);
         if (s == 0.0) continue;
-        for (int k = 0; k < n; ++k) {
+        __syncwarp();
+        if (k < n) {
           const double apk = A[p * n + k], aqk = A[q * n + k];
           A[p * n + k] = c * apk - s * aqk;
           A[q * n + k] = s * apk + c * aqk;
         }
-        for (int k = 0; k < n; ++k) {
+        __syncwarp();
+        if (k < n) {
           const double akp = A[k * n + p], akq = A[k * n + q];
           A[k * n + p] = c * akp - s * akq;
           A[k * n + q] = s * akp + c * akq;
@@ -160,6 +174,7 @@ __device__ void b2_jacobi_small(double *A, double *V, int n) {
           V[k * n + p] = c * vkp - s * vkq;
           V[k * n + q] = s * vkp + c * vkq;
         }
+        __syncwarp();
       }
   }
 }
@@ -172,13 +187,14 @@ k_fock_diis(const B2MolDev *__restrict__ mols, const int *__restrict__ active,
             const double *__restrict__ S, const double *__restrict__ D, const double *__restrict__ J,
             const double *__restrict__ K, const double *__restrict__ Vxc, double *__restrict__ H,
             double *__restrict__ diffJK, double *__restrict__ ring_err, double *__restrict__ ring_h,
-            double *__restrict__ Bmat, double *__restrict__ diis_err) {
-  const int m = blockIdx.x;
+            double *__restrict__ Bmat, double *__restrict__ diis_err, const int *__restrict__ map) {
+  const int m = map ? map[blockIdx.x] : blockIdx.x;
   if (active && !active[m]) return;
   extern __shared__ double sm[];
   __shared__ double red[32];
   __shared__ double sc[10];
   __shared__ double stmp[9];
+  __shared__ double sA[100], sV[100];
   const B2MolDev md = mols[m];
   const int N = md.nao, NN = N * N;
   const long long mo = md.mat_off;
@@ -222,32 +238,37 @@ k_fock_diis(const B2MolDev *__restrict__ mols, const int *__restrict__ active,
     if (threadIdx.x == 0) stmp[k] = (k < nfill) ? s : 0.0;
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {
+    const int l = threadIdx.x;
     double *B = Bmat + (long long)m * 100;
-    if (it == 0) {
-      for (int i = 0; i < 100; ++i) B[i] = 0;
-      for (int i = 1; i < 10; ++i) { B[i] = 1; B[i * 10] = 1; }
+    if (l < 10) {
+      if (it == 0)
+        for (int j = 0; j < 10; ++j) B[l * 10 + j] = (l == 0) == (j == 0) ? 0.0 : 1.0;
     }
-    for (int k = 0; k < nd; ++k) { B[(head + 1) * 10 + 1 + k] = stmp[k]; B[(1 + k) * 10 + head + 1] = stmp[k]; }
-    double A[100], V[100];
-    double mask[10];
-    mask[0] = 1;
-    for (int k = 0; k < nd; ++k) mask[k + 1] = (k < nfill) ? 1.0 : 0.0;
-    for (int i = 0; i < 10; ++i)
-      for (int j = 0; j < 10; ++j) A[i * 10 + j] = B[i * 10 + j] * mask[i] * mask[j];
-    b2_jacobi_small(A, V, 10);
+    __syncwarp();
+    if (l < nd) { B[(head + 1) * 10 + 1 + l] = stmp[l]; B[(1 + l) * 10 + head + 1] = stmp[l]; }
+    __syncwarp();
+    // masked copy: rows/columns of unfilled ring slots are zero
+    for (int i = l; i < 100; i += 32) {
+      const int r = i / 10, c = i - r * 10;
+      const bool keep = (r == 0 || r - 1 < nfill) && (c == 0 || c - 1 < nfill);
+      sA[i] = keep ? B[i] : 0.0;
+    }
+    __syncwarp();
+    b2_jacobi_small_warp(sA, sV);
+    __syncwarp();
     double smax = 0;
-    for (int i = 0; i < 10; ++i) smax = fmax(smax, fabs(A[i * 10 + i]));
+    for (int i = 0; i < 10; ++i) smax = fmax(smax, fabs(sA[i * 10 + i]));
     const double cut = 10.0 * 10.0 * 2.220446049250313e-16 * smax;
-    for (int j = 0; j < 10; ++j) {
+    if (l < 10) {
       double c = 0;
       for (int k = 0; k < 10; ++k) {
-        const double lam = A[k * 10 + k];
-        if (fabs(lam) > cut) c += V[0 * 10 + k] * V[j * 10 + k] / lam;
+        const double lam = sA[k * 10 + k];
+        if (fabs(lam) > cut) c += sV[0 * 10 + k] * sV[l * 10 + k] / lam;
       }
-      sc[j] = c;
+      sc[l] = c;
     }
-    diis_err[m] = emax;
+    if (l == 0) diis_err[m] = emax;
   }
   __syncthreads();
   for (int e = threadIdx.x; e < NN; e += blockDim.x) {
@@ -266,8 +287,9 @@ __global__ void __launch_bounds__(256)
 k_eigh_density(const B2MolDev *__restrict__ mols, const int *__restrict__ active,
                const int *__restrict__ iter, const double *__restrict__ H,
                const double *__restrict__ Linv, double *__restrict__ D, double *__restrict__ mo_energy,
-               double *__restrict__ C, double *__restrict__ ws, int *__restrict__ sweeps) {
-  const int m = blockIdx.x;
+               double *__restrict__ C, double *__restrict__ ws, int *__restrict__ sweeps,
+               const int *__restrict__ map) {
+  const int m = map ? map[blockIdx.x] : blockIdx.x;
   if (active && !active[m]) return;
   extern __shared__ double sm[];
   __shared__ double red[32];
@@ -439,29 +461,52 @@ __global__ void k_chol_inv(const B2MolDev *__restrict__ mols, const double *__re
 static size_t b2_fock_smem(int N) { return sizeof(double) * 4 * N * N; }
 static size_t b2_eigh_smem(int N) { int n = (N + 1) & ~1; return sizeof(double) * (2 * N * N + 2 * n * (n + 1)); }
 
+// One launch per orbital bucket (nao <= 16, 32, 48, 64, more) with shared memory sized for that
+// bucket, so small molecules run several CTAs per SM.  The bucket launches go to the plan's
+// bucket streams, forked from and joined back to the caller's stream with events, so they run
+// concurrently (a serial sequence of launches would leave the GPU idle at each launch's tail).
+template <typename F>
+static int b2_per_bucket(const B2PlanDev &P, cudaStream_t st, F launch) {
+  const bool sub = P.sub.n > 0;
+  const std::vector<int> &off = sub ? P.sub.bkt_off_h : P.bkt_off_h;
+  const int *map = sub ? P.sub.bkt_map : P.bkt_map;
+  B2_CUDA_TRY(cudaEventRecord(P.bkt_ev[B2_NBKT], st));
+  for (int b = B2_NBKT - 1; b >= 0; --b) {          // largest molecules first
+    const int n = off[b + 1] - off[b];
+    if (n <= 0) continue;
+    const int N = std::min(P.h.max_nao, 16 * (b + 1));
+    B2_CUDA_TRY(cudaStreamWaitEvent(P.bkt_stream[b], P.bkt_ev[B2_NBKT], 0));
+    launch(N, n, map + off[b], P.bkt_stream[b]);
+    b2_count_launches(1);
+    B2_CUDA_TRY(cudaGetLastError());
+    B2_CUDA_TRY(cudaEventRecord(P.bkt_ev[b], P.bkt_stream[b]));
+    B2_CUDA_TRY(cudaStreamWaitEvent(st, P.bkt_ev[b], 0));
+  }
+  return B2_OK;
+}
+
 int b2_launch_fock_diis(const B2PlanDev &P, const int *active, const int *iter, double hyb,
                         int use_diis, const double *Hcore, const double *S, const double *D,
                         const double *J, const double *K, const double *Vxc, double *H,
                         double *diffJK, double *ring_err, double *ring_h, double *Bmat,
                         double *diis_err, cudaStream_t st) {
-  size_t sm = b2_fock_smem(P.h.max_nao);
-  B2_CUDA_TRY(cudaFuncSetAttribute(k_fock_diis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  k_fock_diis<<<P.h.nmol, 256, sm, st>>>(P.mols, active, iter, hyb, use_diis, Hcore, S, D, J, K,
-                                          Vxc, H, diffJK, ring_err, ring_h, Bmat, diis_err);
-                                          b2_count_launches(1);
-  B2_CUDA_TRY(cudaGetLastError());
-  return B2_OK;
+  B2_CUDA_TRY(cudaFuncSetAttribute(k_fock_diis, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)b2_fock_smem(P.h.max_nao)));
+  return b2_per_bucket(P, st, [&](int N, int n, const int *map, cudaStream_t s) {
+    k_fock_diis<<<n, 256, b2_fock_smem(N), s>>>(P.mols, active, iter, hyb, use_diis, Hcore, S, D, J, K,
+                                                Vxc, H, diffJK, ring_err, ring_h, Bmat, diis_err, map);
+  });
 }
 
 int b2_launch_eigh_density(const B2PlanDev &P, const int *active, const int *iter, const double *H,
                            const double *Linv, double *D, double *mo_energy, double *C, double *ws,
                            int *sweeps, cudaStream_t st) {
-  size_t sm = b2_eigh_smem(P.h.max_nao);
-  B2_CUDA_TRY(cudaFuncSetAttribute(k_eigh_density, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-  k_eigh_density<<<P.h.nmol, 256, sm, st>>>(P.mols, active, iter, H, Linv, D, mo_energy, C, ws, sweeps);
-  b2_count_launches(1);
-  B2_CUDA_TRY(cudaGetLastError());
-  return B2_OK;
+  B2_CUDA_TRY(cudaFuncSetAttribute(k_eigh_density, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)b2_eigh_smem(P.h.max_nao)));
+  return b2_per_bucket(P, st, [&](int N, int n, const int *map, cudaStream_t s) {
+    k_eigh_density<<<n, 256, b2_eigh_smem(N), s>>>(P.mols, active, iter, H, Linv, D, mo_energy, C, ws,
+                                                   sweeps, map);
+  });
 }
 
 int b2_launch_energy(const B2PlanDev &P, const int *active, const double *D, const double *Hcore,
