@@ -169,7 +169,9 @@ class RKSEngine:
         else:
             tmpl, toff = grid_templates(level)
             cnt = toff[1:] - toff[:-1]
-            P.set_grid([int(sum(cnt[int(q)] for q in m.charges)) for m in self.mols])
+            zall = np.concatenate([np.asarray(m.charges, np.int64) for m in self.mols])
+            owner = np.repeat(np.arange(nm), [m.natm for m in self.mols])
+            P.set_grid(np.bincount(owner, weights=cnt[zall], minlength=nm).astype(np.int64))
             self.S, self.T, self.V = z(nmat), z(nmat), z(nmat)
             self.Hcore, self.Linv, self.D0 = z(nmat), z(nmat), z(nmat)
             self.coords = z(3 * P.n_points)
@@ -201,6 +203,9 @@ class RKSEngine:
         self.guess = guess                  # "minao" or "learned"
         self.net = net
         self.D0_minao = None
+        self._guess_pending = False
+        self._guess_after = self._guess_done = None
+        self._side = None                   # side stream of the learned guess
         self.graph_replays = 0              # kernels replayed from graphs are not in launch_count()
         self._captured = 0
         self.graph_kernels_per_step = 0
@@ -221,15 +226,37 @@ class RKSEngine:
         check(lib().b2_chol_inv(P.h, ptr(self.S), ptr(self.Linv), ptr(self.chol_status), s), "b2_chol_inv")
         self._setup_done = True
         if self.guess == "learned":
+            # the network runs after these kernels on a side stream, started by compute_eri
+            # once the ERI kernels are queued (its host-side graph build then overlaps them)
+            # or by initial(), whichever comes first
+            cur = torch.cuda.current_stream(self.device)
+            self._guess_after = cur.record_event()
+            self._guess_pending = True
+
+    def _start_guess(self):
+        """queue a pending learned guess on a high-priority side stream after the setup kernels"""
+        if not self._guess_pending:
+            return
+        self._guess_pending = False
+        if self._side is None:
+            self._side = torch.cuda.Stream(self.device, priority=-1)
+        self._side.wait_event(self._guess_after)
+        if self.D0_minao is None:
+            self.D0_minao = torch.empty_like(self.D0)
+        with torch.cuda.stream(self._side):
             self.apply_learned_guess()
+        self._guess_done = self._side.record_event()
 
     def apply_learned_guess(self):
-        """D0 <- network prediction (MINAO kept as the fallback)"""
+        """D0 <- network prediction (MINAO kept as the fallback), on the current stream"""
         from .learned import Batch
         if self.net is None:
             from .train_guess import load
             self.net = load(device=self.device)
-        self.D0_minao = self.D0.clone()
+        if self.D0_minao is None:
+            self.D0_minao = self.D0.clone()
+        else:
+            self.D0_minao.copy_(self.D0)
         if not hasattr(self, "_nn_batch"):
             self._nn_batch = Batch(self.mols, device=self.device, mat_off=self.plan.mat_off, nao=self.plan.nao)
         self.net.predict(self._nn_batch, self.D0)
@@ -240,6 +267,7 @@ class RKSEngine:
         check(lib().b2_jk_exchange(self.plan.h, self.prec, ptr(self.eri), ptr(self.eri_x), stream_handle(stream)),
               "b2_jk_exchange")
         self._eri_done = True
+        self._start_guess()
 
     def compute_ao(self, stream=None):
         """Stored AO values + gradients (the reference's grid_AO tensor), for ``xc_from_ao``."""
@@ -296,6 +324,10 @@ class RKSEngine:
 
     def initial(self):
         """D <- D0, then XC and J/K of D0 (nanoDFT.py:146-148)."""
+        self._start_guess()
+        if self._guess_done is not None:
+            torch.cuda.current_stream(self.device).wait_event(self._guess_done)
+            self._guess_done = None
         self.D.copy_(self.D0)
         self.iter.zero_()
         self.active.fill_(1)

@@ -87,11 +87,11 @@ def init_params_np(seed=0):
 
 
 class Batch:
-    """Graph of a list of molecules (host arrays + device copies)."""
+    """Graph of a list of molecules, built on ``device`` (edge and pair lists stay there)."""
 
     def __init__(self, mols, device="cuda", mat_off=None, nao=None):
-        # all molecules at once on a padded (molecule, atom, atom) grid, on ``device``; edge order
-        # per molecule is by receiving atom then sending atom, pair order by (a, b) with a < b
+        # all molecules at once on a padded (molecule, atom, atom) grid; edge order per molecule
+        # is by receiving atom then sending atom, pair order by (a, b) with a < b
         nat = np.array([m.natm for m in mols], np.int64)
         self.n_atoms = [int(n) for n in nat]
         nm, amax = len(mols), int(nat.max()) if len(mols) else 0
@@ -110,31 +110,26 @@ class Batch:
         close = (d < RC) & valid[:, :, None] & valid[:, None, :]
         edge = close & ~torch.eye(amax, dtype=torch.bool, device=dev)[None]
         em, et, es = torch.nonzero(edge.transpose(1, 2), as_tuple=True)   # (molecule, receiver, sender)
-        host = lambda x: x.cpu().numpy()
-        src, dst, rr = [host(es + base[em])], [host(et + base[em])], [host(d[em, es, et])]
+        i32, f32 = torch.int32, torch.float32
+        src, dst, rr = (es + base[em]).to(i32), (et + base[em]).to(i32), d[em, es, et].to(f32)
         pm, a, b = torch.nonzero(torch.triu(close, 1) if amax else close, as_tuple=True)
-        pa, pb, pr = [host(a + base[pm])], [host(b + base[pm])], [host(d[pm, a, b])]
+        pa, pb, pr = (a + base[pm]).to(i32), (b + base[pm]).to(i32), d[pm, a, b].to(f32)
         u = C[pm, b] - C[pm, a]
-        pu = [host(u / torch.clamp(torch.linalg.norm(u, dim=1, keepdim=True), min=1e-30))]
+        pu = (u / torch.clamp(torch.linalg.norm(u, dim=1, keepdim=True), min=1e-30)).to(f32).reshape(-1)
         zf = Zh[valid_h]
+        self.A, self.P, self.Pr = int(len(zf)), int(src.numel()), int(pa.numel())
         mol_of = np.repeat(np.arange(nm), nat)
         width = np.where(Zh <= 2, 1, 5) * valid_h
         ao0 = (np.cumsum(width, 1) - width)[valid_h]
         tmap = np.zeros(max(TYPE) + 1 if TYPE else 1, np.int32)
         for zz, tt in TYPE.items():
             tmap[zz] = tt
-        types = tmap[zf]
+        types = tmap[zf].astype(np.int32)
         heavy = (zf > 2).astype(np.int64)
-        cat = lambda xs, dt: np.ascontiguousarray(np.concatenate(xs) if xs else np.zeros(0), dtype=dt)
-        self.src, self.dst, self.r = cat(src, np.int32), cat(dst, np.int32), cat(rr, np.float32)
-        self.pa, self.pb, self.pr = cat(pa, np.int32), cat(pb, np.int32), cat(pr, np.float32)
-        self.pu = cat(pu, np.float32).reshape(-1)
-        self.types = np.array(types, np.int32)
-        self.A, self.P, self.Pr = len(types), len(self.src), len(self.pa)
-        ptr_ = np.zeros(self.A + 1, np.int64)
-        np.add.at(ptr_, self.dst + 1, 1)
-        self.ptr = np.cumsum(ptr_).astype(np.int32)
-        self.atoms = np.stack([np.array(mol_of), np.array(ao0), np.array(heavy), np.zeros(self.A, int)], 1).astype(np.int32)
+        atoms = np.stack([mol_of, ao0, heavy, np.zeros(self.A, np.int64)], 1).astype(np.int32)
+        cnt = torch.bincount(dst.to(torch.int64), minlength=self.A)
+        ptr_ = torch.zeros(self.A + 1, dtype=torch.int64, device=dev)
+        ptr_[1:] = torch.cumsum(cnt, 0)
         naos = np.array([m.nao for m in mols], np.int32)
         if mat_off is None:
             mat_off = np.concatenate([[0], np.cumsum(naos.astype(np.int64) ** 2)[:-1]]).astype(np.int64)
@@ -142,9 +137,10 @@ class Batch:
         self.nao = np.ascontiguousarray(naos if nao is None else nao, np.int32)
         self.n_mat = int(self.mat_off[-1] + self.nao[-1].astype(np.int64) ** 2) if len(mols) else 0
         self.nent = self.n_mat                 # the loss averages over every matrix entry
-        t = lambda x: torch.from_numpy(x).to(device)
-        self.d = {k: t(getattr(self, k)) for k in ("src", "dst", "r", "pa", "pb", "pr", "pu", "types", "ptr",
-                                                  "atoms", "mat_off", "nao")}
+        t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+        self.d = {"src": src, "dst": dst, "r": rr, "pa": pa, "pb": pb, "pr": pr, "pu": pu.contiguous(),
+                  "types": t(types), "ptr": ptr_.to(i32), "atoms": t(atoms), "mat_off": t(self.mat_off),
+                  "nao": t(self.nao)}
 
 
 class GuessNet:

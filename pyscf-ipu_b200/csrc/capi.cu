@@ -21,11 +21,15 @@ static int b2_note(cudaError_t e) {
 
 #define B2_TRY(x) do { int _rc = b2_note(x); if (_rc) return _rc; } while (0)
 
+// device copy of a host table.  With a stream the copy is queued there (the caller synchronizes
+// that stream before the host vector goes away); without one it completes before returning.
 template <typename T>
-static int b2_upload(T **dst, const std::vector<T> &src) {
+static int b2_upload(T **dst, const std::vector<T> &src, cudaStream_t st = nullptr) {
   size_t n = std::max<size_t>(1, src.size());
   B2_TRY(cudaMalloc((void **)dst, sizeof(T) * n));
-  if (!src.empty()) B2_TRY(cudaMemcpy(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice));
+  if (src.empty()) return B2_OK;
+  if (st) B2_TRY(cudaMemcpyAsync(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, st));
+  else B2_TRY(cudaMemcpy(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice));
   return B2_OK;
 }
 
@@ -50,7 +54,7 @@ static void b2_plan_free(B2PlanDev *P) {
   delete P;
 }
 
-static int b2_set_jk_chunk(B2PlanDev *P, long long elems) {
+static int b2_set_jk_chunk(B2PlanDev *P, long long elems, cudaStream_t st = nullptr) {
   // whole runs of 8 for every thread of a 1024-thread CTA; at most 32768 entries per CTA
   // keeps the fixed-point J/K accumulators exact
   if (elems <= 0) elems = 32768;
@@ -60,11 +64,11 @@ static int b2_set_jk_chunk(B2PlanDev *P, long long elems) {
   for (int m = 0; m < nmol; ++m) off[m + 1] = off[m] + (P->h.mols[m].n4 + elems - 1) / elems;
   cudaFree(P->jk_chunk_off);
   P->jk_chunk_off = nullptr;
-  int rc = b2_upload(&P->jk_chunk_off, off);
+  P->jk_off_h = std::move(off);                   // a queued copy reads the plan's own copy
+  int rc = b2_upload(&P->jk_chunk_off, P->jk_off_h, st);
   if (rc) return rc;
-  P->jk_off_h = off;
   P->jk_chunk = elems;
-  P->jk_nchunks = off[nmol];
+  P->jk_nchunks = P->jk_off_h[nmol];
   return B2_OK;
 }
 
@@ -81,24 +85,24 @@ static void b2_buckets(const B2PlanDev *P, const std::vector<int> &mols, std::ve
 }
 
 // warp-task table of the J/K products and their pair-vector workspace
-static int b2_set_sv(B2PlanDev *P) {
+static int b2_set_sv(B2PlanDev *P, cudaStream_t st) {
   const int nmol = P->h.nmol;
   std::vector<long long> off(nmol + 1, 0);
   for (int m = 0; m < nmol; ++m) {
     const long long N = P->h.mols[m].nao;
     off[m + 1] = off[m] + b2_sv_tasks_host(N * (N + 1) / 2);
   }
-  int rc = b2_upload(&P->sv_off, off);
-  if (rc) return rc;
   P->sv_off_h = off;
+  int rc = b2_upload(&P->sv_off, P->sv_off_h, st);
+  if (rc) return rc;
   P->sv_ntask = off[nmol];
   B2_TRY(cudaMalloc(&P->sv_work, sizeof(double) * 4 * (size_t)std::max(1ll, P->h.n_rows)));
-  std::vector<int> all(nmol), map;
+  std::vector<int> all(nmol);
   for (int m = 0; m < nmol; ++m) all[m] = m;
-  b2_buckets(P, all, map, P->bkt_off_h);
+  b2_buckets(P, all, P->bkt_map_h, P->bkt_off_h);
   for (int b = 0; b < B2_NBKT; ++b) B2_TRY(cudaStreamCreateWithFlags(&P->bkt_stream[b], cudaStreamNonBlocking));
   for (int b = 0; b <= B2_NBKT; ++b) B2_TRY(cudaEventCreateWithFlags(&P->bkt_ev[b], cudaEventDisableTiming));
-  return b2_upload(&P->bkt_map, map);
+  return b2_upload(&P->bkt_map, P->bkt_map_h, st);
 }
 
 extern "C" {
@@ -117,21 +121,29 @@ int b2_plan_create(int nmol, const int *natm, const int *nbas, const int *atm, c
                    const double *env, const int64_t *env_off, void **plan) {
   if (nmol <= 0 || !natm || !nbas || !atm || !bas || !env || !env_off || !plan) return B2_ERR_ARG;
   B2PlanDev *P = new B2PlanDev();
-  int rc = b2_plan_build(P->h, nmol, natm, nbas, atm, bas, env, (const long long *)env_off);
+  int rc = b2_plan_build(P->h, nmol, natm, nbas, atm, bas, env, (const long long *)env_off,
+                         /*pair_tables=*/false);
   if (rc) { delete P; return rc; }
+  // every upload and table kernel goes to one non-blocking stream, synchronized once at the end
+  // (no ordering with, or wait on, work the caller has queued elsewhere on the device)
+  cudaStream_t cs = nullptr;
+  if ((rc = b2_note(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)))) { delete P; return rc; }
   std::vector<double> tab(B2_BOYS_NT * B2_BOYS_NM);
   b2_boys_fill_table(tab.data());
-  std::vector<B2MolDev> mols = P->h.mols;
-  if ((rc = b2_upload(&P->mols, mols)) || (rc = b2_upload(&P->row_off, P->h.row_off)) ||
-      (rc = b2_upload(&P->shells, P->h.shells)) || (rc = b2_upload(&P->pinfo, P->h.pinfo)) ||
-      (rc = b2_upload(&P->ao2sh, P->h.ao2sh)) || (rc = b2_upload(&P->cls_list, P->h.cls_list)) ||
-      (rc = b2_upload(&P->cls_cnt, P->h.cls_cnt)) || (rc = b2_upload(&P->atom_xyz, P->h.atom_xyz)) ||
-      (rc = b2_upload(&P->atom_z, P->h.atom_z)) || (rc = b2_upload(&P->boys, tab)) ||
-      (rc = b2_upload(&P->boys32, std::vector<float>(tab.begin(), tab.end()))) ||
-      (rc = b2_set_jk_chunk(P, 0)) || (rc = b2_build_pairs(*P)) || (rc = b2_set_sv(P))) {
+  std::vector<float> tab32(tab.begin(), tab.end());
+  if ((rc = b2_upload(&P->mols, P->h.mols, cs)) || (rc = b2_upload(&P->row_off, P->h.row_off, cs)) ||
+      (rc = b2_upload(&P->shells, P->h.shells, cs)) || (rc = b2_upload(&P->ao2sh, P->h.ao2sh, cs)) ||
+      (rc = b2_upload(&P->atom_xyz, P->h.atom_xyz, cs)) || (rc = b2_upload(&P->atom_z, P->h.atom_z, cs)) ||
+      (rc = b2_upload(&P->boys, tab, cs)) || (rc = b2_upload(&P->boys32, tab32, cs)) ||
+      (rc = b2_set_jk_chunk(P, 0, cs)) || (rc = b2_build_pairs(*P, cs)) || (rc = b2_set_sv(P, cs))) {
+    cudaStreamSynchronize(cs);
+    cudaStreamDestroy(cs);
     b2_plan_free(P);
     return rc;
   }
+  rc = b2_note(cudaStreamSynchronize(cs));
+  cudaStreamDestroy(cs);
+  if (rc) { b2_plan_free(P); return rc; }
   cudaGetDevice(&P->device);
   *plan = P;
   return B2_OK;

@@ -60,13 +60,14 @@ struct B2PlanDev {
   long long sv_ntask = 0;
   double *sv_work = nullptr;              // 4 x n_rows: x_J, x_K, y_J, y_K
   int *bkt_map = nullptr;                 // molecules ordered by orbital bucket
+  std::vector<int> bkt_map_h;
   std::vector<int> bkt_off_h;             // B2_NBKT + 1 bucket starts in bkt_map
   cudaStream_t bkt_stream[B2_NBKT] = {};  // per-bucket streams (forked from / joined to the caller's)
   cudaEvent_t bkt_ev[B2_NBKT + 1] = {};
 };
 
 int b2_launch_eri_s8(B2PlanDev &P, int precision, void *out, cudaStream_t st);
-int b2_build_pairs(B2PlanDev &P);
+int b2_build_pairs(B2PlanDev &P, cudaStream_t st);
 int b2_launch_exch_build(const B2PlanDev &P, int precision, const void *eri, void *exch, cudaStream_t st);
 int b2_launch_jk_symv(const B2PlanDev &P, int precision, const int *active, const void *eri,
                       const void *exch, const double *D, double *J, double *K, double *work,

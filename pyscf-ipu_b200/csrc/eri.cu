@@ -72,14 +72,21 @@ static void b2_eri_all(const B2PlanDev &P, const B2EriTask *tasks, const std::ve
 #undef B2_G
 }
 
-// Work list on the device: the host makes one counting pass over (shell pair, ket class) and
-// uploads each item's first task index (same grouping and order as b2_eri_tasks); one thread
-// per item then writes its tasks.  A 4096-molecule batch has ~1.7e7 tasks.
-__global__ void k_eri_tasks(const B2MolDev *__restrict__ mols, int nmol, const B2PairInfo *__restrict__ pinfo,
-                            const int *__restrict__ cls_cnt, const int *__restrict__ toff, long long n_sp,
-                            int chunk, int split_p, B2EriTask *__restrict__ tasks) {
-  const long long it = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (it >= 4 * n_sp) return;
+// Work list on the device.  Item it = 4 sp + c (sp: global bra shell pair, c: ket class) owns
+// ceil(cnt / chunk) x nsub tasks, cnt = class-c kets KL <= (I,I); tasks are grouped by
+// (bra class, c) and within a group ordered by item (the order of b2_eri_tasks).  Three passes
+// over tiles of B2_TT items: per-tile group sums, an exclusive scan of each group over the
+// tiles (group totals to the host, which sizes the list), then each tile writes its tasks.
+// A 4096-molecule batch has ~6e6 items and ~1.7e7 tasks.
+#define B2_TT 1024                 // items per tile: 256 threads x 4 consecutive items
+
+__device__ __forceinline__ void b2_task_item(const B2MolDev *__restrict__ mols, int nmol,
+                                             const B2PairInfo *__restrict__ pinfo,
+                                             const int *__restrict__ cls_cnt, long long it, long long n_items,
+                                             int chunk, int split_p, int &grp, int &n, int &mol, int &IJ,
+                                             int &cnt, int &nsub) {
+  grp = 0; n = 0; mol = 0; IJ = 0; cnt = 0; nsub = 1;
+  if (it >= n_items) return;
   const long long sp = it >> 2;
   const int c = (int)(it & 3);
   int lo = 0, hi = nmol - 1;
@@ -87,70 +94,159 @@ __global__ void k_eri_tasks(const B2MolDev *__restrict__ mols, int nmol, const B
     const int mid = (lo + hi + 1) >> 1;
     if (mols[mid].sp_off <= sp) lo = mid; else hi = mid - 1;
   }
-  const B2MolDev md = mols[lo];
+  const B2MolDev &md = mols[lo];
   const B2PairInfo pi = pinfo[sp];
-  const int IJ = (int)(sp - md.sp_off);
   const int spcut = (int)b2_tri(pi.I) + pi.I;
-  const int cnt = cls_cnt[4ll * md.sp_off + (long long)c * md.nsp + spcut];
-  const int nsub = (split_p && pi.lI) ? 3 : 1;
-  long long o = toff[it];
-  for (int s0 = 0; s0 < cnt; s0 += chunk)
-    for (int sub = 0; sub < nsub; ++sub)
-      tasks[o++] = B2EriTask{lo, IJ, c, s0, min(chunk, cnt - s0), nsub > 1 ? sub : -1};
+  mol = lo;
+  IJ = (int)(sp - md.sp_off);
+  cnt = cls_cnt[4ll * md.sp_off + (long long)c * md.nsp + spcut];
+  nsub = (split_p && pi.lI) ? 3 : 1;
+  grp = (pi.lI + 2 * pi.lJ) * 4 + c;
+  n = (cnt + chunk - 1) / chunk * nsub;
 }
 
-static int b2_eri_task_upload(B2PlanDev &P, int precision) {
+__global__ void __launch_bounds__(256)
+k_task_tile_sums(const B2MolDev *__restrict__ mols, int nmol, const B2PairInfo *__restrict__ pinfo,
+                 const int *__restrict__ cls_cnt, long long n_items, int chunk, int split_p,
+                 long long *__restrict__ tile_sum) {
+  __shared__ int s[16];
+  if (threadIdx.x < 16) s[threadIdx.x] = 0;
+  __syncthreads();
+  const long long i0 = (long long)blockIdx.x * B2_TT + 4 * threadIdx.x;
+  for (int k = 0; k < 4; ++k) {
+    int grp, n, mol, IJ, cnt, nsub;
+    b2_task_item(mols, nmol, pinfo, cls_cnt, i0 + k, n_items, chunk, split_p, grp, n, mol, IJ, cnt, nsub);
+    if (n) atomicAdd(&s[grp], n);
+  }
+  __syncthreads();
+  if (threadIdx.x < 16) tile_sum[(long long)blockIdx.x * 16 + threadIdx.x] = s[threadIdx.x];
+}
+
+// one CTA per group: exclusive scan of the group's tile sums in place; total -> gtot[group]
+__global__ void __launch_bounds__(1024)
+k_task_scan(long long *__restrict__ tile_sum, long long ntile, long long *__restrict__ gtot) {
+  __shared__ long long wsum[32];
+  const int g = blockIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  long long carry = 0;
+  for (long long t0 = 0; t0 < ntile; t0 += 1024) {
+    const long long t = t0 + threadIdx.x;
+    const long long v = t < ntile ? tile_sum[t * 16 + g] : 0;
+    long long x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const long long y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+      long long z = wsum[lane];
+      for (int o = 1; o < 32; o <<= 1) {
+        const long long y = __shfl_up_sync(0xffffffffu, z, o);
+        if (lane >= o) z += y;
+      }
+      wsum[lane] = z;                                    // inclusive over warps
+    }
+    __syncthreads();
+    const long long excl = carry + (w ? wsum[w - 1] : 0) + x - v;
+    if (t < ntile) tile_sum[t * 16 + g] = excl;
+    carry += wsum[31];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) gtot[g] = carry;
+}
+
+__global__ void __launch_bounds__(256)
+k_task_write(const B2MolDev *__restrict__ mols, int nmol, const B2PairInfo *__restrict__ pinfo,
+             const int *__restrict__ cls_cnt, long long n_items, int chunk, int split_p,
+             const long long *__restrict__ tile_base, const long long *__restrict__ goff,
+             B2EriTask *__restrict__ tasks) {
+  __shared__ long long wsum[8][16];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const long long i0 = (long long)blockIdx.x * B2_TT + 4 * threadIdx.x;
+  int grp[4], n[4], mol[4], IJ[4], cnt[4], nsub[4];
+  for (int k = 0; k < 4; ++k)
+    b2_task_item(mols, nmol, pinfo, cls_cnt, i0 + k, n_items, chunk, split_p, grp[k], n[k], mol[k], IJ[k],
+                 cnt[k], nsub[k]);
+  // per group: exclusive prefix of this thread's task counts over the CTA (warp scans + warp sums)
+  long long off[4];
+  for (int g = 0; g < 16; ++g) {
+    int v = 0;
+    for (int k = 0; k < 4; ++k) v += grp[k] == g ? n[k] : 0;
+    int x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, o);
+      if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w][g] = x;
+    int run = x - v;                                     // exclusive within the warp
+    for (int k = 0; k < 4; ++k)
+      if (grp[k] == g) { off[k] = run; run += n[k]; }
+  }
+  __syncthreads();
+  for (int k = 0; k < 4; ++k) {
+    if (!n[k]) continue;
+    const int g = grp[k];
+    long long o = goff[g] + tile_base[(long long)blockIdx.x * 16 + g] + off[k];
+    for (int v = 0; v < w; ++v) o += wsum[v][g];
+    const int c = (int)((i0 + k) & 3);
+    for (int s0 = 0; s0 < cnt[k]; s0 += chunk)
+      for (int sub = 0; sub < nsub[k]; ++sub)
+        tasks[o++] = B2EriTask{mol[k], IJ[k], c, s0, min(chunk, cnt[k] - s0), nsub[k] > 1 ? sub : -1};
+  }
+}
+
+static int b2_eri_task_upload(B2PlanDev &P, int precision, cudaStream_t st) {
   B2EriTask *&dst = precision == 64 ? P.eri_tasks64 : P.eri_tasks32;
   std::vector<long long> &goff = precision == 64 ? P.eri_goff64 : P.eri_goff32;
   if (dst) return B2_OK;
   const int chunk = 32;                          // kets per warp task
-  const bool split_p = precision == 64;
-  const B2PlanHost &H = P.h;
-  const long long nsp = H.n_sp;
-  std::vector<int> toff((size_t)std::max(1ll, 4 * nsp));
+  const int split_p = precision == 64 ? 1 : 0;
+  const long long n_items = 4ll * P.h.n_sp;
+  const long long ntile = std::max(1ll, (n_items + B2_TT - 1) / B2_TT);
+  long long *scratch = nullptr;                  // tile sums (16 per tile), group totals, group starts
+  B2_CUDA_TRY(cudaMalloc(&scratch, sizeof(long long) * (size_t)(16 * ntile + 32)));
+  long long *gtot = scratch + 16 * ntile, *dgoff = gtot + 16;
+  std::vector<long long> tot(16, 0);
+  int rc = B2_OK;
+  if (n_items > 0) {
+    k_task_tile_sums<<<(unsigned)ntile, 256, 0, st>>>(P.mols, P.h.nmol, P.pinfo, P.cls_cnt, n_items, chunk,
+                                                      split_p, scratch);
+    k_task_scan<<<16, 1024, 0, st>>>(scratch, ntile, gtot);
+    b2_count_launches(2);
+    if (cudaMemcpyAsync(tot.data(), gtot, sizeof(long long) * 16, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+      rc = B2_ERR_CUDA;
+  }
   std::vector<long long> g(17, 0);
-  for (int pass = 0; pass < 2; ++pass) {
-    std::vector<long long> pos(g.begin(), g.end() - 1);
-    for (int m = 0; m < H.nmol; ++m) {
-      const B2MolDev &md = H.mols[m];
-      for (int IJ = 0; IJ < md.nsp; ++IJ) {
-        const B2PairInfo &pi = H.pinfo[md.sp_off + IJ];
-        const int spcut = (int)b2_tri(pi.I) + pi.I;
-        const int nsub = (split_p && pi.lI) ? 3 : 1;
-        for (int c = 0; c < 4; ++c) {
-          const int cnt = H.cls_cnt[4ll * md.sp_off + (long long)c * md.nsp + spcut];
-          const int grp = (pi.lI + 2 * pi.lJ) * 4 + c;
-          const long long n = (long long)((cnt + chunk - 1) / chunk) * nsub;
-          if (pass == 0) { g[grp + 1] += n; continue; }
-          toff[4 * ((size_t)md.sp_off + IJ) + c] = (int)pos[grp];
-          pos[grp] += n;
-        }
-      }
+  for (int k = 0; k < 16; ++k) g[k + 1] = g[k] + tot[k];
+  if (!rc && g[16] >= (1ll << 31)) rc = B2_ERR_SIZE;
+  if (!rc && cudaMalloc(&dst, sizeof(B2EriTask) * std::max<size_t>(1, (size_t)g[16])) != cudaSuccess) {
+    dst = nullptr;
+    rc = B2_ERR_CUDA;
+  }
+  if (!rc && n_items > 0) {
+    if (cudaMemcpyAsync(dgoff, g.data(), sizeof(long long) * 16, cudaMemcpyHostToDevice, st) != cudaSuccess)
+      rc = B2_ERR_CUDA;
+    else {
+      k_task_write<<<(unsigned)ntile, 256, 0, st>>>(P.mols, P.h.nmol, P.pinfo, P.cls_cnt, n_items, chunk,
+                                                    split_p, scratch, dgoff, dst);
+      b2_count_launches(1);
+      if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) rc = B2_ERR_CUDA;
     }
-    if (pass == 0) {
-      for (int k = 0; k < 16; ++k) g[k + 1] += g[k];
-      if (g[16] >= (1ll << 31)) return B2_ERR_SIZE;
-    }
+  }
+  cudaFree(scratch);
+  if (rc) {
+    cudaFree(dst);
+    dst = nullptr;
+    return rc;
   }
   goff = g;
-  int *dtoff = nullptr;
-  B2_CUDA_TRY(cudaMalloc(&dst, sizeof(B2EriTask) * std::max<size_t>(1, (size_t)g[16])));
-  B2_CUDA_TRY(cudaMalloc(&dtoff, sizeof(int) * toff.size()));
-  B2_CUDA_TRY(cudaMemcpy(dtoff, toff.data(), sizeof(int) * toff.size(), cudaMemcpyHostToDevice));
-  if (nsp > 0) {
-    k_eri_tasks<<<(unsigned)((4 * nsp + 255) / 256), 256>>>(P.mols, H.nmol, P.pinfo, P.cls_cnt, dtoff, nsp,
-                                                            chunk, split_p ? 1 : 0, dst);
-    b2_count_launches(1);
-  }
-  B2_CUDA_TRY(cudaGetLastError());
-  B2_CUDA_TRY(cudaDeviceSynchronize());
-  cudaFree(dtoff);
   return B2_OK;
 }
 
 int b2_launch_eri_s8(B2PlanDev &P, int precision, void *out, cudaStream_t st) {
   if (precision != 64 && precision != 32) return B2_ERR_ARG;
-  int rc = b2_eri_task_upload(P, precision);
+  int rc = b2_eri_task_upload(P, precision, st);
   if (rc) return rc;
   if (precision == 64)
     b2_eri_all<double>(P, P.eri_tasks64, P.eri_goff64, P.pp64, (double *)out, st);
@@ -340,14 +436,52 @@ __global__ void k_pair_prims(const B2MolDev *__restrict__ mols, int nmol, const 
   b2_pair_prims_packed(shells[sh + pi.I], shells[sh + pi.J], pp64 + gp * B2_MAXPP, pp32 + gp * B2_MAXPP);
 }
 
-int b2_build_pairs(B2PlanDev &P) {
-  const long long n = (long long)P.h.n_sp * B2_MAXPP;
+// shell-pair tables of every molecule, one warp per molecule: pair info, the class lists
+// (pairs of each angular class in ascending order, from cls_start) and the inclusive class
+// prefix counts cls_cnt[4 sp_off + c nsp + sp] = #{class-c pairs <= sp}; the host test build
+// fills the same tables (b2_plan_build with pair tables)
+__global__ void __launch_bounds__(256)
+k_plan_pairs(const B2MolDev *__restrict__ mols, int nmol, const B2Shell *__restrict__ shells,
+             B2PairInfo *__restrict__ pinfo, int *__restrict__ cls_list, int *__restrict__ cls_cnt) {
+  const int m = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (m >= nmol) return;                           // whole warp
+  const B2MolDev md = mols[m];
+  const B2Shell *S = shells + md.sh_off;
+  const unsigned le = (2u << lane) - 1u;           // lanes <= this one (lane 31: all)
+  int run[4] = {0, 0, 0, 0};
+  for (int base = 0; base < md.nsp; base += 32) {
+    const int sp = base + lane;
+    int c = -1;
+    if (sp < md.nsp) {
+      const int I = (int)b2_untri(sp), J = sp - (int)b2_tri(I);
+      const int lI = S[I].l, lJ = S[J].l;
+      pinfo[md.sp_off + sp] = B2PairInfo{I, J, lI, lJ, S[I].ao0, S[J].ao0, S[I].nprim * S[J].nprim, 0};
+      c = b2_class(lI, lJ);
+    }
+    for (int cc = 0; cc < 4; ++cc) {
+      const unsigned mk = __ballot_sync(0xffffffffu, c == cc);
+      const int incl = run[cc] + __popc(mk & le);
+      if (sp < md.nsp) cls_cnt[4ll * md.sp_off + (long long)cc * md.nsp + sp] = incl;
+      if (c == cc) cls_list[md.sp_off + md.cls_start[cc] + incl - 1] = sp;
+      run[cc] += __popc(mk);
+    }
+  }
+}
+
+int b2_build_pairs(B2PlanDev &P, cudaStream_t st) {
+  const long long nsp = P.h.n_sp, n = nsp * B2_MAXPP;
+  B2_CUDA_TRY(cudaMalloc(&P.pinfo, sizeof(B2PairInfo) * (size_t)std::max(1ll, nsp)));
+  B2_CUDA_TRY(cudaMalloc(&P.cls_list, sizeof(int) * (size_t)std::max(1ll, nsp)));
+  B2_CUDA_TRY(cudaMalloc(&P.cls_cnt, sizeof(int) * (size_t)std::max(1ll, 4 * nsp)));
   B2_CUDA_TRY(cudaMalloc(&P.pp64, sizeof(B2PairPrim<double>) * (size_t)std::max(1ll, n)));
   B2_CUDA_TRY(cudaMalloc(&P.pp32, sizeof(B2PairPrim<float>) * (size_t)std::max(1ll, n)));
   if (n > 0) {
-    k_pair_prims<<<(unsigned)((P.h.n_sp + 127) / 128), 128>>>(P.mols, P.h.nmol, P.shells, P.pinfo,
-                                                              P.h.n_sp, P.pp64, P.pp32);
-    b2_count_launches(1);
+    k_plan_pairs<<<(unsigned)((P.h.nmol + 7) / 8), 256, 0, st>>>(P.mols, P.h.nmol, P.shells, P.pinfo,
+                                                                 P.cls_list, P.cls_cnt);
+    k_pair_prims<<<(unsigned)((nsp + 127) / 128), 128, 0, st>>>(P.mols, P.h.nmol, P.shells, P.pinfo,
+                                                               nsp, P.pp64, P.pp32);
+    b2_count_launches(2);
     B2_CUDA_TRY(cudaGetLastError());
   }
   return B2_OK;

@@ -46,7 +46,7 @@ struct B2PlanHost {
   std::vector<int> atom_z;
 };
 
-static inline int b2_class(int lK, int lL) { return lK + 2 * lL; }   // ss=0, ps=1, sp=2, pp=3
+B2_HD int b2_class(int lK, int lL) { return lK + 2 * lL; }   // ss=0, ps=1, sp=2, pp=3
 
 // primitive pair x (= ia * B2_MAXPRIM + ib) of shells a, b: zeta, centre P, P-A, P-B and
 // K = c_a c_b exp(-a b / zeta |AB|^2) sqrt(2) pi^{5/4} / zeta; absent primitives give an inert
@@ -100,12 +100,31 @@ B2_HD void b2_pair_prims_packed(const B2Shell &a, const B2Shell &b, B2PairPrim<d
 }
 
 // returns B2_OK or an error code
+// pair_tables: also fill pinfo / cls_list / cls_cnt here (the host test build); the device plan
+// builds them with k_plan_pairs and keeps only per-molecule and per-shell work on the host.
 static int b2_plan_build(B2PlanHost &P, int nmol, const int *natm, const int *nbas, const int *atm,
-                         const int *bas, const double *env, const long long *env_off) {
+                         const int *bas, const double *env, const long long *env_off,
+                         bool pair_tables = true) {
   P = B2PlanHost();
   P.nmol = nmol;
   P.mols.resize(nmol);
   P.row_off.assign(nmol + 1, 0);
+  long long tot_sh = 0, tot_atm = 0, tot_sp = 0;
+  for (int m = 0; m < nmol; ++m) {
+    tot_sh += nbas[m];
+    tot_atm += natm[m];
+    tot_sp += (long long)nbas[m] * (nbas[m] + 1) / 2;
+  }
+  if (tot_sp >= (1ll << 31) / 4) return B2_ERR_SIZE;
+  P.shells.reserve(tot_sh);
+  P.ao2sh.reserve(3 * tot_sh);
+  P.atom_xyz.reserve(3 * tot_atm);
+  P.atom_z.reserve(tot_atm);
+  if (pair_tables) {
+    P.pinfo.reserve(tot_sp);
+    P.cls_list.reserve(tot_sp);
+    P.cls_cnt.reserve(4 * tot_sp);
+  }
   int atm_row = 0, bas_row = 0;
   for (int m = 0; m < nmol; ++m) {
     const int *A = atm + (size_t)atm_row * B2_ATM_SLOTS;
@@ -155,33 +174,40 @@ static int b2_plan_build(B2PlanHost &P, int nmol, const int *natm, const int *nb
     md.eri_off = P.n_eri;
     md.row_off = P.n_rows;
     md.mat_off = P.n_mat;
-    // shell pairs
+    // class starts: pairs (I, J <= I) of class lI + 2 lJ, counted from the shells' l in O(nbas)
     const B2Shell *S = &P.shells[md.sh_off];
-    std::vector<int> cls(nsp);
-    for (int I = 0; I < nbas[m]; ++I)
-      for (int J = 0; J <= I; ++J) {
-        const B2Shell &a = S[I], &b = S[J];
-        B2PairInfo pi;
-        pi.I = I; pi.J = J; pi.lI = a.l; pi.lJ = b.l; pi.ao0I = a.ao0; pi.ao0J = b.ao0;
-        pi.nprim = a.nprim * b.nprim; pi.pad = 0;
-        P.pinfo.push_back(pi);
-        cls[(int)b2_tri(I) + J] = b2_class(a.l, b.l);
-      }
-    // class lists and prefix counts
-    int start = 0;
-    for (int c = 0; c < 4; ++c) {
-      md.cls_start[c] = start;
-      for (int sp = 0; sp < nsp; ++sp)
-        if (cls[sp] == c) { P.cls_list.push_back(sp); ++start; }
+    int ccount[4] = {0, 0, 0, 0}, nl[2] = {0, 0};
+    for (int I = 0; I < nbas[m]; ++I) {
+      ++nl[S[I].l];
+      ccount[b2_class(S[I].l, 0)] += nl[0];
+      ccount[b2_class(S[I].l, 1)] += nl[1];
     }
-    md.cls_start[4] = start;
-    size_t base = P.cls_cnt.size();
-    P.cls_cnt.resize(base + 4 * (size_t)nsp);
-    for (int c = 0; c < 4; ++c) {
-      int cnt = 0;
-      for (int sp = 0; sp < nsp; ++sp) {
-        if (cls[sp] == c) ++cnt;
-        P.cls_cnt[base + (size_t)c * nsp + sp] = cnt;
+    for (int c = 0, start = 0; c < 4; ++c) { md.cls_start[c] = start; start += ccount[c]; }
+    md.cls_start[4] = nsp;
+    if (pair_tables) {
+      // shell pairs
+      std::vector<int> cls(nsp);
+      for (int I = 0; I < nbas[m]; ++I)
+        for (int J = 0; J <= I; ++J) {
+          const B2Shell &a = S[I], &b = S[J];
+          B2PairInfo pi;
+          pi.I = I; pi.J = J; pi.lI = a.l; pi.lJ = b.l; pi.ao0I = a.ao0; pi.ao0J = b.ao0;
+          pi.nprim = a.nprim * b.nprim; pi.pad = 0;
+          P.pinfo.push_back(pi);
+          cls[(int)b2_tri(I) + J] = b2_class(a.l, b.l);
+        }
+      // class lists and prefix counts
+      for (int c = 0; c < 4; ++c)
+        for (int sp = 0; sp < nsp; ++sp)
+          if (cls[sp] == c) P.cls_list.push_back(sp);
+      size_t base = P.cls_cnt.size();
+      P.cls_cnt.resize(base + 4 * (size_t)nsp);
+      for (int c = 0; c < 4; ++c) {
+        int cnt = 0;
+        for (int sp = 0; sp < nsp; ++sp) {
+          if (cls[sp] == c) ++cnt;
+          P.cls_cnt[base + (size_t)c * nsp + sp] = cnt;
+        }
       }
     }
     P.mols[m] = md;
