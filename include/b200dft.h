@@ -53,6 +53,9 @@ int b2_plan_destroy(b2_plan_t plan);
  *              jk_chunk, jk_nchunks */
 int b2_plan_info(b2_plan_t plan, int64_t *info);
 
+/* Bytes plan creation copied host -> device (its tables, staged in pinned host memory). */
+int b2_plan_h2d_bytes(b2_plan_t plan, int64_t *bytes);
+
 /* Host copies of per-molecule offsets/sizes (arrays of nmol). */
 int b2_plan_offsets(b2_plan_t plan, int64_t *eri_off, int64_t *mat_off, int *nao, int *nocc);
 

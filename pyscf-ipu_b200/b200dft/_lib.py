@@ -25,6 +25,7 @@ SIGNATURES = {
     "b2_plan_create": [_I, _P, _P, _P, _P, _P, _P, _P],
     "b2_plan_destroy": [_P],
     "b2_plan_info": [_P, _P],
+    "b2_plan_h2d_bytes": [_P, _P],
     "b2_plan_offsets": [_P, _P, _P, _P, _P],
     "b2_plan_set_jk_chunk": [_P, _L],
     "b2_plan_set_xc_impl": [_P, _I],

@@ -51,6 +51,9 @@ class Plan:
         check(lib().b2_plan_offsets(h, ptr(self.eri_off), ptr(self.mat_off), ptr(self.nao),
                                     ptr(self.nocc)), "b2_plan_offsets")
         self.grid_off = None
+        hb = ctypes.c_int64()
+        check(lib().b2_plan_h2d_bytes(h, ctypes.byref(hb)), "b2_plan_h2d_bytes")
+        self.h2d_bytes = hb.value
 
     def set_grid(self, npoints):
         goff = np.concatenate([[0], np.cumsum(npoints)]).astype(np.int64)
@@ -472,3 +475,54 @@ class RKSEngine:
 
     def close(self):
         self.plan.close()
+
+
+def _run_one(mols, plan, level, precision, guess, net, run_kw):
+    """one batch to convergence; returns host arrays, the engine's device memory released
+    (back to the allocator cache, where the next batch's engine finds it)"""
+    eng = RKSEngine(mols, level=level, precision=precision, guess=guess, net=net, plan=plan)
+    try:
+        r = eng.run_converged(**run_kw)
+        out = {k: r[k].cpu().numpy() for k in ("energy", "iterations", "converged", "mo_energy",
+                                               "last5", "diis_err")}
+        out["its_run"] = r["its_run"]
+        out["h2d_bytes"] = plan.h2d_bytes + getattr(getattr(eng, "_nn_batch", None), "h2d_bytes", 0)
+        return out
+    finally:
+        eng.close()
+
+
+def run_batches(batches, level=0, precision="mixed", guess="learned", net=None, prefetch=True, **run_kw):
+    """Run a sequence of molecule batches to convergence, one ``RKSEngine`` each, yielding
+    ``(mols, result)`` per batch with the result's arrays on the host (energy, iterations,
+    converged, mo_energy, last5, diis_err).
+
+    With ``prefetch`` the next batch's plan (host tables, upload and device table build on the
+    plan's own stream) is made on a worker thread while the current batch runs on the GPU; the
+    C call releases the interpreter lock, so the two overlap.  ``run_kw`` goes to
+    ``run_converged``."""
+    from concurrent.futures import ThreadPoolExecutor
+    if guess == "learned" and net is None:
+        from .train_guess import load
+        net = load()
+    it = iter(batches)
+    dev = torch.cuda.current_device()
+
+    def make(mols):
+        torch.cuda.set_device(dev)          # worker threads start on device 0
+        return list(mols), Plan(mols)
+
+    ex = ThreadPoolExecutor(1) if prefetch else None
+    try:
+        first = next(it, None)
+        pending = None if first is None else (ex.submit(make, first) if ex else make(first))
+        while pending is not None:
+            mols, plan = pending.result() if ex else pending
+            nxt = next(it, None)
+            pending = None if nxt is None else (ex.submit(make, nxt) if ex else make(nxt))
+            out = _run_one(mols, plan, level, precision, guess, net, run_kw)
+            del plan                      # the engine and plan are released before the next batch
+            yield mols, out
+    finally:
+        if ex:
+            ex.shutdown(wait=True)

@@ -102,10 +102,10 @@ class Batch:
             Ch[valid_h] = np.concatenate([m.coords for m in mols])
             Zh[valid_h] = np.concatenate([m.charges for m in mols])
         dev = torch.device(device)
+        base_h = (np.concatenate([[0], np.cumsum(nat)[:-1]]).astype(np.int64) if nm else np.zeros(0, np.int64))
         C = torch.from_numpy(Ch).to(dev)
         valid = torch.from_numpy(valid_h).to(dev)
-        base = torch.from_numpy(np.concatenate([[0], np.cumsum(nat)[:-1]]).astype(np.int64) if nm
-                                else np.zeros(0, np.int64)).to(dev)
+        base = torch.from_numpy(base_h).to(dev)
         d = torch.sqrt(((C[:, :, None] - C[:, None]) ** 2).sum(-1))
         close = (d < RC) & valid[:, :, None] & valid[:, None, :]
         edge = close & ~torch.eye(amax, dtype=torch.bool, device=dev)[None]
@@ -138,6 +138,8 @@ class Batch:
         self.n_mat = int(self.mat_off[-1] + self.nao[-1].astype(np.int64) ** 2) if len(mols) else 0
         self.nent = self.n_mat                 # the loss averages over every matrix entry
         t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(dev)
+        self.h2d_bytes = int(Ch.nbytes + valid_h.nbytes + base_h.nbytes + types.nbytes + atoms.nbytes +
+                             self.mat_off.nbytes + self.nao.nbytes)     # host -> device copies
         self.d = {"src": src, "dst": dst, "r": rr, "pa": pa, "pb": pb, "pr": pr, "pu": pu.contiguous(),
                   "types": t(types), "ptr": ptr_.to(i32), "atoms": t(atoms), "mat_off": t(self.mat_off),
                   "nao": t(self.nao)}

@@ -17,8 +17,8 @@ the GDB-11 SMILES + RDKit conformers the reference reads, which are not availabl
 
 Pipelining (the reference overlaps host preparation with device compute the same way): a
 ``spawn`` process pool generates and parses molecules in chunks of one batch; a host thread
-keeps the next batch ready while the GPU runs the current one; a writer thread converts and
-appends finished batches.  Each batch is one ``RKSEngine`` run to convergence: molecules retire
+keeps the next batch ready, its plan already built and on the device, while the GPU runs the
+current one; a writer thread converts and appends finished batches.  Each batch is one ``RKSEngine`` run to convergence: molecules retire
 individually as they converge (their kernels skip them, and the J/K and XC launches are
 compacted to the stragglers), so a batch ends when its slowest molecule converges.
 """
@@ -35,7 +35,7 @@ import numpy as np
 import torch
 
 from .constants import HARTREE_TO_EV
-from .engine import RKSEngine
+from .engine import Plan, RKSEngine
 from .molgen import stream_chunk
 
 QM1B_COLUMNS = ("smile", "atoms", "z", "energy", "homo", "lumo", "N", "std", "y", "pos")
@@ -137,15 +137,21 @@ def run_stream(n_total, batch=4096, seed=0, level=0, precision="mixed", guess="l
         return [pool.apply_async(stream_chunk, ((seed_, s0, min(step, start + n - s0), mh),))
                 for s0 in range(start, start + n, step)]
 
+    dev = torch.cuda.current_device()
+
     def produce():
         try:
+            torch.cuda.set_device(dev)      # plans are built on this thread
+
             pending = [submit(c) for c in chunks[:2]]
             for k in range(len(chunks)):
                 parts = pending.pop(0)
                 if k + 2 < len(chunks):
                     pending.append(submit(chunks[k + 2]))
                 items = [x for p in parts for x in p.get()]
-                ready.put(items)
+                # the batch's plan (host tables, upload, device tables) is built here, off the
+                # GPU thread, while the previous batch runs
+                ready.put((items, Plan([m for _, _, m in items])))
         except Exception as e:          # surfaced by the main loop
             err.append(e)
         ready.put(None)
@@ -168,11 +174,13 @@ def run_stream(n_total, batch=4096, seed=0, level=0, precision="mixed", guess="l
     tw.start()
     try:
         while True:
-            items = ready.get()
-            if items is None or err:
+            got = ready.get()
+            if got is None or err:
                 break
+            items, plan = got
             g0 = time.perf_counter()
-            eng = RKSEngine([m for _, _, m in items], level=level, precision=precision, guess=guess, net=net)
+            eng = RKSEngine([m for _, _, m in items], level=level, precision=precision, guess=guess, net=net,
+                            plan=plan)
             res = eng.run_converged(e_tol=e_tol, diis_tol=diis_tol)
             res = {k: (v.clone() if torch.is_tensor(v) else v) for k, v in res.items()}
             torch.cuda.synchronize()

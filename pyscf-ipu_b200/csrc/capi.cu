@@ -11,6 +11,7 @@
 
 static thread_local std::string g_last_error;
 #include <atomic>
+#include <mutex>
 static std::atomic<long long> g_b2_launches{0};
 void b2_count_launches(long long n) { g_b2_launches += n; }
 
@@ -21,15 +22,35 @@ static int b2_note(cudaError_t e) {
 
 #define B2_TRY(x) do { int _rc = b2_note(x); if (_rc) return _rc; } while (0)
 
-// device copy of a host table.  With a stream the copy is queued there (the caller synchronizes
-// that stream before the host vector goes away); without one it completes before returning.
+// Plan uploads: every table is packed into one pinned staging buffer (kept and reused by later
+// plans, grown when a larger batch needs it) and copied with cudaMemcpyAsync on the plan's
+// stream; the staging lock is held until that stream has been synchronized.
+struct B2Upload {
+  cudaStream_t st = nullptr;
+  unsigned char *stage = nullptr;
+  size_t cap = 0, used = 0, bytes = 0;
+};
+static std::mutex g_stage_mu;
+static unsigned char *g_stage = nullptr;
+static size_t g_stage_cap = 0;
+
+// device copy of a host table: staged and queued with an upload context, else synchronous
 template <typename T>
-static int b2_upload(T **dst, const std::vector<T> &src, cudaStream_t st = nullptr) {
+static int b2_upload(T **dst, const std::vector<T> &src, B2Upload *u = nullptr) {
   size_t n = std::max<size_t>(1, src.size());
   B2_TRY(cudaMalloc((void **)dst, sizeof(T) * n));
   if (src.empty()) return B2_OK;
-  if (st) B2_TRY(cudaMemcpyAsync(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice, st));
-  else B2_TRY(cudaMemcpy(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice));
+  const size_t nb = sizeof(T) * src.size();
+  if (!u) {
+    B2_TRY(cudaMemcpy(*dst, src.data(), nb, cudaMemcpyHostToDevice));
+    return B2_OK;
+  }
+  const size_t at = (u->used + 255) / 256 * 256;
+  if (at + nb > u->cap) return B2_ERR_SIZE;
+  std::memcpy(u->stage + at, src.data(), nb);
+  B2_TRY(cudaMemcpyAsync(*dst, u->stage + at, nb, cudaMemcpyHostToDevice, u->st));
+  u->used = at + nb;
+  u->bytes += nb;
   return B2_OK;
 }
 
@@ -54,7 +75,7 @@ static void b2_plan_free(B2PlanDev *P) {
   delete P;
 }
 
-static int b2_set_jk_chunk(B2PlanDev *P, long long elems, cudaStream_t st = nullptr) {
+static int b2_set_jk_chunk(B2PlanDev *P, long long elems, B2Upload *u = nullptr) {
   // whole runs of 8 for every thread of a 1024-thread CTA; at most 32768 entries per CTA
   // keeps the fixed-point J/K accumulators exact
   if (elems <= 0) elems = 32768;
@@ -64,8 +85,8 @@ static int b2_set_jk_chunk(B2PlanDev *P, long long elems, cudaStream_t st = null
   for (int m = 0; m < nmol; ++m) off[m + 1] = off[m] + (P->h.mols[m].n4 + elems - 1) / elems;
   cudaFree(P->jk_chunk_off);
   P->jk_chunk_off = nullptr;
-  P->jk_off_h = std::move(off);                   // a queued copy reads the plan's own copy
-  int rc = b2_upload(&P->jk_chunk_off, P->jk_off_h, st);
+  P->jk_off_h = std::move(off);
+  int rc = b2_upload(&P->jk_chunk_off, P->jk_off_h, u);
   if (rc) return rc;
   P->jk_chunk = elems;
   P->jk_nchunks = P->jk_off_h[nmol];
@@ -85,7 +106,7 @@ static void b2_buckets(const B2PlanDev *P, const std::vector<int> &mols, std::ve
 }
 
 // warp-task table of the J/K products and their pair-vector workspace
-static int b2_set_sv(B2PlanDev *P, cudaStream_t st) {
+static int b2_set_sv(B2PlanDev *P, B2Upload *u) {
   const int nmol = P->h.nmol;
   std::vector<long long> off(nmol + 1, 0);
   for (int m = 0; m < nmol; ++m) {
@@ -93,7 +114,7 @@ static int b2_set_sv(B2PlanDev *P, cudaStream_t st) {
     off[m + 1] = off[m] + b2_sv_tasks_host(N * (N + 1) / 2);
   }
   P->sv_off_h = off;
-  int rc = b2_upload(&P->sv_off, P->sv_off_h, st);
+  int rc = b2_upload(&P->sv_off, P->sv_off_h, u);
   if (rc) return rc;
   P->sv_ntask = off[nmol];
   B2_TRY(cudaMalloc(&P->sv_work, sizeof(double) * 4 * (size_t)std::max(1ll, P->h.n_rows)));
@@ -102,7 +123,7 @@ static int b2_set_sv(B2PlanDev *P, cudaStream_t st) {
   b2_buckets(P, all, P->bkt_map_h, P->bkt_off_h);
   for (int b = 0; b < B2_NBKT; ++b) B2_TRY(cudaStreamCreateWithFlags(&P->bkt_stream[b], cudaStreamNonBlocking));
   for (int b = 0; b <= B2_NBKT; ++b) B2_TRY(cudaEventCreateWithFlags(&P->bkt_ev[b], cudaEventDisableTiming));
-  return b2_upload(&P->bkt_map, P->bkt_map_h, st);
+  return b2_upload(&P->bkt_map, P->bkt_map_h, u);
 }
 
 extern "C" {
@@ -126,26 +147,50 @@ int b2_plan_create(int nmol, const int *natm, const int *nbas, const int *atm, c
   if (rc) { delete P; return rc; }
   // every upload and table kernel goes to one non-blocking stream, synchronized once at the end
   // (no ordering with, or wait on, work the caller has queued elsewhere on the device)
-  cudaStream_t cs = nullptr;
-  if ((rc = b2_note(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking)))) { delete P; return rc; }
   std::vector<double> tab(B2_BOYS_NT * B2_BOYS_NM);
   b2_boys_fill_table(tab.data());
   std::vector<float> tab32(tab.begin(), tab.end());
-  if ((rc = b2_upload(&P->mols, P->h.mols, cs)) || (rc = b2_upload(&P->row_off, P->h.row_off, cs)) ||
-      (rc = b2_upload(&P->shells, P->h.shells, cs)) || (rc = b2_upload(&P->ao2sh, P->h.ao2sh, cs)) ||
-      (rc = b2_upload(&P->atom_xyz, P->h.atom_xyz, cs)) || (rc = b2_upload(&P->atom_z, P->h.atom_z, cs)) ||
-      (rc = b2_upload(&P->boys, tab, cs)) || (rc = b2_upload(&P->boys32, tab32, cs)) ||
-      (rc = b2_set_jk_chunk(P, 0, cs)) || (rc = b2_build_pairs(*P, cs)) || (rc = b2_set_sv(P, cs))) {
-    cudaStreamSynchronize(cs);
-    cudaStreamDestroy(cs);
+  const B2PlanHost &H = P->h;
+  size_t need = 16 * 256 + sizeof(B2MolDev) * H.mols.size() + sizeof(long long) * H.row_off.size() +
+                sizeof(B2Shell) * H.shells.size() + sizeof(int) * H.ao2sh.size() +
+                sizeof(double) * H.atom_xyz.size() + sizeof(int) * H.atom_z.size() +
+                sizeof(double) * tab.size() + sizeof(float) * tab32.size() +
+                (2 * sizeof(long long) + sizeof(int)) * (size_t)(nmol + 1);
+  std::lock_guard<std::mutex> lock(g_stage_mu);
+  if (need > g_stage_cap) {
+    if (g_stage) cudaFreeHost(g_stage);
+    g_stage = nullptr;
+    g_stage_cap = 0;
+    const size_t cap = need + need / 4;
+    if ((rc = b2_note(cudaMallocHost((void **)&g_stage, cap)))) { delete P; return rc; }
+    g_stage_cap = cap;
+  }
+  B2Upload u;
+  u.stage = g_stage;
+  u.cap = g_stage_cap;
+  if ((rc = b2_note(cudaStreamCreateWithFlags(&u.st, cudaStreamNonBlocking)))) { delete P; return rc; }
+  if ((rc = b2_upload(&P->mols, H.mols, &u)) || (rc = b2_upload(&P->row_off, H.row_off, &u)) ||
+      (rc = b2_upload(&P->shells, H.shells, &u)) || (rc = b2_upload(&P->ao2sh, H.ao2sh, &u)) ||
+      (rc = b2_upload(&P->atom_xyz, H.atom_xyz, &u)) || (rc = b2_upload(&P->atom_z, H.atom_z, &u)) ||
+      (rc = b2_upload(&P->boys, tab, &u)) || (rc = b2_upload(&P->boys32, tab32, &u)) ||
+      (rc = b2_set_jk_chunk(P, 0, &u)) || (rc = b2_build_pairs(*P, u.st)) || (rc = b2_set_sv(P, &u))) {
+    cudaStreamSynchronize(u.st);
+    cudaStreamDestroy(u.st);
     b2_plan_free(P);
     return rc;
   }
-  rc = b2_note(cudaStreamSynchronize(cs));
-  cudaStreamDestroy(cs);
+  rc = b2_note(cudaStreamSynchronize(u.st));
+  cudaStreamDestroy(u.st);
   if (rc) { b2_plan_free(P); return rc; }
+  P->h2d_bytes = (long long)u.bytes;
   cudaGetDevice(&P->device);
   *plan = P;
+  return B2_OK;
+}
+
+int b2_plan_h2d_bytes(void *plan, int64_t *bytes) {
+  if (!plan || !bytes) return B2_ERR_ARG;
+  *bytes = ((B2PlanDev *)plan)->h2d_bytes;
   return B2_OK;
 }
 

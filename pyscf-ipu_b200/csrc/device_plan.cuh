@@ -49,6 +49,7 @@ struct B2PlanDev {
   long long jk_chunk = 0;
   long long jk_nchunks = 0;
   int device = 0;
+  long long h2d_bytes = 0;                // bytes copied host -> device by plan creation
   B2GridDev g;
   B2EriTask *eri_tasks32 = nullptr, *eri_tasks64 = nullptr;
   std::vector<long long> eri_goff32, eri_goff64;   // task group (class combination) starts

@@ -83,3 +83,24 @@ def test_stream_gpu_matches_direct_batches(tmp_path):
     E = eng.run_converged()["energy"].cpu().numpy() * HARTREE_TO_EV
     eng.close()
     np.testing.assert_allclose(np.array(t["energy"]), E, atol=2e-3)   # eV, 1e-4 Ha
+
+
+@pytest.mark.gpu
+def test_run_batches_prefetch_matches_serial():
+    """the public batch API gives the same results with the next plan built on a worker thread
+    (overlapping the current batch) as without, and as one engine per batch"""
+    from b200dft.engine import RKSEngine, run_batches
+    b1 = [m for _, _, m in stream_chunk((5, 0, 12, 4))]
+    b2 = [m for _, _, m in stream_chunk((5, 12, 9, 5))]
+    pre = list(run_batches([b1, b2], guess="minao", prefetch=True))
+    ser = list(run_batches([b1, b2], guess="minao", prefetch=False))
+    assert [len(m) for m, _ in pre] == [12, 9]
+    for (_, a), (_, b) in zip(pre, ser):
+        # float32 atomics in the grid reductions: runs agree to rounding, not bit for bit
+        np.testing.assert_allclose(a["energy"], b["energy"], rtol=0, atol=1e-9)
+        np.testing.assert_array_equal(a["iterations"], b["iterations"])
+        assert a["converged"].all() and a["h2d_bytes"] > 0
+    eng = RKSEngine(b2, level=0, precision="mixed", guess="minao")
+    E = eng.run_converged()["energy"].cpu().numpy()
+    eng.close()
+    np.testing.assert_allclose(pre[1][1]["energy"], E, rtol=0, atol=1e-9)
