@@ -15,17 +15,20 @@
 //
 // The exchange list is built once per ERI list (k_exch_build: two gathers per entry from the
 // molecule's s8 list, which stays in L2).  The product kernel (k_symv) gives each warp a strip
-// of 128 columns and a block of 64 rows of one molecule: lanes own 4 columns each, read every
-// row segment with coalesced loads, keep the column sums y[Q] += A[P,Q] x[P] in float64
-// registers for the whole block and reduce each row sum y[P] += sum_Q A[P,Q] x[Q] with warp
-// shuffles; one float64 global atomic per row per strip and per column per block.  Every
-// product and sum is float64 (the lists may be stored in float32).  Algorithmic bytes per call:
-// 2 n4 sizeof(T) per molecule (both lists once).
+// of 128 columns and a block of 64 rows of one molecule: lanes own 4 columns each and copy every
+// row segment with coalesced cp.async into a 3-stage shared-memory ring (groups of 8 rows, two
+// groups in flight while one is reduced), keep the column sums y[Q] += A[P,Q] x[P] in float64
+// registers for the whole block and reduce the row sums y[P] += sum_Q A[P,Q] x[Q] of 8 rows at
+// a time with one transposed butterfly of warp shuffles; one float64 global atomic per row per
+// strip and per column per block.  Every product and sum is float64 (the lists may be stored in
+// float32).  Algorithmic bytes per call: 2 n4 sizeof(T) per molecule (both lists once).
 #include "device_plan.cuh"
 
 #define B2_SV_STRIP 128
 #define B2_SV_ROWS 64
-#define B2_SV_GROUP 8           // rows whose loads are in flight together
+#define B2_SV_GROUP 8           // rows per copy group (the row-sum butterfly is written for 8)
+#define B2_SV_STAGES 3          // copy groups in each warp's shared-memory ring
+#define B2_SV_WARPS 4           // warps (tasks) per CTA
 
 __device__ __forceinline__ long long b2_sv_untri(long long p) {
   long long i = (long long)((sqrt(8.0 * (double)p + 1.0) - 1.0) * 0.5);
@@ -100,14 +103,90 @@ __host__ __device__ inline long long b2_sv_tasks(long long n2) {
   return t;
 }
 
+// cp.async of one list entry into shared memory (zero fill when !ok; the address is then
+// not read but kept valid)
+template <int B>
+__device__ __forceinline__ void b2_cp_async(uint32_t dst, const void *src, bool ok);
+template <>
+__device__ __forceinline__ void b2_cp_async<4>(uint32_t dst, const void *src, bool ok) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" :: "r"(dst), "l"(src), "r"(ok ? 4 : 0) : "memory");
+}
+template <>
+__device__ __forceinline__ void b2_cp_async<8>(uint32_t dst, const void *src, bool ok) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" :: "r"(dst), "l"(src), "r"(ok ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void b2_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void b2_cp_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
+
+// copies of one row group (rows P0.. of the row block ending at r1, zero beyond it) into a
+// stage [B2_SV_GROUP][B2_SV_STRIP] of the warp's ring; each lane copies exactly the entries
+// it reads later (its 4 columns), so no cross-lane synchronisation is needed.  Pair indices
+// are int: a molecule's pair count n2 <= 3240 keeps tri(P) < 2^23.
 template <typename T>
-__global__ void __launch_bounds__(256)
+__device__ __forceinline__ void b2_sv_issue(const T *__restrict__ A, int P0, int r1, const int (&qc)[4],
+                                            uint32_t stage, int lane) {
+#pragma unroll
+  for (int rr = 0; rr < B2_SV_GROUP; ++rr) {
+    const int P = P0 + rr;
+    const T *row = A + (P * (P + 1) >> 1);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const bool ok = P < r1 && qc[c] <= P;
+      b2_cp_async<sizeof(T)>(stage + (uint32_t)((rr * B2_SV_STRIP + lane + 32 * c) * sizeof(T)),
+                             ok ? (const void *)(row + qc[c]) : (const void *)A, ok);
+    }
+  }
+}
+
+// one row group: column sums into yc, row sums reduced over the warp and added to y
+template <typename T>
+__device__ __forceinline__ void b2_sv_use(const T *__restrict__ st, const double *__restrict__ x, int P0,
+                                          int r1, const int (&qc)[4], const double (&xq)[4], double (&yc)[4],
+                                          double *__restrict__ y, int lane) {
+  double rs[B2_SV_GROUP];
+#pragma unroll
+  for (int rr = 0; rr < B2_SV_GROUP; ++rr) {
+    const int P = P0 + rr;
+    const double xp = P < r1 ? x[P] : 0.0;
+    rs[rr] = 0.0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      const double av = (double)st[rr * B2_SV_STRIP + lane + 32 * c];
+      rs[rr] += av * xq[c];
+      if (qc[c] < P) yc[c] += av * xp;
+    }
+  }
+  // transposed butterfly: each step hands half of the remaining rows to the partner lane,
+  // 4 + 2 + 1 + 1 + 1 shuffles for the 8 rows; lane 4r ends with the warp total of row r
+  const bool h16 = lane & 16, h8 = lane & 8, h4 = lane & 4;
+  double s4[4], s2[2];
+#pragma unroll
+  for (int k = 0; k < 4; ++k)                  // s4[k]: row (h16 ? 4 : 0) + k
+    s4[k] = (h16 ? rs[k + 4] : rs[k]) + __shfl_xor_sync(0xffffffffu, h16 ? rs[k] : rs[k + 4], 16);
+#pragma unroll
+  for (int k = 0; k < 2; ++k)                  // s2[k]: row (h16 ? 4 : 0) + (h8 ? 2 : 0) + k
+    s2[k] = (h8 ? s4[k + 2] : s4[k]) + __shfl_xor_sync(0xffffffffu, h8 ? s4[k] : s4[k + 2], 8);
+  double s1 = (h4 ? s2[1] : s2[0]) + __shfl_xor_sync(0xffffffffu, h4 ? s2[0] : s2[1], 4);
+  s1 += __shfl_xor_sync(0xffffffffu, s1, 2);
+  s1 += __shfl_xor_sync(0xffffffffu, s1, 1);
+  if ((lane & 3) == 0 && P0 + (lane >> 2) < r1 && s1 != 0.0) atomicAdd(&y[P0 + (lane >> 2)], s1);
+}
+
+template <typename T>
+__host__ __device__ constexpr int b2_sv_smem() {    // bytes per CTA
+  return B2_SV_WARPS * B2_SV_STAGES * B2_SV_GROUP * B2_SV_STRIP * (int)sizeof(T);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(32 * B2_SV_WARPS)
 k_symv(const B2MolDev *__restrict__ mols, const long long *__restrict__ task_off, int nmol,
        const int *__restrict__ active, const int *__restrict__ mol_map, const T *__restrict__ eri,
        const T *__restrict__ exch, const double *__restrict__ xJ, const double *__restrict__ xK,
        double *__restrict__ yJ, double *__restrict__ yK) {
-  const int lane = threadIdx.x & 31;
-  const long long t = (long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  extern __shared__ __align__(16) unsigned char sv_smem[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const long long t = (long long)blockIdx.x * B2_SV_WARPS + w;
   if (t >= task_off[nmol]) return;
   int lo = 0, hi = nmol - 1;
   while (lo < hi) {
@@ -117,20 +196,20 @@ k_symv(const B2MolDev *__restrict__ mols, const long long *__restrict__ task_off
   const int m = mol_map ? mol_map[lo] : lo;
   if (active && !active[m]) return;
   const B2MolDev md = mols[m];
-  const long long n2 = (long long)md.nao * (md.nao + 1) / 2;
+  const int n2 = md.nao * (md.nao + 1) / 2;
   // blockIdx.y: 0 = J (s8 list, x_J), 1 = K (exchange list, x_K)
   const T *A = (blockIdx.y == 0 ? eri : exch) + md.eri_off;
   const double *x = (blockIdx.y == 0 ? xJ : xK) + md.row_off;
   double *y = (blockIdx.y == 0 ? yJ : yK) + md.row_off;
-  long long u = t - task_off[lo], q0 = 0;
+  int u = (int)(t - task_off[lo]), q0 = 0;
   for (;;) {                                   // strip and row block of local task u
-    const long long nb = (n2 - q0 + B2_SV_ROWS - 1) / B2_SV_ROWS;
+    const int nb = (n2 - q0 + B2_SV_ROWS - 1) / B2_SV_ROWS;
     if (u < nb) break;
     u -= nb;
     q0 += B2_SV_STRIP;
   }
-  const long long r0 = q0 + u * B2_SV_ROWS, r1 = min(r0 + B2_SV_ROWS, n2);
-  long long qc[4];
+  const int r0 = q0 + u * B2_SV_ROWS, r1 = min(r0 + B2_SV_ROWS, n2);
+  int qc[4];
   double xq[4], yc[4];
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
@@ -138,42 +217,24 @@ k_symv(const B2MolDev *__restrict__ mols, const long long *__restrict__ task_off
     xq[c] = qc[c] < n2 ? x[qc[c]] : 0.0;
     yc[c] = 0.0;
   }
-  // rows in groups of B2_SV_GROUP: all loads of a group are issued before any is used (the
-  // kernel is bound by memory latency otherwise), and the group's row reductions interleave
-  for (long long P0 = r0; P0 < r1; P0 += B2_SV_GROUP) {
-    T a[B2_SV_GROUP][4];
-    double xp[B2_SV_GROUP];
+  // ring of B2_SV_STAGES row groups per warp: group g + STAGES - 1 is copied while group g is
+  // reduced (the kernel is bound by memory latency otherwise)
+  constexpr int SB = B2_SV_GROUP * B2_SV_STRIP;                   // entries per stage
+  T *ring = reinterpret_cast<T *>(sv_smem) + (size_t)w * B2_SV_STAGES * SB;
+  const uint32_t ring_s = (uint32_t)__cvta_generic_to_shared(ring);
+  const int ng = (r1 - r0 + B2_SV_GROUP - 1) / B2_SV_GROUP;
 #pragma unroll
-    for (int rr = 0; rr < B2_SV_GROUP; ++rr) {
-      const long long P = P0 + rr;
-      const bool ok = P < r1;
-      const T *row = A + b2_tri(P);
-      xp[rr] = ok ? x[P] : 0.0;
-#pragma unroll
-      for (int c = 0; c < 4; ++c) a[rr][c] = (ok && qc[c] <= P) ? row[qc[c]] : (T)0;
-    }
-    double rs[B2_SV_GROUP];
-#pragma unroll
-    for (int rr = 0; rr < B2_SV_GROUP; ++rr) {
-      const long long P = P0 + rr;
-      rs[rr] = 0.0;
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const double av = (double)a[rr][c];
-        rs[rr] += av * xq[c];
-        if (qc[c] < P) yc[c] += av * xp[rr];
-      }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-      for (int rr = 0; rr < B2_SV_GROUP; ++rr) rs[rr] += __shfl_xor_sync(0xffffffffu, rs[rr], o);
-    if (lane < B2_SV_GROUP && P0 + lane < r1) {
-      double v = rs[0];
-#pragma unroll
-      for (int rr = 1; rr < B2_SV_GROUP; ++rr) v = lane == rr ? rs[rr] : v;
-      if (v != 0.0) atomicAdd(&y[P0 + lane], v);
-    }
+  for (int g = 0; g < B2_SV_STAGES - 1; ++g) {
+    if (g < ng) b2_sv_issue(A, r0 + g * B2_SV_GROUP, r1, qc, ring_s + (uint32_t)(g * SB * sizeof(T)), lane);
+    b2_cp_commit();
+  }
+  for (int g = 0; g < ng; ++g) {
+    const int gn = g + B2_SV_STAGES - 1;
+    if (gn < ng)
+      b2_sv_issue(A, r0 + gn * B2_SV_GROUP, r1, qc, ring_s + (uint32_t)((gn % B2_SV_STAGES) * SB * sizeof(T)), lane);
+    b2_cp_commit();
+    b2_cp_wait<B2_SV_STAGES - 1>();            // this lane's copies of group g have landed
+    b2_sv_use(ring + (g % B2_SV_STAGES) * SB, x, r0 + g * B2_SV_GROUP, r1, qc, xq, yc, y, lane);
   }
 #pragma unroll
   for (int c = 0; c < 4; ++c)
@@ -226,13 +287,18 @@ int b2_launch_jk_symv(const B2PlanDev &P, int precision, const int *active, cons
   k_sv_x<<<nm, 256, 0, st>>>(P.mols, active, map, D, xJ, xK, yJ, yK);
   b2_count_launches(1);
   if (ntask > 0) {
-    const dim3 grid((unsigned)((ntask + 7) / 8), 2);
-    if (precision == 64)
-      k_symv<double><<<grid, 256, 0, st>>>(P.mols, toff, nm, active, map, (const double *)eri,
-                                           (const double *)exch, xJ, xK, yJ, yK);
-    else
-      k_symv<float><<<grid, 256, 0, st>>>(P.mols, toff, nm, active, map, (const float *)eri,
-                                          (const float *)exch, xJ, xK, yJ, yK);
+    const dim3 grid((unsigned)((ntask + B2_SV_WARPS - 1) / B2_SV_WARPS), 2);
+    if (precision == 64) {
+      B2_CUDA_TRY(cudaFuncSetAttribute(k_symv<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       b2_sv_smem<double>()));
+      k_symv<double><<<grid, 32 * B2_SV_WARPS, b2_sv_smem<double>(), st>>>(
+          P.mols, toff, nm, active, map, (const double *)eri, (const double *)exch, xJ, xK, yJ, yK);
+    } else {
+      B2_CUDA_TRY(cudaFuncSetAttribute(k_symv<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       b2_sv_smem<float>()));
+      k_symv<float><<<grid, 32 * B2_SV_WARPS, b2_sv_smem<float>(), st>>>(
+          P.mols, toff, nm, active, map, (const float *)eri, (const float *)exch, xJ, xK, yJ, yK);
+    }
     b2_count_launches(1);
   }
   k_sv_out<<<nm, 256, 0, st>>>(P.mols, active, map, yJ, yK, J, K);
