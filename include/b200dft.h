@@ -71,6 +71,10 @@ int b2_plan_set_xc_tiles(b2_plan_t plan, int tiles_per_cta);
 /* Error code of the tensor-core XC kernel's bounded waits (0 = none); reset != 0 clears it. */
 int b2_xc_tc_status(int reset, int *status);
 
+/* Error flag of the J/K product kernel's copy waits (0 = none; 1 = a wait on a row-group
+ * copy gave up and that warp's contribution is missing); reset != 0 clears it after reading. */
+int b2_jk_status(int reset, int *status);
+
 /* Restrict the J/K and XC launches to a subset of the batch's molecules (host int[n] molecule
  * indices; n = 0 restores the full batch).  Used when few molecules are still iterating, so the
  * launches cover only their work. */
@@ -96,8 +100,9 @@ int b2_jk_s8(b2_plan_t plan, int precision, const int *active, const void *eri, 
  * (an equivalent regrouping of the sums of sparse_symmetric_ERI.py:86-137). */
 int b2_jk_exchange(b2_plan_t plan, int precision, const void *eri, void *exch, void *stream);
 /* J and K as b2_jk_s8, computed as two symmetric matrix-vector products over the s8 list and
- * the exchange list (float64 arithmetic, no shared-memory atomics).  Uses a plan-owned
- * workspace: one call at a time per plan. */
+ * the exchange list (float64 arithmetic, no shared-memory atomics).  Both lists must start
+ * 16-byte aligned (B2_ERR_ARG otherwise) and hold the plan's padded layout (n_eri_total
+ * entries).  Uses a plan-owned workspace: one call at a time per plan. */
 int b2_jk_pairs(b2_plan_t plan, int precision, const int *active, const void *eri,
                 const void *exch, const double *D, double *J, double *K, void *stream);
 

@@ -245,6 +245,14 @@ int b2_xc_tc_status(int reset, int *status) {
   return B2_OK;
 }
 
+int b2_jk_status(int reset, int *status) {
+  if (!status) return B2_ERR_ARG;
+  const int v = b2_jk_status_read(reset);
+  if (v < 0) return B2_ERR_CUDA;
+  *status = v;
+  return B2_OK;
+}
+
 int b2_plan_set_subset(void *plan, const int *mols, int n) {
   if (!plan || n < 0 || (n > 0 && !mols)) return B2_ERR_ARG;
   B2PlanDev *P = (B2PlanDev *)plan;

@@ -74,6 +74,7 @@ int b2_launch_jk_symv(const B2PlanDev &P, int precision, const int *active, cons
                       const void *exch, const double *D, double *J, double *K, double *work,
                       cudaStream_t st);
 long long b2_sv_tasks_host(long long n2);
+int b2_jk_status_read(int reset);     // error flag of the J/K product kernel (-1: CUDA error)
 int b2_launch_jk_s8(const B2PlanDev &P, int precision, const int *active, const void *eri,
                     const double *D, double *J, double *K, cudaStream_t st);
 int b2_zero_active(const B2PlanDev &P, const int *active, double *A, double *B, cudaStream_t st);

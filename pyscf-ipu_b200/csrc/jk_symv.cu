@@ -15,9 +15,9 @@
 //
 // The exchange list is built once per ERI list (k_exch_build: two gathers per entry from the
 // molecule's s8 list, which stays in L2).  The product kernel (k_symv) gives each warp a strip
-// of 128 columns and a block of 64 rows of one molecule: lanes own 4 columns each and copy every
-// row segment with coalesced cp.async into a 3-stage shared-memory ring (groups of 8 rows, two
-// groups in flight while one is reduced), keep the column sums y[Q] += A[P,Q] x[P] in float64
+// of 128 columns and a block of 64 rows of one molecule: lanes own 4 columns each; every row
+// segment arrives by one bulk copy (8 lanes issue a group's 8 rows) in a 3-stage shared-memory
+// ring (groups of 8 rows, two groups in flight while one is reduced), keep the column sums y[Q] += A[P,Q] x[P] in float64
 // registers for the whole block and reduce the row sums y[P] += sum_Q A[P,Q] x[Q] of 8 rows at
 // a time with one transposed butterfly of warp shuffles; one float64 global atomic per row per
 // strip and per column per block.  Every product and sum is float64 (the lists may be stored in
@@ -25,10 +25,16 @@
 #include "device_plan.cuh"
 
 #define B2_SV_STRIP 128
-#define B2_SV_ROWS 64
+#ifndef B2_SV_ROWS
+#define B2_SV_ROWS 64           // rows per warp task
+#endif
 #define B2_SV_GROUP 8           // rows per copy group (the row-sum butterfly is written for 8)
+#ifndef B2_SV_STAGES
 #define B2_SV_STAGES 3          // copy groups in each warp's shared-memory ring
+#endif
+#ifndef B2_SV_WARPS
 #define B2_SV_WARPS 4           // warps (tasks) per CTA
+#endif
 
 __device__ __forceinline__ long long b2_sv_untri(long long p) {
   long long i = (long long)((sqrt(8.0 * (double)p + 1.0) - 1.0) * 0.5);
@@ -103,56 +109,80 @@ __host__ __device__ inline long long b2_sv_tasks(long long n2) {
   return t;
 }
 
-// cp.async of one list entry into shared memory (zero fill when !ok; the address is then
-// not read but kept valid)
-template <int B>
-__device__ __forceinline__ void b2_cp_async(uint32_t dst, const void *src, bool ok);
-template <>
-__device__ __forceinline__ void b2_cp_async<4>(uint32_t dst, const void *src, bool ok) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" :: "r"(dst), "l"(src), "r"(ok ? 4 : 0) : "memory");
-}
-template <>
-__device__ __forceinline__ void b2_cp_async<8>(uint32_t dst, const void *src, bool ok) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" :: "r"(dst), "l"(src), "r"(ok ? 8 : 0) : "memory");
-}
-__device__ __forceinline__ void b2_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void b2_cp_wait() { asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory"); }
+__device__ int g_b2_sv_err = 0;   // 1: a wait on a row-group copy gave up (status: b2_jk_status)
 
-// copies of one row group (rows P0.. of the row block ending at r1, zero beyond it) into a
-// stage [B2_SV_GROUP][B2_SV_STRIP] of the warp's ring; each lane copies exactly the entries
-// it reads later (its 4 columns), so no cross-lane synchronisation is needed.  Pair indices
-// are int: a molecule's pair count n2 <= 3240 keeps tri(P) < 2^23.
-template <typename T>
-__device__ __forceinline__ void b2_sv_issue(const T *__restrict__ A, int P0, int r1, const int (&qc)[4],
-                                            uint32_t stage, int lane) {
-#pragma unroll
-  for (int rr = 0; rr < B2_SV_GROUP; ++rr) {
-    const int P = P0 + rr;
-    const T *row = A + (P * (P + 1) >> 1);
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const bool ok = P < r1 && qc[c] <= P;
-      b2_cp_async<sizeof(T)>(stage + (uint32_t)((rr * B2_SV_STRIP + lane + 32 * c) * sizeof(T)),
-                             ok ? (const void *)(row + qc[c]) : (const void *)A, ok);
-    }
+#define B2_SV_SPIN (1 << 22)       // polls of an mbarrier before a wait gives up
+
+__device__ __forceinline__ void b2_sv_mbar_init(uint32_t a) {     // one arrival per row of a group
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(a), "n"(B2_SV_GROUP) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void b2_sv_expect(uint32_t a, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(a), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void b2_sv_bulk(uint32_t dst, const void *src, uint32_t bytes, uint32_t mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               :: "r"(dst), "l"(src), "r"(bytes), "r"(mbar) : "memory");
+}
+__device__ __forceinline__ bool b2_sv_wait(uint32_t a, uint32_t parity) {
+  for (int it = 0; it < B2_SV_SPIN; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok) : "r"(a), "r"(parity) : "memory");
+    if (ok) return true;
   }
+  return false;
 }
 
-// one row group: column sums into yc, row sums reduced over the warp and added to y
+// Row segments of one row group (rows P0.., the row block ends at r1) -> one stage of the warp's
+// ring: lane rr < B2_SV_GROUP copies row P0 + rr with one bulk copy of A[P, q0 .. min(q0+128,
+// P+1)), widened to the 16-byte-aligned bytes around it (the molecule's list starts 128-byte
+// aligned and is padded to a multiple of 32 entries, so the widened range stays inside it), and
+// arrives on the stage's mbarrier (8 arrivals, each expecting its own bytes; a lane without a row
+// arrives expecting none).  Row rr lands at byte rr * b2_sv_rb of the stage with its first entry
+// at in-row offset (tri(P) + q0) mod (16 / sizeof(T)).  Pair indices are int: n2 <= 3240 keeps
+// tri(P) < 2^23.
 template <typename T>
-__device__ __forceinline__ void b2_sv_use(const T *__restrict__ st, const double *__restrict__ x, int P0,
-                                          int r1, const int (&qc)[4], const double (&xq)[4], double (&yc)[4],
-                                          double *__restrict__ y, int lane) {
+__host__ __device__ constexpr int b2_sv_rb() { return B2_SV_STRIP * (int)sizeof(T) + 32; }   // row bytes
+template <typename T>
+__device__ __forceinline__ void b2_sv_issue(const T *__restrict__ A, int P0, int r1, int q0, uint32_t stage,
+                                            uint32_t mbar, int lane) {
+  if (lane >= B2_SV_GROUP) return;
+  const int P = P0 + lane;
+  uint32_t bytes = 0;
+  long long a0 = 0;
+  if (P < r1) {
+    const long long e0 = (P * (P + 1) >> 1) + q0;
+    const long long b0 = e0 * (long long)sizeof(T);
+    const long long b1 = (e0 + min(q0 + B2_SV_STRIP, P + 1) - q0) * (long long)sizeof(T);
+    a0 = b0 & ~15ll;
+    bytes = (uint32_t)(((b1 + 15) & ~15ll) - a0);
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  b2_sv_expect(mbar, bytes);
+  if (bytes) b2_sv_bulk(stage + (uint32_t)(lane * b2_sv_rb<T>()), reinterpret_cast<const char *>(A) + a0, bytes, mbar);
+}
+
+// one row group from its stage: column sums into yc, row sums reduced over the warp into y
+template <typename T>
+__device__ __forceinline__ void b2_sv_use(const unsigned char *__restrict__ stage, const double *__restrict__ x,
+                                          int P0, int r1, int q0, const int (&qc)[4], const double (&xq)[4],
+                                          double (&yc)[4], double *__restrict__ y, int lane) {
+  constexpr int MSK = 16 / (int)sizeof(T) - 1;
   double rs[B2_SV_GROUP];
 #pragma unroll
   for (int rr = 0; rr < B2_SV_GROUP; ++rr) {
     const int P = P0 + rr;
-    const double xp = P < r1 ? x[P] : 0.0;
+    const bool ok = P < r1;
+    const T *row = reinterpret_cast<const T *>(stage + rr * b2_sv_rb<T>()) + (((P * (P + 1) >> 1) + q0) & MSK);
+    const double xp = ok ? x[P] : 0.0;
     rs[rr] = 0.0;
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      const double av = (double)st[rr * B2_SV_STRIP + lane + 32 * c];
+      // entries past the row's end (Q > P) and rows past the block are not copied: masked
+      const double av = (ok && qc[c] <= P) ? (double)row[lane + 32 * c] : 0.0;
       rs[rr] += av * xq[c];
       if (qc[c] < P) yc[c] += av * xp;
     }
@@ -174,8 +204,10 @@ __device__ __forceinline__ void b2_sv_use(const T *__restrict__ st, const double
 }
 
 template <typename T>
-__host__ __device__ constexpr int b2_sv_smem() {    // bytes per CTA
-  return B2_SV_WARPS * B2_SV_STAGES * B2_SV_GROUP * B2_SV_STRIP * (int)sizeof(T);
+__host__ __device__ constexpr int b2_sv_stage_bytes() { return B2_SV_GROUP * b2_sv_rb<T>(); }
+template <typename T>
+__host__ __device__ constexpr int b2_sv_smem() {    // bytes per CTA: the rings, then the mbarriers
+  return B2_SV_WARPS * B2_SV_STAGES * (b2_sv_stage_bytes<T>() + 8);
 }
 
 template <typename T>
@@ -219,22 +251,34 @@ k_symv(const B2MolDev *__restrict__ mols, const long long *__restrict__ task_off
   }
   // ring of B2_SV_STAGES row groups per warp: group g + STAGES - 1 is copied while group g is
   // reduced (the kernel is bound by memory latency otherwise)
-  constexpr int SB = B2_SV_GROUP * B2_SV_STRIP;                   // entries per stage
-  T *ring = reinterpret_cast<T *>(sv_smem) + (size_t)w * B2_SV_STAGES * SB;
+  constexpr int SB = b2_sv_stage_bytes<T>();
+  unsigned char *ring = sv_smem + (size_t)w * B2_SV_STAGES * SB;
   const uint32_t ring_s = (uint32_t)__cvta_generic_to_shared(ring);
+  const uint32_t mbar_s = (uint32_t)__cvta_generic_to_shared(sv_smem + B2_SV_WARPS * B2_SV_STAGES * SB) +
+                          8u * (uint32_t)(w * B2_SV_STAGES);
   const int ng = (r1 - r0 + B2_SV_GROUP - 1) / B2_SV_GROUP;
-#pragma unroll
-  for (int g = 0; g < B2_SV_STAGES - 1; ++g) {
-    if (g < ng) b2_sv_issue(A, r0 + g * B2_SV_GROUP, r1, qc, ring_s + (uint32_t)(g * SB * sizeof(T)), lane);
-    b2_cp_commit();
+  if (lane == 0)
+    for (int k = 0; k < B2_SV_STAGES; ++k) b2_sv_mbar_init(mbar_s + 8u * k);
+  __syncwarp();
+  for (int g = 0; g < B2_SV_STAGES - 1 && g < ng; ++g)
+    b2_sv_issue(A, r0 + g * B2_SV_GROUP, r1, q0, ring_s + (uint32_t)(g * SB), mbar_s + 8u * g, lane);
+  int g = 0;
+  for (; g < ng; ++g) {
+    const int gn = g + B2_SV_STAGES - 1, sn = gn % B2_SV_STAGES, sc = g % B2_SV_STAGES;
+    __syncwarp();                              // every lane is done with stage sn (group g - 1)
+    if (gn < ng) b2_sv_issue(A, r0 + gn * B2_SV_GROUP, r1, q0, ring_s + (uint32_t)(sn * SB), mbar_s + 8u * sn, lane);
+    const bool landed = b2_sv_wait(mbar_s + 8u * sc, (uint32_t)((g / B2_SV_STAGES) & 1));
+    if (!__all_sync(0xffffffffu, landed)) {    // warp-uniform: the reduction below needs every lane
+      if (lane == 0) atomicExch(&g_b2_sv_err, 1);
+      break;
+    }
+    b2_sv_use<T>(ring + sc * SB, x, r0 + g * B2_SV_GROUP, r1, q0, qc, xq, yc, y, lane);
   }
-  for (int g = 0; g < ng; ++g) {
-    const int gn = g + B2_SV_STAGES - 1;
-    if (gn < ng)
-      b2_sv_issue(A, r0 + gn * B2_SV_GROUP, r1, qc, ring_s + (uint32_t)((gn % B2_SV_STAGES) * SB * sizeof(T)), lane);
-    b2_cp_commit();
-    b2_cp_wait<B2_SV_STAGES - 1>();            // this lane's copies of group g have landed
-    b2_sv_use(ring + (g % B2_SV_STAGES) * SB, x, r0 + g * B2_SV_GROUP, r1, qc, xq, yc, y, lane);
+  if (g < ng) {
+    // gave up: wait (bounded) for the copies still in flight into this warp's ring, then leave
+    for (int k = g; k < ng && k < g + B2_SV_STAGES; ++k)
+      b2_sv_wait(mbar_s + 8u * (k % B2_SV_STAGES), (uint32_t)((k / B2_SV_STAGES) & 1));
+    return;
   }
 #pragma unroll
   for (int c = 0; c < 4; ++c)
@@ -276,6 +320,9 @@ int b2_launch_jk_symv(const B2PlanDev &P, int precision, const int *active, cons
                       const void *exch, const double *D, double *J, double *K, double *work,
                       cudaStream_t st) {
   if (precision != 64 && precision != 32) return B2_ERR_ARG;
+  // the product kernel bulk-copies row segments widened to 16-byte boundaries: both lists must
+  // start 16-byte aligned (every molecule's list then starts 128-byte aligned)
+  if ((reinterpret_cast<uintptr_t>(eri) | reinterpret_cast<uintptr_t>(exch)) & 15) return B2_ERR_ARG;
   const bool sub = P.sub.n > 0;
   const int nm = sub ? P.sub.n : P.h.nmol;
   const int *map = sub ? P.sub.mol_map : nullptr;
@@ -308,3 +355,13 @@ int b2_launch_jk_symv(const B2PlanDev &P, int precision, const int *active, cons
 }
 
 long long b2_sv_tasks_host(long long n2) { return b2_sv_tasks(n2); }
+
+int b2_jk_status_read(int reset) {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_b2_sv_err, sizeof(int)) != cudaSuccess) return -1;
+  if (reset) {
+    const int z = 0;
+    if (cudaMemcpyToSymbol(g_b2_sv_err, &z, sizeof(int)) != cudaSuccess) return -1;
+  }
+  return v;
+}

@@ -120,6 +120,9 @@ def test_jk_pairs_parity(cuda, prec):
     check(lib().b2_jk_pairs(P.h, prec, ptr(active), ptr(eri_t), ptr(exch), ptr(D), ptr(J), ptr(K),
                             stream_handle()), "jk_pairs")
     torch.cuda.synchronize()
+    st = ctypes.c_int(-1)
+    check(lib().b2_jk_status(1, ctypes.byref(st)), "b2_jk_status")
+    assert st.value == 0                       # no row-group copy wait gave up
     Jh, Kh = J.cpu().numpy(), K.cpu().numpy()
     for mi, (m, g) in enumerate(zip(mols, gs)):
         if mi == 1:
