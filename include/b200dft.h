@@ -53,6 +53,11 @@ int b2_plan_destroy(b2_plan_t plan);
  *              jk_chunk, jk_nchunks */
 int b2_plan_info(b2_plan_t plan, int64_t *info);
 
+/* Plans and grid tables take device memory from a per-device pool that keeps freed blocks for
+ * the next plan (no device synchronisation between batches).  This returns the pool's unused
+ * blocks to the driver. */
+int b2_release_cached_memory(void);
+
 /* Bytes plan creation copied host -> device (its tables, staged in pinned host memory). */
 int b2_plan_h2d_bytes(b2_plan_t plan, int64_t *bytes);
 

@@ -21,6 +21,7 @@ _D = ctypes.c_double
 # name -> argtypes (all return int status)
 SIGNATURES = {
     "b2_version": [],
+    "b2_release_cached_memory": [],
     "b2_launch_count": [_P],
     "b2_plan_create": [_I, _P, _P, _P, _P, _P, _P, _P],
     "b2_plan_destroy": [_P],

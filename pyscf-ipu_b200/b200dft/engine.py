@@ -24,6 +24,19 @@ NMO = 72     # mo_energy row stride used by the device kernels
 NZ = 10      # nuclear charges 0..9 indexed in the grid template table
 
 
+_SIDE = {}
+
+
+def _side_stream(device):
+    """one high-priority side stream per device, shared by every engine: memory the caching
+    allocator hands out on a stream is reused only by later allocations on that stream"""
+    d = torch.device(device)
+    key = d.index if d.index is not None else torch.cuda.current_device()
+    if key not in _SIDE:
+        _SIDE[key] = torch.cuda.Stream(torch.device("cuda", key), priority=-1)
+    return _SIDE[key]
+
+
 class Plan:
     """Owner of a ``b2_plan_t`` built from the molecules' libcint arrays."""
 
@@ -242,7 +255,7 @@ class RKSEngine:
             return
         self._guess_pending = False
         if self._side is None:
-            self._side = torch.cuda.Stream(self.device, priority=-1)
+            self._side = _side_stream(self.device)
         self._side.wait_event(self._guess_after)
         if self.D0_minao is None:
             self.D0_minao = torch.empty_like(self.D0)
@@ -408,8 +421,10 @@ class RKSEngine:
             c0 = launch_count()
             with torch.cuda.stream(st):
                 # explicit capture: torch.cuda.graph() would also run gc.collect() and release
-                # the allocator cache (both slow for large batches, neither needed here)
-                g.capture_begin()
+                # the allocator cache (both slow for large batches, neither needed here).
+                # Thread-local mode: another thread may build the next batch's plan (allocations,
+                # copies, synchronisation) meanwhile without invalidating this capture.
+                g.capture_begin(capture_error_mode="thread_local")
                 try:
                     self.step(use_diis)
                 finally:
@@ -477,11 +492,15 @@ class RKSEngine:
         self.plan.close()
 
 
-def _run_one(mols, plan, level, precision, guess, net, run_kw):
+def _run_one(mols, plan, level, precision, guess, net, run_kw, after_prepare=None):
     """one batch to convergence; returns host arrays, the engine's device memory released
-    (back to the allocator cache, where the next batch's engine finds it)"""
+    (back to the allocator cache, where the next batch's engine finds it).  ``after_prepare``
+    runs once the batch's setup and ERI work is queued."""
     eng = RKSEngine(mols, level=level, precision=precision, guess=guess, net=net, plan=plan)
     try:
+        eng.prepare()
+        if after_prepare is not None:
+            after_prepare()
         r = eng.run_converged(**run_kw)
         out = {k: r[k].cpu().numpy() for k in ("energy", "iterations", "converged", "mo_energy",
                                                "last5", "diis_err")}
@@ -498,9 +517,9 @@ def run_batches(batches, level=0, precision="mixed", guess="learned", net=None, 
     converged, mo_energy, last5, diis_err).
 
     With ``prefetch`` the next batch's plan (host tables, upload and device table build on the
-    plan's own stream) is made on a worker thread while the current batch runs on the GPU; the
-    C call releases the interpreter lock, so the two overlap.  ``run_kw`` goes to
-    ``run_converged``."""
+    plan's own stream) is made on a worker thread while the current batch runs on the GPU (from
+    the moment its ERI work is queued); the C call releases the interpreter lock, so the two
+    overlap.  ``run_kw`` goes to ``run_converged``."""
     from concurrent.futures import ThreadPoolExecutor
     if guess == "learned" and net is None:
         from .train_guess import load
@@ -515,13 +534,20 @@ def run_batches(batches, level=0, precision="mixed", guess="learned", net=None, 
     ex = ThreadPoolExecutor(1) if prefetch else None
     try:
         first = next(it, None)
-        pending = None if first is None else (ex.submit(make, first) if ex else make(first))
-        while pending is not None:
-            mols, plan = pending.result() if ex else pending
+        cur = None if first is None else make(first)
+        while cur is not None:
+            mols, plan = cur
             nxt = next(it, None)
-            pending = None if nxt is None else (ex.submit(make, nxt) if ex else make(nxt))
-            out = _run_one(mols, plan, level, precision, guess, net, run_kw)
+            fut = []
+            # the next plan's table kernels start once this batch's setup and ERI kernels are
+            # queued, so they do not hold up the kernels this batch waits on first
+            start = (lambda: fut.append(ex.submit(make, nxt))) if (ex and nxt is not None) else None
+            out = _run_one(mols, plan, level, precision, guess, net, run_kw, after_prepare=start)
             del plan                      # the engine and plan are released before the next batch
+            if nxt is None:
+                cur = None
+            else:
+                cur = fut[0].result() if fut else make(nxt)
             yield mols, out
     finally:
         if ex:

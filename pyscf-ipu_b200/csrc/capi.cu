@@ -4,6 +4,7 @@
 #include <string>
 #include <algorithm>
 #include "device_plan.cuh"
+#include "devmem.cuh"
 #include "xc.cuh"
 #include "scf.cuh"
 #include "xc_math.cuh"
@@ -22,6 +23,43 @@ static int b2_note(cudaError_t e) {
 
 #define B2_TRY(x) do { int _rc = b2_note(x); if (_rc) return _rc; } while (0)
 
+static std::mutex g_pool_mu;
+static cudaMemPool_t g_pool[64] = {};
+
+static cudaError_t b2_pool(cudaMemPool_t *out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  if (!g_pool[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if ((e = cudaMemPoolCreate(&pool, &props)) != cudaSuccess) return e;
+    uint64_t keep = ~0ull;
+    int no = 0;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    cudaMemPoolSetAttribute(pool, cudaMemPoolReuseAllowInternalDependencies, &no);
+    g_pool[dev] = pool;
+  }
+  *out = g_pool[dev];
+  return cudaSuccess;
+}
+
+cudaError_t b2_dmalloc(void **p, size_t bytes, cudaStream_t st) {
+  cudaMemPool_t pool = nullptr;
+  cudaError_t e = b2_pool(&pool);
+  if (e != cudaSuccess) return e;
+  return cudaMallocFromPoolAsync(p, bytes ? bytes : 16, pool, st);
+}
+
+void b2_dfree(void *p, cudaStream_t st) {
+  if (p) cudaFreeAsync(p, st);
+}
+
 // Plan uploads: every table is packed into one pinned staging buffer (kept and reused by later
 // plans, grown when a larger batch needs it) and copied with cudaMemcpyAsync on the plan's
 // stream; the staging lock is held until that stream has been synchronized.
@@ -38,7 +76,7 @@ static size_t g_stage_cap = 0;
 template <typename T>
 static int b2_upload(T **dst, const std::vector<T> &src, B2Upload *u = nullptr) {
   size_t n = std::max<size_t>(1, src.size());
-  B2_TRY(cudaMalloc((void **)dst, sizeof(T) * n));
+  B2_TRY(b2_dmalloc_t(dst, sizeof(T) * n, u ? u->st : nullptr));
   if (src.empty()) return B2_OK;
   const size_t nb = sizeof(T) * src.size();
   if (!u) {
@@ -55,21 +93,24 @@ static int b2_upload(T **dst, const std::vector<T> &src, B2Upload *u = nullptr) 
 }
 
 static void b2_subset_free(B2PlanDev *P) {
-  cudaFree(P->sub.mol_map); cudaFree(P->sub.jk_off); cudaFree(P->sub.x32); cudaFree(P->sub.x64);
-  cudaFree(P->sub.xtc); cudaFree(P->sub.sv_off); cudaFree(P->sub.bkt_map);
+  b2_dfree(P->sub.mol_map); b2_dfree(P->sub.jk_off); b2_dfree(P->sub.x32); b2_dfree(P->sub.x64);
+  b2_dfree(P->sub.xtc); b2_dfree(P->sub.sv_off); b2_dfree(P->sub.bkt_map);
   P->sub = B2SubsetDev();
 }
 
+// frees go to the legacy stream (after all work queued on blocking streams); the plan's own
+// bucket streams are drained first
 static void b2_plan_free(B2PlanDev *P) {
   if (!P) return;
+  for (int b = 0; b < B2_NBKT; ++b) if (P->bkt_stream[b]) cudaStreamSynchronize(P->bkt_stream[b]);
   b2_subset_free(P);
   b2_grid_free(*P);
-  cudaFree(P->mols); cudaFree(P->row_off); cudaFree(P->shells); cudaFree(P->pinfo);
-  cudaFree(P->pp64); cudaFree(P->pp32); cudaFree(P->ao2sh); cudaFree(P->cls_list);
-  cudaFree(P->cls_cnt); cudaFree(P->atom_xyz); cudaFree(P->atom_z); cudaFree(P->boys); cudaFree(P->boys32);
-  cudaFree(P->jk_chunk_off);
-  cudaFree(P->eri_tasks32); cudaFree(P->eri_tasks64);
-  cudaFree(P->sv_off); cudaFree(P->sv_work); cudaFree(P->bkt_map);
+  b2_dfree(P->mols); b2_dfree(P->row_off); b2_dfree(P->shells); b2_dfree(P->pinfo);
+  b2_dfree(P->pp64); b2_dfree(P->pp32); b2_dfree(P->ao2sh); b2_dfree(P->cls_list);
+  b2_dfree(P->cls_cnt); b2_dfree(P->atom_xyz); b2_dfree(P->atom_z); b2_dfree(P->boys); b2_dfree(P->boys32);
+  b2_dfree(P->jk_chunk_off);
+  b2_dfree(P->eri_tasks32); b2_dfree(P->eri_tasks64);
+  b2_dfree(P->sv_off); b2_dfree(P->sv_work); b2_dfree(P->bkt_map);
   for (int b = 0; b < B2_NBKT; ++b) if (P->bkt_stream[b]) cudaStreamDestroy(P->bkt_stream[b]);
   for (int b = 0; b <= B2_NBKT; ++b) if (P->bkt_ev[b]) cudaEventDestroy(P->bkt_ev[b]);
   delete P;
@@ -83,7 +124,7 @@ static int b2_set_jk_chunk(B2PlanDev *P, long long elems, B2Upload *u = nullptr)
   const int nmol = P->h.nmol;
   std::vector<long long> off(nmol + 1, 0);
   for (int m = 0; m < nmol; ++m) off[m + 1] = off[m] + (P->h.mols[m].n4 + elems - 1) / elems;
-  cudaFree(P->jk_chunk_off);
+  b2_dfree(P->jk_chunk_off);
   P->jk_chunk_off = nullptr;
   P->jk_off_h = std::move(off);
   int rc = b2_upload(&P->jk_chunk_off, P->jk_off_h, u);
@@ -117,7 +158,7 @@ static int b2_set_sv(B2PlanDev *P, B2Upload *u) {
   int rc = b2_upload(&P->sv_off, P->sv_off_h, u);
   if (rc) return rc;
   P->sv_ntask = off[nmol];
-  B2_TRY(cudaMalloc(&P->sv_work, sizeof(double) * 4 * (size_t)std::max(1ll, P->h.n_rows)));
+  B2_TRY(b2_dmalloc_t(&P->sv_work, sizeof(double) * 4 * (size_t)std::max(1ll, P->h.n_rows), u ? u->st : nullptr));
   std::vector<int> all(nmol);
   for (int m = 0; m < nmol; ++m) all[m] = m;
   b2_buckets(P, all, P->bkt_map_h, P->bkt_off_h);
@@ -185,6 +226,13 @@ int b2_plan_create(int nmol, const int *natm, const int *nbas, const int *atm, c
   P->h2d_bytes = (long long)u.bytes;
   cudaGetDevice(&P->device);
   *plan = P;
+  return B2_OK;
+}
+
+int b2_release_cached_memory(void) {
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  for (int d = 0; d < 64; ++d)
+    if (g_pool[d] && cudaMemPoolTrimTo(g_pool[d], 0) != cudaSuccess) return b2_note(cudaGetLastError());
   return B2_OK;
 }
 

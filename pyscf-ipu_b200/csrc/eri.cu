@@ -12,6 +12,7 @@
 // CTA whose bra shell pair owns its row ij.
 #include "eri_sq.cuh"
 #include "device_plan.cuh"
+#include "devmem.cuh"
 
 template <typename T, int LI, int LJ, int LK, int LL>
 __global__ void __launch_bounds__(128)
@@ -204,7 +205,7 @@ static int b2_eri_task_upload(B2PlanDev &P, int precision, cudaStream_t st) {
   const long long n_items = 4ll * P.h.n_sp;
   const long long ntile = std::max(1ll, (n_items + B2_TT - 1) / B2_TT);
   long long *scratch = nullptr;                  // tile sums (16 per tile), group totals, group starts
-  B2_CUDA_TRY(cudaMalloc(&scratch, sizeof(long long) * (size_t)(16 * ntile + 32)));
+  B2_CUDA_TRY(b2_dmalloc_t(&scratch, sizeof(long long) * (size_t)(16 * ntile + 32), st));
   long long *gtot = scratch + 16 * ntile, *dgoff = gtot + 16;
   std::vector<long long> tot(16, 0);
   int rc = B2_OK;
@@ -220,7 +221,7 @@ static int b2_eri_task_upload(B2PlanDev &P, int precision, cudaStream_t st) {
   std::vector<long long> g(17, 0);
   for (int k = 0; k < 16; ++k) g[k + 1] = g[k] + tot[k];
   if (!rc && g[16] >= (1ll << 31)) rc = B2_ERR_SIZE;
-  if (!rc && cudaMalloc(&dst, sizeof(B2EriTask) * std::max<size_t>(1, (size_t)g[16])) != cudaSuccess) {
+  if (!rc && b2_dmalloc_t(&dst, sizeof(B2EriTask) * std::max<size_t>(1, (size_t)g[16]), st) != cudaSuccess) {
     dst = nullptr;
     rc = B2_ERR_CUDA;
   }
@@ -234,9 +235,9 @@ static int b2_eri_task_upload(B2PlanDev &P, int precision, cudaStream_t st) {
       if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess) rc = B2_ERR_CUDA;
     }
   }
-  cudaFree(scratch);
+  b2_dfree(scratch, st);
   if (rc) {
-    cudaFree(dst);
+    b2_dfree(dst, st);
     dst = nullptr;
     return rc;
   }
@@ -471,11 +472,11 @@ k_plan_pairs(const B2MolDev *__restrict__ mols, int nmol, const B2Shell *__restr
 
 int b2_build_pairs(B2PlanDev &P, cudaStream_t st) {
   const long long nsp = P.h.n_sp, n = nsp * B2_MAXPP;
-  B2_CUDA_TRY(cudaMalloc(&P.pinfo, sizeof(B2PairInfo) * (size_t)std::max(1ll, nsp)));
-  B2_CUDA_TRY(cudaMalloc(&P.cls_list, sizeof(int) * (size_t)std::max(1ll, nsp)));
-  B2_CUDA_TRY(cudaMalloc(&P.cls_cnt, sizeof(int) * (size_t)std::max(1ll, 4 * nsp)));
-  B2_CUDA_TRY(cudaMalloc(&P.pp64, sizeof(B2PairPrim<double>) * (size_t)std::max(1ll, n)));
-  B2_CUDA_TRY(cudaMalloc(&P.pp32, sizeof(B2PairPrim<float>) * (size_t)std::max(1ll, n)));
+  B2_CUDA_TRY(b2_dmalloc_t(&P.pinfo, sizeof(B2PairInfo) * (size_t)std::max(1ll, nsp), st));
+  B2_CUDA_TRY(b2_dmalloc_t(&P.cls_list, sizeof(int) * (size_t)std::max(1ll, nsp), st));
+  B2_CUDA_TRY(b2_dmalloc_t(&P.cls_cnt, sizeof(int) * (size_t)std::max(1ll, 4 * nsp), st));
+  B2_CUDA_TRY(b2_dmalloc_t(&P.pp64, sizeof(B2PairPrim<double>) * (size_t)std::max(1ll, n), st));
+  B2_CUDA_TRY(b2_dmalloc_t(&P.pp32, sizeof(B2PairPrim<float>) * (size_t)std::max(1ll, n), st));
   if (n > 0) {
     k_plan_pairs<<<(unsigned)((P.h.nmol + 7) / 8), 256, 0, st>>>(P.mols, P.h.nmol, P.shells, P.pinfo,
                                                                  P.cls_list, P.cls_cnt);

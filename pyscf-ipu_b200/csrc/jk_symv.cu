@@ -15,9 +15,10 @@
 //
 // The exchange list is built once per ERI list (k_exch_build: two gathers per entry from the
 // molecule's s8 list, which stays in L2).  The product kernel (k_symv) gives each warp a strip
-// of 128 columns and a block of 64 rows of one molecule: lanes own 4 columns each; every row
-// segment arrives by one bulk copy (8 lanes issue a group's 8 rows) in a 3-stage shared-memory
-// ring (groups of 8 rows, two groups in flight while one is reduced), keep the column sums y[Q] += A[P,Q] x[P] in float64
+// of 128 columns and a block of 128 rows of one molecule: lanes own 4 columns each; every row
+// segment arrives by one bulk copy (8 lanes issue a group's 8 rows) in a 2-stage shared-memory
+// ring (groups of 8 rows: the next group is in flight while one is reduced; 3 CTAs of 8 warps
+// per SM), keep the column sums y[Q] += A[P,Q] x[P] in float64
 // registers for the whole block and reduce the row sums y[P] += sum_Q A[P,Q] x[Q] of 8 rows at
 // a time with one transposed butterfly of warp shuffles; one float64 global atomic per row per
 // strip and per column per block.  Every product and sum is float64 (the lists may be stored in
@@ -26,14 +27,14 @@
 
 #define B2_SV_STRIP 128
 #ifndef B2_SV_ROWS
-#define B2_SV_ROWS 64           // rows per warp task
+#define B2_SV_ROWS 128          // rows per warp task
 #endif
 #define B2_SV_GROUP 8           // rows per copy group (the row-sum butterfly is written for 8)
 #ifndef B2_SV_STAGES
-#define B2_SV_STAGES 3          // copy groups in each warp's shared-memory ring
+#define B2_SV_STAGES 2          // copy groups in each warp's shared-memory ring
 #endif
 #ifndef B2_SV_WARPS
-#define B2_SV_WARPS 4           // warps (tasks) per CTA
+#define B2_SV_WARPS 8           // warps (tasks) per CTA
 #endif
 
 __device__ __forceinline__ long long b2_sv_untri(long long p) {
@@ -102,7 +103,7 @@ __global__ void k_sv_x(const B2MolDev *__restrict__ mols, const int *__restrict_
   }
 }
 
-// warp tasks of one molecule: strips of 128 columns, each cut into blocks of 64 rows (P >= Q)
+// warp tasks of one molecule: strips of 128 columns, each cut into blocks of B2_SV_ROWS rows (P >= Q)
 __host__ __device__ inline long long b2_sv_tasks(long long n2) {
   long long t = 0;
   for (long long q0 = 0; q0 < n2; q0 += B2_SV_STRIP) t += (n2 - q0 + B2_SV_ROWS - 1) / B2_SV_ROWS;

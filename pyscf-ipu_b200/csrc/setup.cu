@@ -6,6 +6,7 @@
 // setup reproduces the host setup to rounding.
 #include <vector>
 #include "device_plan.cuh"
+#include "devmem.cuh"
 #include "setup.cuh"
 
 // ------------------------------------------------------------------ one-electron matrices
@@ -236,10 +237,10 @@ int b2_launch_grid_build(B2PlanDev &P, int nz, const double *tmpl_host, const lo
   apo[P.h.n_atm] = tot;
   if (tot != P.g.n_points) return B2_ERR_ARG;
   const long long ntm = tmpl_off_host[nz];
-  cudaFree(P.g.tmpl); cudaFree(P.g.tmpl_off); cudaFree(P.g.atom_pt_off);
-  B2_CUDA_TRY(cudaMalloc(&P.g.tmpl, sizeof(double) * 4 * std::max(1ll, ntm)));
-  B2_CUDA_TRY(cudaMalloc(&P.g.tmpl_off, sizeof(long long) * (nz + 1)));
-  B2_CUDA_TRY(cudaMalloc(&P.g.atom_pt_off, sizeof(long long) * apo.size()));
+  b2_dfree(P.g.tmpl); b2_dfree(P.g.tmpl_off); b2_dfree(P.g.atom_pt_off);
+  B2_CUDA_TRY(b2_dmalloc_t(&P.g.tmpl, sizeof(double) * 4 * std::max(1ll, ntm)));
+  B2_CUDA_TRY(b2_dmalloc_t(&P.g.tmpl_off, sizeof(long long) * (nz + 1)));
+  B2_CUDA_TRY(b2_dmalloc_t(&P.g.atom_pt_off, sizeof(long long) * apo.size()));
   B2_CUDA_TRY(cudaMemcpy(P.g.tmpl, tmpl_host, sizeof(double) * 4 * ntm, cudaMemcpyHostToDevice));
   B2_CUDA_TRY(cudaMemcpy(P.g.tmpl_off, tmpl_off_host, sizeof(long long) * (nz + 1), cudaMemcpyHostToDevice));
   B2_CUDA_TRY(cudaMemcpy(P.g.atom_pt_off, apo.data(), sizeof(long long) * apo.size(), cudaMemcpyHostToDevice));

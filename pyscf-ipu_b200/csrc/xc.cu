@@ -9,6 +9,7 @@
 //   V_xc = AO0^T (sum_c AO_c * rt_c),  V_xc <- V_xc + V_xc^T
 // AO values are stored per molecule as [4][G][nao] (component-major, grid rows).
 #include "device_plan.cuh"
+#include "devmem.cuh"
 #include "xc_math.cuh"
 #include "xc.cuh"
 
@@ -264,12 +265,12 @@ int b2_grid_setup(B2PlanDev &P, const long long *grid_off_host) {
   P.g.xblk64_h = x64;
   P.g.xblk_tc_h = xtc;
   size_t nb = sizeof(long long) * (nmol + 1);
-  B2_CUDA_TRY(cudaMalloc(&P.g.grid_off, nb));
-  B2_CUDA_TRY(cudaMalloc(&P.g.gblk_off, nb));
-  B2_CUDA_TRY(cudaMalloc(&P.g.xblk32, nb));
-  B2_CUDA_TRY(cudaMalloc(&P.g.xblk64, nb));
-  B2_CUDA_TRY(cudaMalloc(&P.g.xblk_tc, nb));
-  B2_CUDA_TRY(cudaMalloc(&P.g.ao_off, nb));
+  B2_CUDA_TRY(b2_dmalloc_t(&P.g.grid_off, nb));
+  B2_CUDA_TRY(b2_dmalloc_t(&P.g.gblk_off, nb));
+  B2_CUDA_TRY(b2_dmalloc_t(&P.g.xblk32, nb));
+  B2_CUDA_TRY(b2_dmalloc_t(&P.g.xblk64, nb));
+  B2_CUDA_TRY(b2_dmalloc_t(&P.g.xblk_tc, nb));
+  B2_CUDA_TRY(b2_dmalloc_t(&P.g.ao_off, nb));
   B2_CUDA_TRY(cudaMemcpy(P.g.grid_off, goff.data(), nb, cudaMemcpyHostToDevice));
   B2_CUDA_TRY(cudaMemcpy(P.g.gblk_off, gblk.data(), nb, cudaMemcpyHostToDevice));
   B2_CUDA_TRY(cudaMemcpy(P.g.xblk32, x32.data(), nb, cudaMemcpyHostToDevice));
@@ -285,9 +286,9 @@ int b2_xc_set_tpc(B2PlanDev &P, int tpc) {
   b2_xc_split(P.g.grid_off_h, P.h.nmol, 128, P.g.tpc_tc, xtc, tpc);
   long long *d = nullptr;
   const size_t nb = sizeof(long long) * (P.h.nmol + 1);
-  B2_CUDA_TRY(cudaMalloc(&d, nb));
+  B2_CUDA_TRY(b2_dmalloc_t(&d, nb));
   B2_CUDA_TRY(cudaMemcpy(d, xtc.data(), nb, cudaMemcpyHostToDevice));
-  cudaFree(P.g.xblk_tc);
+  b2_dfree(P.g.xblk_tc);
   P.g.xblk_tc = d;
   P.g.xblk_tc_h = xtc;
   P.g.n_xblk_tc = xtc[P.h.nmol];
@@ -295,10 +296,10 @@ int b2_xc_set_tpc(B2PlanDev &P, int tpc) {
 }
 
 void b2_grid_free(B2PlanDev &P) {
-  cudaFree(P.g.grid_off); cudaFree(P.g.gblk_off); cudaFree(P.g.xblk32); cudaFree(P.g.xblk64);
-  cudaFree(P.g.xblk_tc);
-  cudaFree(P.g.ao_off);
-  cudaFree(P.g.tmpl); cudaFree(P.g.tmpl_off); cudaFree(P.g.atom_pt_off);
+  b2_dfree(P.g.grid_off); b2_dfree(P.g.gblk_off); b2_dfree(P.g.xblk32); b2_dfree(P.g.xblk64);
+  b2_dfree(P.g.xblk_tc);
+  b2_dfree(P.g.ao_off);
+  b2_dfree(P.g.tmpl); b2_dfree(P.g.tmpl_off); b2_dfree(P.g.atom_pt_off);
   P.g = B2GridDev();
 }
 
