@@ -166,26 +166,40 @@ __device__ __forceinline__ void b2_sv_issue(const T *__restrict__ A, int P0, int
   if (bytes) b2_sv_bulk(stage + (uint32_t)(lane * b2_sv_rb<T>()), reinterpret_cast<const char *>(A) + a0, bytes, mbar);
 }
 
-// one row group from its stage: column sums into yc, row sums reduced over the warp into y
-template <typename T>
+// one row group from its stage: column sums into yc, row sums reduced over the warp into y.
+// FULL: every row of the group is in the block and lies below the strip (P >= q0 + 128), so all
+// 128 columns are present and off-diagonal: no masks.
+template <typename T, bool FULL>
 __device__ __forceinline__ void b2_sv_use(const unsigned char *__restrict__ stage, const double *__restrict__ x,
                                           int P0, int r1, int q0, const int (&qc)[4], const double (&xq)[4],
                                           double (&yc)[4], double *__restrict__ y, int lane) {
   constexpr int MSK = 16 / (int)sizeof(T) - 1;
   double rs[B2_SV_GROUP];
+  int off = ((P0 * (P0 + 1) >> 1) + q0) & MSK;  // in-row offset of the row's first entry
 #pragma unroll
   for (int rr = 0; rr < B2_SV_GROUP; ++rr) {
     const int P = P0 + rr;
-    const bool ok = P < r1;
-    const T *row = reinterpret_cast<const T *>(stage + rr * b2_sv_rb<T>()) + (((P * (P + 1) >> 1) + q0) & MSK);
-    const double xp = ok ? x[P] : 0.0;
+    const T *row = reinterpret_cast<const T *>(stage + rr * b2_sv_rb<T>()) + off;
+    off = (off + P + 1) & MSK;                   // tri(P + 1) = tri(P) + P + 1
     rs[rr] = 0.0;
+    if (FULL) {
+      const double xp = x[P];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      // entries past the row's end (Q > P) and rows past the block are not copied: masked
-      const double av = (ok && qc[c] <= P) ? (double)row[lane + 32 * c] : 0.0;
-      rs[rr] += av * xq[c];
-      if (qc[c] < P) yc[c] += av * xp;
+      for (int c = 0; c < 4; ++c) {
+        const double av = (double)row[lane + 32 * c];
+        rs[rr] += av * xq[c];
+        yc[c] += av * xp;
+      }
+    } else {
+      const bool ok = P < r1;
+      const double xp = ok ? x[P] : 0.0;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        // entries past the row's end (Q > P) and rows past the block are not copied: masked
+        const double av = (ok && qc[c] <= P) ? (double)row[lane + 32 * c] : 0.0;
+        rs[rr] += av * xq[c];
+        if (qc[c] < P) yc[c] += av * xp;
+      }
     }
   }
   // transposed butterfly: each step hands half of the remaining rows to the partner lane,
@@ -273,7 +287,11 @@ k_symv(const B2MolDev *__restrict__ mols, const long long *__restrict__ task_off
       if (lane == 0) atomicExch(&g_b2_sv_err, 1);
       break;
     }
-    b2_sv_use<T>(ring + sc * SB, x, r0 + g * B2_SV_GROUP, r1, q0, qc, xq, yc, y, lane);
+    const int P0 = r0 + g * B2_SV_GROUP;
+    if (r0 >= q0 + B2_SV_STRIP && P0 + B2_SV_GROUP <= r1)
+      b2_sv_use<T, true>(ring + sc * SB, x, P0, r1, q0, qc, xq, yc, y, lane);
+    else
+      b2_sv_use<T, false>(ring + sc * SB, x, P0, r1, q0, qc, xq, yc, y, lane);
   }
   if (g < ng) {
     // gave up: wait (bounded) for the copies still in flight into this warp's ring, then leave
