@@ -105,27 +105,36 @@ __device__ int b2_jacobi(double *A, double *V, int n, int nreal, double *rot, in
         rot[2 * k] = c; rot[2 * k + 1] = s;
       }
       __syncthreads();
-      for (int e = threadIdx.x; e < half * n; e += blockDim.x) {      // rows: A <- J^T A
-        const int k = e / n, col = e - (e / n) * n;
-        const int p = prs[2 * k], q = prs[2 * k + 1];
-        const double c = rot[2 * k], s = rot[2 * k + 1];
-        if (s == 0.0) continue;
-        const double apk = A[p * ld + col], aqk = A[q * ld + col];
-        A[p * ld + col] = c * apk - s * aqk;
-        A[q * ld + col] = s * apk + c * aqk;
-      }
-      __syncthreads();
-      for (int e = threadIdx.x; e < half * n; e += blockDim.x) {      // cols: A <- A J, V <- V J
-        const int k = e / n, row = e - (e / n) * n;
-        const int p = prs[2 * k], q = prs[2 * k + 1];
-        const double c = rot[2 * k], s = rot[2 * k + 1];
-        if (s == 0.0) continue;
-        const double akp = A[row * ld + p], akq = A[row * ld + q];
-        A[row * ld + p] = c * akp - s * akq;
-        A[row * ld + q] = s * akp + c * akq;
-        const double vkp = V[row * ld + p], vkq = V[row * ld + q];
-        V[row * ld + p] = c * vkp - s * vkq;
-        V[row * ld + q] = s * vkp + c * vkq;
+      // one pass per round: block (k, l) of A (rows of pair k, columns of pair l) <- G_k A_kl G_l^T,
+      // rows first then columns, exactly the arithmetic of a row pass followed by a column pass;
+      // V's columns of pair l <- V G_l^T
+      for (int e = threadIdx.x; e < half * half + n * half; e += blockDim.x) {
+        if (e < half * half) {
+          const int k = e / half, l = e - (e / half) * half;
+          const int p = prs[2 * k], q = prs[2 * k + 1], pl = prs[2 * l], ql = prs[2 * l + 1];
+          const double ck = rot[2 * k], sk = rot[2 * k + 1], cl = rot[2 * l], sl = rot[2 * l + 1];
+          if (sk == 0.0 && sl == 0.0) continue;
+          double a00 = A[p * ld + pl], a01 = A[p * ld + ql], a10 = A[q * ld + pl], a11 = A[q * ld + ql];
+          if (sk != 0.0) {
+            const double b00 = ck * a00 - sk * a10, b10 = sk * a00 + ck * a10;
+            const double b01 = ck * a01 - sk * a11, b11 = sk * a01 + ck * a11;
+            a00 = b00; a10 = b10; a01 = b01; a11 = b11;
+          }
+          if (sl != 0.0) {
+            const double b00 = cl * a00 - sl * a01, b01 = sl * a00 + cl * a01;
+            const double b10 = cl * a10 - sl * a11, b11 = sl * a10 + cl * a11;
+            a00 = b00; a01 = b01; a10 = b10; a11 = b11;
+          }
+          A[p * ld + pl] = a00; A[p * ld + ql] = a01; A[q * ld + pl] = a10; A[q * ld + ql] = a11;
+        } else {
+          const int e2 = e - half * half, l = e2 / n, row = e2 - (e2 / n) * n;
+          const double cl = rot[2 * l], sl = rot[2 * l + 1];
+          if (sl == 0.0) continue;
+          const int pl = prs[2 * l], ql = prs[2 * l + 1];
+          const double vkp = V[row * ld + pl], vkq = V[row * ld + ql];
+          V[row * ld + pl] = cl * vkp - sl * vkq;
+          V[row * ld + ql] = sl * vkp + cl * vkq;
+        }
       }
       __syncthreads();
     }
@@ -303,36 +312,40 @@ k_eigh_density(const B2MolDev *__restrict__ mols, const int *__restrict__ active
   const int ld = n + 1;                            // odd leading dimension: no bank conflicts
   const long long mo = md.mat_off;
   const bool warm = ws && iter && iter[m] > 0;
-  double *sL = sm, *sT = sL + NN, *sA = sT + NN, *sV = sA + n * ld;
-  for (int e = threadIdx.x; e < NN; e += blockDim.x) { sL[e] = Linv[mo + e]; sA[e] = H[mo + e]; }
+  // shared memory holds A and V only; L and W are read from global memory (L1)
+  double *sA = sm, *sV = sA + n * ld;
+  const double *gL = Linv + mo, *gH = H + mo, *gW = ws ? ws + mo : nullptr;
+  for (int e = threadIdx.x; e < NN; e += blockDim.x) {                         // L H -> sV
+    const int r = e / N, c = e - (e / N) * N;
+    double s = 0;
+    for (int k = 0; k < N; ++k) s += gL[r * N + k] * gH[k * N + c];
+    sV[r * ld + c] = s;
+  }
   __syncthreads();
-  b2_mm(sL, sA, sT, N, false);                    // L H
-  __syncthreads();
-  // F' = (L H) L^T into sA (leading dimension ld, padded to n)
+  // F' = (L H) L^T into sA (padded to n: decoupled padding sorts last); consecutive threads take
+  // consecutive rows, so the L row is a broadcast and sV / sA are read and written conflict-free
   for (int e = threadIdx.x; e < n * n; e += blockDim.x) {
-    const int r = e / n, c = e - (e / n) * n;
+    const int c = e / n, r = e - (e / n) * n;
     double s = 0;
     if (r < N && c < N)
-      for (int k = 0; k < N; ++k) s += sT[r * N + k] * sL[c * N + k];
+      for (int k = 0; k < N; ++k) s += sV[r * ld + k] * gL[c * N + k];
     else if (r == c)
-      s = 1e30;                                    // padding: decoupled, sorts last
+      s = 1e30;
     sA[r * ld + c] = s;
   }
   __syncthreads();
   if (warm) {
-    for (int e = threadIdx.x; e < NN; e += blockDim.x) sT[e] = ws[mo + e];     // W
-    __syncthreads();
     for (int e = threadIdx.x; e < NN; e += blockDim.x) {                       // F' W -> sV
       const int r = e / N, c = e - (e / N) * N;
       double s = 0;
-      for (int k = 0; k < N; ++k) s += sA[r * ld + k] * sT[k * N + c];
+      for (int k = 0; k < N; ++k) s += sA[r * ld + k] * gW[k * N + c];
       sV[r * ld + c] = s;
     }
     __syncthreads();
     for (int e = threadIdx.x; e < NN; e += blockDim.x) {                       // W^T (F' W) -> sA
       const int r = e / N, c = e - (e / N) * N;
       double s = 0;
-      for (int k = 0; k < N; ++k) s += sT[k * N + r] * sV[k * ld + c];
+      for (int k = 0; k < N; ++k) s += gW[k * N + r] * sV[k * ld + c];
       sA[r * ld + c] = s;
     }
     __syncthreads();
@@ -340,18 +353,17 @@ k_eigh_density(const B2MolDev *__restrict__ mols, const int *__restrict__ active
   const int sw = b2_jacobi(sA, sV, n, N, rot, prs, red, 30);
   for (int i = threadIdx.x; i < n; i += blockDim.x) evals[i] = sA[i * ld + i];
   __syncthreads();
-  if (warm) {                                                                   // W V' -> sA
-    for (int e = threadIdx.x; e < NN; e += blockDim.x) {
-      const int r = e / N, c = e - (e / N) * N;
-      double s = 0;
-      for (int k = 0; k < N; ++k) s += sT[r * N + k] * sV[k * ld + c];
-      sA[r * ld + c] = s;
+  // eigenvectors E in the orthogonal basis: W V' (warm) or V', into sA
+  for (int e = threadIdx.x; e < NN; e += blockDim.x) {
+    const int r = e / N, c = e - (e / N) * N;
+    double s;
+    if (warm) {
+      s = 0;
+      for (int k = 0; k < N; ++k) s += gW[r * N + k] * sV[k * ld + c];
+    } else {
+      s = sV[r * ld + c];
     }
-  } else {
-    for (int e = threadIdx.x; e < NN; e += blockDim.x) {
-      const int r = e / N, c = e - (e / N) * N;
-      sA[r * ld + c] = sV[r * ld + c];
-    }
+    sA[r * ld + c] = s;
   }
   __syncthreads();
   if (ws)
@@ -368,22 +380,22 @@ k_eigh_density(const B2MolDev *__restrict__ mols, const int *__restrict__ active
   }
   __syncthreads();
   for (int k = threadIdx.x; k < N; k += blockDim.x) mo_energy[(long long)m * B2_MAXNAO + k] = evals[order[k]];
-  // C[:, k] = L^T V[:, order[k]]  (all N columns, into sT)
+  // C[:, k] = L^T E[:, order[k]]  (all N columns, into sV)
   for (int e = threadIdx.x; e < NN; e += blockDim.x) {
     const int r = e / N, k = e - (e / N) * N;
     const int col = order[k];
     double s = 0;
-    for (int a = 0; a < N; ++a) s += sL[a * N + r] * sA[a * ld + col];
-    sT[e] = s;
+    for (int a = 0; a < N; ++a) s += gL[a * N + r] * sA[a * ld + col];
+    sV[r * ld + k] = s;
   }
   __syncthreads();
   const int nocc = md.nocc;
   for (int e = threadIdx.x; e < NN; e += blockDim.x) {
     const int a = e / N, b = e - (e / N) * N;
     double s = 0;
-    for (int k = 0; k < nocc; ++k) s += sT[a * N + k] * sT[b * N + k];
+    for (int k = 0; k < nocc; ++k) s += sV[a * ld + k] * sV[b * ld + k];
     D[mo + e] = 2.0 * s;
-    if (C) C[mo + e] = sT[e];
+    if (C) C[mo + e] = sV[a * ld + b];
   }
   if (threadIdx.x == 0 && sweeps) sweeps[m] = sw;
 }
@@ -459,7 +471,7 @@ __global__ void k_chol_inv(const B2MolDev *__restrict__ mols, const double *__re
 }
 
 static size_t b2_fock_smem(int N) { return sizeof(double) * 4 * N * N; }
-static size_t b2_eigh_smem(int N) { int n = (N + 1) & ~1; return sizeof(double) * (2 * N * N + 2 * n * (n + 1)); }
+static size_t b2_eigh_smem(int N) { int n = (N + 1) & ~1; return sizeof(double) * 2 * n * (n + 1); }
 
 // One launch per orbital bucket (nao <= 16, 32, 48, 64, more) with shared memory sized for that
 // bucket, so small molecules run several CTAs per SM.  The bucket launches go to the plan's
