@@ -330,9 +330,11 @@ def main():
         barrier()
         t0 = time.perf_counter()
         h2d = d2h = 0
+        marks = [t0]
         for _, out in run_batches([mols] * a.steps, **kw):
             h2d += out["h2d_bytes"]
             d2h += sum(v.nbytes for v in out.values() if isinstance(v, np.ndarray))
+            marks.append(time.perf_counter())
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         barrier()
@@ -340,6 +342,7 @@ def main():
         e2e = {"value": shard.aggregate_rate(a.nmol, world, dt / a.steps), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d // a.steps), "d2h_bytes_per_step": int(d2h // a.steps),
                "steps": a.steps, "timing": "wall clock over the steps, max over ranks",
+               "step_ms": [round(1e3 * (b - a_), 1) for a_, b in zip(marks[:-1], marks[1:])],
                "api": "b200dft.engine.run_batches (plan of the next batch prefetched on a worker thread)"}
 
     if rank == 0:

@@ -89,17 +89,27 @@ __device__ int b2_jacobi(double *A, double *V, int n, int nreal, double *rot, in
     if (off <= 1e-26 * tot || off < 1e-300) break;
     for (int r = 0; r < n - 1; ++r) {
       if (threadIdx.x < half) {
+        // round-robin pairs: index 0 fixed, the others rotate by r (k - 1 + r < 2 (n - 1))
         const int k = threadIdx.x;
-        const int a = (k == 0) ? 0 : ((k - 1 + r) % (n - 1)) + 1;
-        const int kb = n - 1 - k;
-        const int b = ((kb - 1 + r) % (n - 1)) + 1;
+        int a = k - 1 + r, b = n - 2 - k + r;
+        if (a >= n - 1) a -= n - 1;
+        if (b >= n - 1) b -= n - 1;
+        a = (k == 0) ? 0 : a + 1;
+        b += 1;
         const int p = min(a, b), q = max(a, b);
         double c, s;
-        const double apq = A[p * ld + q];
-        if (fabs(apq) <= 1e-300 || fabs(apq) < 1e-17 * sqrt(fabs(A[p * ld + p] * A[q * ld + q]))) {
+        const double apq = A[p * ld + q], app = A[p * ld + p], aqq = A[q * ld + q];
+        if (fabs(apq) <= 1e-300 || apq * apq < 1e-34 * fabs(app * aqq)) {
           c = 1.0; s = 0.0;                         // already negligible
         } else {
-          b2_schur2(A[p * ld + p], A[q * ld + q], apq, c, s);
+          // sym.schur2 (Golub & Van Loan) with tau = d / b, d = aqq - app, b = 2 apq:
+          // t = sign(tau) / (|tau| + sqrt(1 + tau^2)) = sign(tau) |b| / (|d| + sqrt(d^2 + b^2))
+          // (one square root, one division; padding never gets here: its couplings are zero)
+          const double d = aqq - app, bb = 2.0 * apq;
+          const double sg = (d == 0.0 || ((d > 0.0) == (bb > 0.0))) ? 1.0 : -1.0;
+          const double t = sg * fabs(bb) / (fabs(d) + sqrt(d * d + bb * bb));
+          c = rsqrt(1.0 + t * t);
+          s = t * c;
         }
         prs[2 * k] = p; prs[2 * k + 1] = q;
         rot[2 * k] = c; rot[2 * k + 1] = s;
@@ -292,7 +302,7 @@ k_fock_diis(const B2MolDev *__restrict__ mols, const int *__restrict__ active,
 // sweeps run on W^T F' W, which is nearly diagonal once the SCF settles (2-3 sweeps instead of
 // 6-8); the eigenvectors are W V'.  The result is the same eigen-decomposition up to the sign
 // and order of eigenvectors, which the density does not depend on.
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(512)
 k_eigh_density(const B2MolDev *__restrict__ mols, const int *__restrict__ active,
                const int *__restrict__ iter, const double *__restrict__ H,
                const double *__restrict__ Linv, double *__restrict__ D, double *__restrict__ mo_energy,
@@ -516,7 +526,7 @@ int b2_launch_eigh_density(const B2PlanDev &P, const int *active, const int *ite
   B2_CUDA_TRY(cudaFuncSetAttribute(k_eigh_density, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)b2_eigh_smem(P.h.max_nao)));
   return b2_per_bucket(P, st, [&](int N, int n, const int *map, cudaStream_t s) {
-    k_eigh_density<<<n, 256, b2_eigh_smem(N), s>>>(P.mols, active, iter, H, Linv, D, mo_energy, C, ws,
+    k_eigh_density<<<n, N > 32 ? 512 : 256, b2_eigh_smem(N), s>>>(P.mols, active, iter, H, Linv, D, mo_energy, C, ws,
                                                    sweeps, map);
   });
 }
