@@ -276,9 +276,9 @@ def main():
     jk_bytes = nlists * P.n_eri * rbytes
     achieved = jk_bytes / (jk_ms / 1000.0) / 1e9
     # DRAM traffic per launch: ncu capture of the same kernel on the 256-molecule batch
-    # (k_symv: 868.3 MB read + 6.7 MB written for 860.8 MB of float32 list entries),
+    # (k_symv: 868.8 MB read + 6.4 MB written for 860.7 MB of float32 list entries),
     # scaled to this launch by the number of entries processed (traffic grows with the lists)
-    traffic = jk_bytes * (875.0 / 860.8) if (a.precision == "mixed" and nlists == 2) else None
+    traffic = jk_bytes * (875.2 / 860.7) if (a.precision == "mixed" and nlists == 2) else None
     roofline = {"kernel": "k_symv" if nlists == 2 else "k_jk_s8", "bound": "hbm", "achieved": achieved,
                 "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
                 "traffic_source": "ncu 256-molecule capture scaled by list size",
