@@ -106,7 +106,7 @@ static void b2_plan_free(B2PlanDev *P) {
   b2_subset_free(P);
   b2_grid_free(*P);
   b2_dfree(P->mols); b2_dfree(P->row_off); b2_dfree(P->shells); b2_dfree(P->pinfo);
-  b2_dfree(P->pp64); b2_dfree(P->pp32); b2_dfree(P->ao2sh); b2_dfree(P->cls_list);
+  b2_dfree(P->pp64); b2_dfree(P->pp32); b2_dfree(P->pp32_n); b2_dfree(P->ao2sh); b2_dfree(P->cls_list);
   b2_dfree(P->cls_cnt); b2_dfree(P->atom_xyz); b2_dfree(P->atom_z); b2_dfree(P->boys); b2_dfree(P->boys32);
   b2_dfree(P->jk_chunk_off);
   b2_dfree(P->eri_tasks32); b2_dfree(P->eri_tasks64);

@@ -38,6 +38,7 @@ struct B2PlanDev {
   B2PairInfo *pinfo = nullptr;
   B2PairPrim<double> *pp64 = nullptr;
   B2PairPrim<float> *pp32 = nullptr;
+  unsigned char *pp32_n = nullptr;        // per shell pair: surviving float32 primitive pairs
   int *ao2sh = nullptr;
   int *cls_list = nullptr;
   int *cls_cnt = nullptr;

@@ -10,6 +10,7 @@
 // all components of one shell quartet (float32 form) or of one bra component (float64 form,
 // p bras split over 3 lanes), looping over the chunk's kets.  Every s8 entry is written exactly once, by the
 // CTA whose bra shell pair owns its row ij.
+#include <type_traits>
 #include "eri_sq.cuh"
 #include "device_plan.cuh"
 #include "devmem.cuh"
@@ -44,6 +45,124 @@ k_eri_sq(const B2EriTask *__restrict__ tasks, long long ntask, const B2MolDev *_
   }
 }
 
+// Flattened form for the float32 classes with at most 3 components per shell quartet: the
+// warp's (ket, ket primitive pair) entries are packed over the lanes (a ket's primitive pairs
+// survive screening in numbers 0..9, so one ket per lane left the warp waiting for its
+// largest ket); each lane sums its entry over the bra's primitive pairs, a same-ket segmented
+// shuffle scan (segments <= 9 lanes, 4 steps) combines the entries of each ket in a fixed
+// order, and the segment's last lane adds the sum to the ket's accumulator in shared memory.
+// component block <-> flat list (unrolled: constant indices, registers only)
+template <typename S>
+__device__ __forceinline__ void b2_fl_flatten(const float (&acc)[S::NI][S::NJ][S::NK][S::NL], float *v) {
+  int t = 0;
+#pragma unroll
+  for (int a = 0; a < S::NI; ++a)
+#pragma unroll
+    for (int b = 0; b < S::NJ; ++b)
+#pragma unroll
+      for (int c = 0; c < S::NK; ++c)
+#pragma unroll
+        for (int d = 0; d < S::NL; ++d) v[t++] = acc[a][b][c][d];
+}
+template <typename S>
+__device__ __forceinline__ void b2_fl_unflatten(const float *v, float (&acc)[S::NI][S::NJ][S::NK][S::NL]) {
+  int t = 0;
+#pragma unroll
+  for (int a = 0; a < S::NI; ++a)
+#pragma unroll
+    for (int b = 0; b < S::NJ; ++b)
+#pragma unroll
+      for (int c = 0; c < S::NK; ++c)
+#pragma unroll
+        for (int d = 0; d < S::NL; ++d) acc[a][b][c][d] = v[t++];
+}
+
+template <int LI, int LJ, int LK, int LL>
+__global__ void __launch_bounds__(128)
+k_eri_fl(const B2EriTask *__restrict__ tasks, long long ntask, const B2MolDev *__restrict__ mols,
+         const B2PairInfo *__restrict__ pinfo, const B2PairPrim<float> *__restrict__ pp,
+         const unsigned char *__restrict__ ppn, const int *__restrict__ cls_list, const float *__restrict__ btab,
+         float *__restrict__ out) {
+  using S = B2Sq<float, LI, LJ, LK, LL, -1>;
+  constexpr int NC = S::NI * S::NJ * S::NK * S::NL;
+  static_assert(NC <= 3, "flattened ERI form: at most 3 components");
+  __shared__ B2PairPrim<float> sbra[4][B2_MAXPP];
+  __shared__ int s_nb[4];
+  __shared__ int s_off[4][32], s_kl[4][32];
+  __shared__ unsigned char s_map[4][32 * B2_MAXPP];
+  __shared__ float s_acc[4][32][NC];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long long ti = (long long)blockIdx.x * 4 + w;
+  if (ti >= ntask) return;                        // whole warp
+  const B2EriTask tk = tasks[ti];
+  const B2MolDev md = mols[tk.mol];
+  const B2PairInfo bp = pinfo[md.sp_off + tk.IJ];
+  if (lane == 0) {
+    const B2PairPrim<float> *src = pp + (size_t)(md.sp_off + tk.IJ) * B2_MAXPP;
+    int nb = 0;
+    for (int x = 0; x < B2_MAXPP; ++x)
+      if (src[x].K != 0.f) sbra[w][nb++] = src[x];
+    s_nb[w] = nb;
+  }
+  // this lane's ket (tasks of batch plans hold at most 32 kets) and its surviving primitive pairs
+  int KL = 0, nq = 0;
+  if (lane < tk.count) {
+    KL = cls_list[md.sp_off + md.cls_start[tk.cls] + tk.start + lane];
+    nq = ppn[md.sp_off + KL];
+  }
+  int inc = nq;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  const int E = __shfl_sync(0xffffffffu, inc, 31), exc = inc - nq;
+  s_off[w][lane] = exc;
+  s_kl[w][lane] = KL;
+  for (int j = 0; j < nq; ++j) s_map[w][exc + j] = (unsigned char)lane;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) s_acc[w][lane][c] = 0.f;
+  __syncwarp();
+  const int nb = s_nb[w];
+  const B2PairPrim<float> *ppm = pp + (size_t)md.sp_off * B2_MAXPP;
+  for (int e0 = 0; e0 < E; e0 += 32) {
+    const int e = e0 + lane;
+    const bool valid = e < E;
+    const int k = valid ? (int)s_map[w][e] : -1 - lane;   // entries past the end: unique keys
+    float acc[S::NI][S::NJ][S::NK][S::NL];
+    S::zero(acc);
+    if (valid) {
+      const B2PairPrim<float> Q = ppm[(size_t)s_kl[w][k] * B2_MAXPP + (e - s_off[w][k])];
+      for (int p = 0; p < nb; ++p) S::quartet(sbra[w][p], Q, btab, acc);
+    }
+    float a[NC];
+    b2_fl_flatten<S>(acc, a);
+#pragma unroll
+    for (int o = 1; o < 16; o <<= 1) {                     // same-ket inclusive scan
+      const int ko = __shfl_up_sync(0xffffffffu, k, o);
+      const bool take = lane >= o && ko == k;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const float y = __shfl_up_sync(0xffffffffu, a[c], o);
+        if (take) a[c] += y;
+      }
+    }
+    const int kn = __shfl_down_sync(0xffffffffu, k, 1);
+    if (valid && (lane == 31 || kn != k))
+#pragma unroll
+      for (int c = 0; c < NC; ++c) s_acc[w][k][c] += a[c];
+    __syncwarp();
+  }
+  if (lane < tk.count) {
+    const B2PairInfo kp = pinfo[md.sp_off + KL];
+    float acc[S::NI][S::NJ][S::NK][S::NL], a[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) a[c] = s_acc[w][lane][c];
+    b2_fl_unflatten<S>(a, acc);
+    S::template store<float>(out + md.eri_off, bp, kp, acc);
+  }
+}
+
 template <typename T> static const T *b2_boys_table(const B2PlanDev &P);
 template <> const double *b2_boys_table<double>(const B2PlanDev &P) { return P.boys; }
 template <> const float *b2_boys_table<float>(const B2PlanDev &P) { return P.boys32; }
@@ -60,12 +179,30 @@ static void b2_eri_group(const B2PlanDev &P, const B2EriTask *tasks, long long n
   }
 }
 
+// batch plans: the float32 classes with at most 3 components take the flattened kernel
+template <typename T, int LI, int LJ, int LK, int LL>
+static void b2_eri_group_batch(const B2PlanDev &P, const B2EriTask *tasks, long long n,
+                               const B2PairPrim<T> *pp, T *out, cudaStream_t st) {
+  constexpr int NC = (LI ? 3 : 1) * (LJ ? 3 : 1) * (LK ? 3 : 1) * (LL ? 3 : 1);
+  if constexpr (std::is_same<T, float>::value && NC <= 3) {
+    const long long maxg = 4 * ((1ll << 31) - 1);
+    for (long long t0 = 0; t0 < n; t0 += maxg) {
+      const long long nt = std::min(maxg, n - t0);
+      k_eri_fl<LI, LJ, LK, LL><<<(unsigned)((nt + 3) / 4), 128, 0, st>>>(
+          tasks + t0, nt, P.mols, P.pinfo, pp, P.pp32_n, P.cls_list, P.boys32, out);
+      b2_count_launches(1);
+    }
+  } else {
+    b2_eri_group<T, LI, LJ, LK, LL>(P, tasks, n, pp, out, st);
+  }
+}
+
 template <typename T>
 static void b2_eri_all(const B2PlanDev &P, const B2EriTask *tasks, const std::vector<long long> &g,
                        const B2PairPrim<T> *pp, T *out, cudaStream_t st) {
 #define B2_G(grp, LI, LJ, LK, LL)                                                            \
   if (g[grp + 1] > g[grp])                                                                   \
-    b2_eri_group<T, LI, LJ, LK, LL>(P, tasks + g[grp], g[grp + 1] - g[grp], pp, out, st);
+    b2_eri_group_batch<T, LI, LJ, LK, LL>(P, tasks + g[grp], g[grp + 1] - g[grp], pp, out, st);
   B2_G(0, 0, 0, 0, 0) B2_G(1, 0, 0, 1, 0) B2_G(2, 0, 0, 0, 1) B2_G(3, 0, 0, 1, 1)
   B2_G(4, 1, 0, 0, 0) B2_G(5, 1, 0, 1, 0) B2_G(6, 1, 0, 0, 1) B2_G(7, 1, 0, 1, 1)
   B2_G(8, 0, 1, 0, 0) B2_G(9, 0, 1, 1, 0) B2_G(10, 0, 1, 0, 1) B2_G(11, 0, 1, 1, 1)
@@ -424,7 +561,8 @@ extern "C" int b2_int2e_sph_s8_noalloc(const int *atm, int natm, const int *bas,
 // and packed), one thread per shell pair; same code as the host test build
 __global__ void k_pair_prims(const B2MolDev *__restrict__ mols, int nmol, const B2Shell *__restrict__ shells,
                              const B2PairInfo *__restrict__ pinfo, long long n_sp,
-                             B2PairPrim<double> *__restrict__ pp64, B2PairPrim<float> *__restrict__ pp32) {
+                             B2PairPrim<double> *__restrict__ pp64, B2PairPrim<float> *__restrict__ pp32,
+                             unsigned char *__restrict__ pp32_n) {
   const long long gp = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (gp >= n_sp) return;
   int lo = 0, hi = nmol - 1;
@@ -434,7 +572,9 @@ __global__ void k_pair_prims(const B2MolDev *__restrict__ mols, int nmol, const 
   }
   const B2PairInfo pi = pinfo[gp];
   const int sh = mols[lo].sh_off;
-  b2_pair_prims_packed(shells[sh + pi.I], shells[sh + pi.J], pp64 + gp * B2_MAXPP, pp32 + gp * B2_MAXPP);
+  int n32 = 0;
+  b2_pair_prims_packed(shells[sh + pi.I], shells[sh + pi.J], pp64 + gp * B2_MAXPP, pp32 + gp * B2_MAXPP, &n32);
+  pp32_n[gp] = (unsigned char)n32;
 }
 
 // shell-pair tables of every molecule, one warp per molecule: pair info, the class lists
@@ -477,11 +617,12 @@ int b2_build_pairs(B2PlanDev &P, cudaStream_t st) {
   B2_CUDA_TRY(b2_dmalloc_t(&P.cls_cnt, sizeof(int) * (size_t)std::max(1ll, 4 * nsp), st));
   B2_CUDA_TRY(b2_dmalloc_t(&P.pp64, sizeof(B2PairPrim<double>) * (size_t)std::max(1ll, n), st));
   B2_CUDA_TRY(b2_dmalloc_t(&P.pp32, sizeof(B2PairPrim<float>) * (size_t)std::max(1ll, n), st));
+  B2_CUDA_TRY(b2_dmalloc_t(&P.pp32_n, (size_t)std::max(1ll, nsp), st));
   if (n > 0) {
     k_plan_pairs<<<(unsigned)((P.h.nmol + 7) / 8), 256, 0, st>>>(P.mols, P.h.nmol, P.shells, P.pinfo,
                                                                  P.cls_list, P.cls_cnt);
     k_pair_prims<<<(unsigned)((nsp + 127) / 128), 128, 0, st>>>(P.mols, P.h.nmol, P.shells, P.pinfo,
-                                                               nsp, P.pp64, P.pp32);
+                                                               nsp, P.pp64, P.pp32, P.pp32_n);
     b2_count_launches(2);
     B2_CUDA_TRY(cudaGetLastError());
   }

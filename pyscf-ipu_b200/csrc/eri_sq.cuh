@@ -15,9 +15,7 @@ struct B2Sq {
   static constexpr int NJ = LJ ? 3 : 1, NK = LK ? 3 : 1, NL = LL ? 3 : 1;
   static constexpr int L = LI + LJ + LK + LL;
 
-  B2_HD static void eval(const B2PairPrim<T> *__restrict__ bra, int nb,
-                         const B2PairPrim<T> *__restrict__ ket, const T *__restrict__ btab,
-                         T acc[NI][NJ][NK][NL]) {
+  B2_HD static void zero(T acc[NI][NJ][NK][NL]) {
 #pragma unroll
     for (int a = 0; a < NI; ++a)
 #pragma unroll
@@ -26,92 +24,102 @@ struct B2Sq {
         for (int c = 0; c < NK; ++c)
 #pragma unroll
           for (int d = 0; d < NL; ++d) acc[a][b][c][d] = (T)0;
+  }
+
+  // one primitive quartet (bra primitive pair Bp, ket primitive pair Q) added to acc
+  B2_HD static void quartet(const B2PairPrim<T> &Bp, const B2PairPrim<T> &Q, const T *__restrict__ btab,
+                            T acc[NI][NJ][NK][NL]) {
+    const T eta = Q.zeta;
+    const T v = Q.h2z;
+    const T QC[3] = {Q.PAx, Q.PAy, Q.PAz};
+    const T QD[3] = {Q.PBx, Q.PBy, Q.PBz};
+
+    const T zeta = Bp.zeta;
+    const T u = Bp.h2z;
+    const T sig = zeta + eta;
+    const T rho = b2_div<T>(zeta * eta, sig);
+    const T X[3] = {Bp.Px - Q.Px, Bp.Py - Q.Py, Bp.Pz - Q.Pz};
+    const T tt = rho * (X[0] * X[0] + X[1] * X[1] + X[2] * X[2]);
+    const T pref = Bp.K * Q.K * b2_rsqrt<T>(sig);
+    T F[L + 1];
+    b2_boys<T, L, T>(tt, btab, F);
+    T f[L + 3];
+    {
+      T m2r = (T)-2 * rho, s = pref;
+#pragma unroll
+      for (int n = 0; n <= L; ++n) { f[n] = s * F[n]; s *= m2r; }
+      f[L + 1] = (T)0;
+      f[L + 2] = (T)0;
+    }
+    const T PA[3] = {Bp.PAx, Bp.PAy, Bp.PAz};
+    const T PB[3] = {Bp.PBx, Bp.PBy, Bp.PBz};
+#pragma unroll
+    for (int ia = 0; ia < NI; ++ia) {
+      const int a = CI < 0 ? ia : CI;
+      const T sa = LI ? PA[a] : (T)1;
+      const T xa = LI ? X[a] : (T)0;
+#pragma unroll
+      for (int b = 0; b < NJ; ++b) {
+        const T sb = LJ ? PB[b] : (T)1;
+        const T xb = LJ ? X[b] : (T)0;
+        const T abf = (LI && LJ && a == b) ? (T)1 : (T)0;
+        const T E0 = sa * sb + abf * u;
+        const T Ea = LI ? sb * u : (T)0;
+        const T Eb = LJ ? sa * u : (T)0;
+        const T Eab = (LI && LJ) ? u * u : (T)0;
+        const T lin = Ea * xa + Eb * xb + Eab * abf;
+        const T quad = Eab * xa * xb;
+        const T g0 = E0 * f[0] + lin * f[1] + quad * f[2];
+        if (LK == 0 && LL == 0) {
+          acc[ia][b][0][0] += g0;
+          continue;
+        }
+        const T g1 = E0 * f[1] + lin * f[2] + quad * f[3];
+        const T A1 = Ea * f[1] + Eab * xb * f[2];
+        const T B1 = Eb * f[1] + Eab * xa * f[2];
+        T Bc[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          Bc[c] = X[c] * g1 + ((LI && c == a) ? A1 : (T)0) + ((LJ && c == b) ? B1 : (T)0);
+        if (LK && !LL) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) acc[ia][b][c][0] += QC[c] * g0 - v * Bc[c];
+        } else if (!LK && LL) {
+#pragma unroll
+          for (int d = 0; d < 3; ++d) acc[ia][b][0][d] += QD[d] * g0 - v * Bc[d];
+        } else {
+          const T g2 = E0 * f[2] + lin * f[3] + quad * f[4];
+          const T A2 = Ea * f[2] + Eab * xb * f[3];
+          const T B2 = Eb * f[2] + Eab * xa * f[3];
+          const T W = Eab * f[2];
+          T V2[3];
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+            V2[c] = ((LI && c == a) ? A2 : (T)0) + ((LJ && c == b) ? B2 : (T)0);
+          const T vv = v * v;
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+              const int wcd = (LI && LJ) ? ((c == a && d == b) ? 1 : 0) + ((d == a && c == b) ? 1 : 0) : 0;
+              const T Bcd = (c == d ? g1 : (T)0) + X[c] * X[d] * g2 + X[d] * V2[c] + X[c] * V2[d] +
+                            (wcd ? W * (T)wcd : (T)0);
+              const T F0 = QC[c] * QD[d] + (c == d ? v : (T)0);
+              acc[ia][b][c][d] += F0 * g0 - v * (QD[d] * Bc[c] + QC[c] * Bc[d]) + vv * Bcd;
+            }
+        }
+      }
+    }
+  }
+
+  B2_HD static void eval(const B2PairPrim<T> *__restrict__ bra, int nb,
+                         const B2PairPrim<T> *__restrict__ ket, const T *__restrict__ btab,
+                         T acc[NI][NJ][NK][NL]) {
+    zero(acc);
     for (int q = 0; q < B2_MAXPP; ++q) {
       const B2PairPrim<T> Q = ket[q];
       if (Q.K == (T)0) break;                 // packed: the rest of the pair is inert
-      const T eta = Q.zeta;
-      const T v = Q.h2z;
-      const T QC[3] = {Q.PAx, Q.PAy, Q.PAz};
-      const T QD[3] = {Q.PBx, Q.PBy, Q.PBz};
-      for (int p = 0; p < nb; ++p) {
-        const B2PairPrim<T> &Bp = bra[p];
-        const T zeta = Bp.zeta;
-        const T u = Bp.h2z;
-        const T sig = zeta + eta;
-        const T rho = b2_div<T>(zeta * eta, sig);
-        const T X[3] = {Bp.Px - Q.Px, Bp.Py - Q.Py, Bp.Pz - Q.Pz};
-        const T tt = rho * (X[0] * X[0] + X[1] * X[1] + X[2] * X[2]);
-        const T pref = Bp.K * Q.K * b2_rsqrt<T>(sig);
-        T F[L + 1];
-        b2_boys<T, L, T>(tt, btab, F);
-        T f[L + 3];
-        {
-          T m2r = (T)-2 * rho, s = pref;
-#pragma unroll
-          for (int n = 0; n <= L; ++n) { f[n] = s * F[n]; s *= m2r; }
-          f[L + 1] = (T)0;
-          f[L + 2] = (T)0;
-        }
-        const T PA[3] = {Bp.PAx, Bp.PAy, Bp.PAz};
-        const T PB[3] = {Bp.PBx, Bp.PBy, Bp.PBz};
-#pragma unroll
-        for (int ia = 0; ia < NI; ++ia) {
-          const int a = CI < 0 ? ia : CI;
-          const T sa = LI ? PA[a] : (T)1;
-          const T xa = LI ? X[a] : (T)0;
-#pragma unroll
-          for (int b = 0; b < NJ; ++b) {
-            const T sb = LJ ? PB[b] : (T)1;
-            const T xb = LJ ? X[b] : (T)0;
-            const T abf = (LI && LJ && a == b) ? (T)1 : (T)0;
-            const T E0 = sa * sb + abf * u;
-            const T Ea = LI ? sb * u : (T)0;
-            const T Eb = LJ ? sa * u : (T)0;
-            const T Eab = (LI && LJ) ? u * u : (T)0;
-            const T lin = Ea * xa + Eb * xb + Eab * abf;
-            const T quad = Eab * xa * xb;
-            const T g0 = E0 * f[0] + lin * f[1] + quad * f[2];
-            if (LK == 0 && LL == 0) {
-              acc[ia][b][0][0] += g0;
-              continue;
-            }
-            const T g1 = E0 * f[1] + lin * f[2] + quad * f[3];
-            const T A1 = Ea * f[1] + Eab * xb * f[2];
-            const T B1 = Eb * f[1] + Eab * xa * f[2];
-            T Bc[3];
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-              Bc[c] = X[c] * g1 + ((LI && c == a) ? A1 : (T)0) + ((LJ && c == b) ? B1 : (T)0);
-            if (LK && !LL) {
-#pragma unroll
-              for (int c = 0; c < 3; ++c) acc[ia][b][c][0] += QC[c] * g0 - v * Bc[c];
-            } else if (!LK && LL) {
-#pragma unroll
-              for (int d = 0; d < 3; ++d) acc[ia][b][0][d] += QD[d] * g0 - v * Bc[d];
-            } else {
-              const T g2 = E0 * f[2] + lin * f[3] + quad * f[4];
-              const T A2 = Ea * f[2] + Eab * xb * f[3];
-              const T B2 = Eb * f[2] + Eab * xa * f[3];
-              const T W = Eab * f[2];
-              T V2[3];
-#pragma unroll
-              for (int c = 0; c < 3; ++c)
-                V2[c] = ((LI && c == a) ? A2 : (T)0) + ((LJ && c == b) ? B2 : (T)0);
-              const T vv = v * v;
-#pragma unroll
-              for (int c = 0; c < 3; ++c)
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                  const int wcd = (LI && LJ) ? ((c == a && d == b) ? 1 : 0) + ((d == a && c == b) ? 1 : 0) : 0;
-                  const T Bcd = (c == d ? g1 : (T)0) + X[c] * X[d] * g2 + X[d] * V2[c] + X[c] * V2[d] +
-                                (wcd ? W * (T)wcd : (T)0);
-                  const T F0 = QC[c] * QD[d] + (c == d ? v : (T)0);
-                  acc[ia][b][c][d] += F0 * g0 - v * (QD[d] * Bc[c] + QC[c] * Bc[d]) + vv * Bcd;
-                }
-            }
-          }
-        }
-      }
+      for (int p = 0; p < nb; ++p) quartet(bra[p], Q, btab, acc);
     }
   }
 

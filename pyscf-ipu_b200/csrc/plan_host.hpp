@@ -84,7 +84,7 @@ B2_HD void b2_pair_prim32(const B2PairPrim<double> &q, B2PairPrim<float> &f) {
 #define B2_PP_SCREEN64 1e-15
 #define B2_PP_SCREEN32 1e-11
 B2_HD void b2_pair_prims_packed(const B2Shell &a, const B2Shell &b, B2PairPrim<double> *q64,
-                                B2PairPrim<float> *q32) {
+                                B2PairPrim<float> *q32, int *n32_out = nullptr) {
   B2PairPrim<double> all[B2_MAXPP];
   for (int x = 0; x < B2_MAXPP; ++x) b2_pair_prim(a, b, x, all[x]);
   int n64 = 0, n32 = 0;
@@ -97,6 +97,7 @@ B2_HD void b2_pair_prims_packed(const B2Shell &a, const B2Shell &b, B2PairPrim<d
   b2_pair_prim(a, b, B2_MAXPP * B2_MAXPP, inert);          // out-of-range index: inert entry
   for (int x = n64; x < B2_MAXPP; ++x) q64[x] = inert;
   for (int x = n32; x < B2_MAXPP; ++x) b2_pair_prim32(inert, q32[x]);
+  if (n32_out) *n32_out = n32;                              // surviving float32 primitive pairs
 }
 
 // returns B2_OK or an error code
