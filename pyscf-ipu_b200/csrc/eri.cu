@@ -45,7 +45,7 @@ k_eri_sq(const B2EriTask *__restrict__ tasks, long long ntask, const B2MolDev *_
   }
 }
 
-// Flattened form for the float32 classes with at most 9 components per shell quartet: the
+// Flattened form for the float32 classes with at most 27 components per shell quartet: the
 // warp's (ket, ket primitive pair) entries are packed over the lanes (a ket's primitive pairs
 // survive screening in numbers 0..9, so one ket per lane left the warp waiting for its
 // largest ket); each lane sums its entry over the bra's primitive pairs, a same-ket segmented
@@ -85,7 +85,7 @@ k_eri_fl(const B2EriTask *__restrict__ tasks, long long ntask, const B2MolDev *_
          float *__restrict__ out) {
   using S = B2Sq<float, LI, LJ, LK, LL, -1>;
   constexpr int NC = S::NI * S::NJ * S::NK * S::NL;
-  static_assert(NC <= 9, "flattened ERI form: at most 9 components");
+  static_assert(NC <= 27, "flattened ERI form: at most 27 components");
   __shared__ B2PairPrim<float> sbra[4][B2_MAXPP];
   __shared__ int s_nb[4];
   __shared__ int s_off[4][32], s_kl[4][32];
@@ -179,12 +179,12 @@ static void b2_eri_group(const B2PlanDev &P, const B2EriTask *tasks, long long n
   }
 }
 
-// batch plans: the float32 classes with at most 9 components take the flattened kernel
+// batch plans: the float32 classes with at most 27 components take the flattened kernel
 template <typename T, int LI, int LJ, int LK, int LL>
 static void b2_eri_group_batch(const B2PlanDev &P, const B2EriTask *tasks, long long n,
                                const B2PairPrim<T> *pp, T *out, cudaStream_t st) {
   constexpr int NC = (LI ? 3 : 1) * (LJ ? 3 : 1) * (LK ? 3 : 1) * (LL ? 3 : 1);
-  if constexpr (std::is_same<T, float>::value && NC <= 9) {
+  if constexpr (std::is_same<T, float>::value && NC <= 27) {
     const long long maxg = 4 * ((1ll << 31) - 1);
     for (long long t0 = 0; t0 < n; t0 += maxg) {
       const long long nt = std::min(maxg, n - t0);
