@@ -46,6 +46,16 @@ template <typename T> B2_HD T b2_exp_neg(T t) { return exp(-t); }
 template <> __device__ __forceinline__ float b2_exp_neg<float>(float t) { return __expf(-t); }
 #endif
 
+// 1 / t and 1 / sqrt(t): exact for float64; for float32 one hardware reciprocal square root
+// (relative error ~1e-7) and its square
+template <typename T> B2_HD void b2_inv_rsqrt(T t, T &inv, T &rt) { inv = (T)1 / t; rt = sqrt(inv); }
+#ifdef __CUDA_ARCH__
+template <> __device__ __forceinline__ void b2_inv_rsqrt<float>(float t, float &inv, float &rt) {
+  rt = rsqrtf(t);
+  inv = rt * rt;
+}
+#endif
+
 // F[0..L] at T; `table` is the table in double (float64 kernels) or float (float32 kernels).
 template <typename T, int L, typename TT>
 B2_HD void b2_boys(T t, const TT *__restrict__ table, T *F) {
@@ -66,8 +76,9 @@ B2_HD void b2_boys(T t, const TT *__restrict__ table, T *F) {
       for (int m = L - 1; m >= 0; --m) F[m] = (t2 * F[m + 1] + et) * (T)(1.0 / (2 * m + 1));
     }
   } else {
-    T inv = (T)1 / t;
-    F[0] = (T)0.886226925452758014 * sqrt(inv);      // sqrt(pi)/2 / sqrt(T)
+    T inv, rt;                                        // 1 / T, 1 / sqrt(T)
+    b2_inv_rsqrt<T>(t, inv, rt);
+    F[0] = (T)0.886226925452758014 * rt;              // sqrt(pi)/2 / sqrt(T)
 #pragma unroll
     for (int m = 0; m < L; ++m) F[m + 1] = (T)(2 * m + 1) * (T)0.5 * inv * F[m];
   }
@@ -79,4 +90,13 @@ template <typename T> B2_HD T b2_rsqrt(T x) { return (T)1 / sqrt(x); }
 #ifdef __CUDA_ARCH__
 template <> __device__ __forceinline__ float b2_div<float>(float a, float b) { return __fdividef(a, b); }
 template <> __device__ __forceinline__ float b2_rsqrt<float>(float x) { return rsqrtf(x); }
+#endif
+// a / s and 1 / sqrt(s): exact for float64; for float32 one hardware reciprocal square root r
+// and a / s = a r^2 (no separate division)
+template <typename T> B2_HD void b2_rho_rs(T a, T s, T &q, T &rs) { q = b2_div<T>(a, s); rs = b2_rsqrt<T>(s); }
+#ifdef __CUDA_ARCH__
+template <> __device__ __forceinline__ void b2_rho_rs<float>(float a, float s, float &q, float &rs) {
+  rs = rsqrtf(s);
+  q = a * (rs * rs);
+}
 #endif

@@ -44,9 +44,10 @@ struct B2Shell {               // one contracted shell of one molecule
   int l, ao0, nprim, atom;
 };
 
-// primitive-pair data of a shell pair (bra or ket), precision T
+// primitive-pair data of a shell pair (bra or ket), precision T; 16-byte aligned (48 / 96
+// bytes) so that kernels load it with 128-bit vector loads
 template <typename T>
-struct B2PairPrim {
+struct __align__(16) B2PairPrim {
   T zeta, Px, Py, Pz, K, PAx, PAy, PAz, PBx, PBy, PBz, h2z;   // h2z = 1 / (2 zeta)
 };
 

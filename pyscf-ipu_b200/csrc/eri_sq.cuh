@@ -37,10 +37,11 @@ struct B2Sq {
     const T zeta = Bp.zeta;
     const T u = Bp.h2z;
     const T sig = zeta + eta;
-    const T rho = b2_div<T>(zeta * eta, sig);
+    T rho, rs;                                // rho = zeta eta / sig, rs = 1 / sqrt(sig)
+    b2_rho_rs<T>(zeta * eta, sig, rho, rs);
     const T X[3] = {Bp.Px - Q.Px, Bp.Py - Q.Py, Bp.Pz - Q.Pz};
     const T tt = rho * (X[0] * X[0] + X[1] * X[1] + X[2] * X[2]);
-    const T pref = Bp.K * Q.K * b2_rsqrt<T>(sig);
+    const T pref = Bp.K * Q.K * rs;
     T F[L + 1];
     b2_boys<T, L, T>(tt, btab, F);
     T f[L + 3];
