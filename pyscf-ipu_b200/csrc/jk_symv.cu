@@ -70,8 +70,12 @@ k_exch_build(const B2MolDev *__restrict__ mols, const long long *__restrict__ ch
     int i = (int)b2_sv_untri(P), l = (int)(P - b2_tri(i));
     int j = (int)b2_sv_untri(Q), k = (int)(Q - b2_tri(j));
     const int n = (int)min(8ll, p1 - e0);
-    for (int r = 0; r < n; ++r) {
-      X[e0 + r] = E[b2_sv_idx(i, j, k, l)] + E[b2_sv_idx(i, k, j, l)];
+    // all 16 gather addresses first, then the loads (8 entries' gathers in flight together)
+    long long ia[8], ib[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      ia[r] = b2_sv_idx(i, j, k, l);
+      ib[r] = b2_sv_idx(i, k, j, l);
       if (Q == P) {                 // next row (il): Q = 0, (j,k) = (0,0)
         ++P; Q = 0; j = 0; k = 0;
         if (++l > i) { ++i; l = 0; }
@@ -80,6 +84,15 @@ k_exch_build(const B2MolDev *__restrict__ mols, const long long *__restrict__ ch
         if (++k > j) { ++j; k = 0; }
       }
     }
+    T va[8], vb[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      va[r] = r < n ? E[ia[r]] : (T)0;
+      vb[r] = r < n ? E[ib[r]] : (T)0;
+    }
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+      if (r < n) X[e0 + r] = va[r] + vb[r];
   }
 }
 
