@@ -70,6 +70,29 @@ int b2hc_eri_s8(int nmol, const int *natm, const int *nbas, const int *atm, cons
 }
 
 // B3LYP at n points (double): rho (4, n) as in the reference (rho[1:4] = half gradient)
+// class starts of every molecule as the device plan computes them (from the shells' l, no pair
+// tables) and as the host pair tables give them: out_fast / out_ref hold 5 ints per molecule,
+// plus the pair tables' per-class inclusive counts at the last pair (must equal the class sizes)
+int b2hc_plan_classes(int nmol, const int *natm, const int *nbas, const int *atm, const int *bas,
+                      const double *env, const long long *env_off, int *out_fast, int *out_ref) {
+  B2PlanHost F, R;
+  int rc = b2_plan_build(F, nmol, natm, nbas, atm, bas, env, env_off, /*pair_tables=*/false);
+  if (rc) return rc;
+  if ((rc = b2_plan_build(R, nmol, natm, nbas, atm, bas, env, env_off, /*pair_tables=*/true))) return rc;
+  for (int m = 0; m < nmol; ++m) {
+    const B2MolDev &md = R.mols[m];
+    for (int c = 0; c < 5; ++c) {
+      out_fast[5 * m + c] = F.mols[m].cls_start[c];
+      out_ref[5 * m + c] = md.cls_start[c];
+    }
+    for (int c = 0; c < 4; ++c) {                 // class sizes from the prefix counts
+      const int last = md.nsp ? R.cls_cnt[4ll * md.sp_off + (long long)c * md.nsp + md.nsp - 1] : 0;
+      if (last != md.cls_start[c + 1] - md.cls_start[c]) return -100 - c;
+    }
+  }
+  return 0;
+}
+
 int b2hc_b3lyp(int n, const double *rho, double *exc, double *vrho, double *vgamma) {
   for (int g = 0; g < n; ++g) {
     double r[4] = {rho[g], rho[n + g], rho[2 * n + g], rho[3 * n + g]};

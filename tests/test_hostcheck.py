@@ -82,3 +82,26 @@ def test_b3lyp_device_math():
     np.testing.assert_allclose(e, e0, rtol=1e-12)
     np.testing.assert_allclose(vr, vr0, rtol=1e-12)
     np.testing.assert_allclose(vg, vg0, rtol=1e-10)
+
+
+def test_plan_class_starts_without_pair_tables():
+    """the device plan counts each molecule's shell pairs per angular class from the shells' l
+    alone (its pair tables are built on the GPU); the counts must equal the host pair tables'"""
+    from b200dft.molgen import config3_batch
+    hc = _hc()
+    mols = [Mole(s) for s in config3_batch(48, seed=5)] + [Mole(methane()), Mole("H 0 0 0; H 0 0 0.74")]
+    atm = np.ascontiguousarray(np.concatenate([m._atm for m in mols]), np.int32)
+    bas = np.ascontiguousarray(np.concatenate([m._bas for m in mols]), np.int32)
+    env = np.concatenate([m._env for m in mols])
+    eo = np.cumsum([0] + [len(m._env) for m in mols[:-1]]).astype(np.int64)
+    natm = np.array([m.natm for m in mols], np.int32)
+    nbas = np.array([m.nbas for m in mols], np.int32)
+    fast = np.zeros(5 * len(mols), np.int32)
+    ref = np.full(5 * len(mols), -1, np.int32)
+    rc = hc.b2hc_plan_classes(len(mols), _p(natm, ctypes.c_int), _p(nbas, ctypes.c_int), _p(atm, ctypes.c_int),
+                              _p(bas, ctypes.c_int), _p(env, ctypes.c_double), _p(eo, ctypes.c_longlong),
+                              _p(fast, ctypes.c_int), _p(ref, ctypes.c_int))
+    assert rc == 0
+    np.testing.assert_array_equal(fast, ref)
+    nsp = nbas.astype(np.int64) * (nbas + 1) // 2
+    np.testing.assert_array_equal(fast.reshape(-1, 5)[:, 4], nsp)
