@@ -331,19 +331,28 @@ def main():
         t0 = time.perf_counter()
         h2d = d2h = 0
         marks = [t0]
-        ke = max(a.steps, 6)             # at least 6 batches: one host hiccup weighs less
+        host = []
+        ke = max(a.steps, 10)            # at least 10 batches: one host hiccup weighs less
+        import gc
+        gcl = []                         # garbage-collector pauses in the timed region (ms)
+        gcb = lambda ph, info: gcl.append((ph, time.perf_counter(), info.get("generation")))
+        gc.callbacks.append(gcb)
         for _, out in run_batches([mols] * ke, **kw):
+            host.append(dict({k: round(v, 1) for k, v in out["host_ms"].items()}, its=out["its_run"]))
             h2d += out["h2d_bytes"]
             d2h += sum(v.nbytes for v in out.values() if isinstance(v, np.ndarray))
             marks.append(time.perf_counter())
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
+        gc.callbacks.remove(gcb)
+        gc_pauses = [round(1e3 * (b[1] - a_[1]), 1) for a_, b in zip(gcl[0::2], gcl[1::2]) if a_[2] == 2]
         barrier()
         dt = max_over_ranks(dt * 1000.0) / 1000.0
         e2e = {"value": shard.aggregate_rate(a.nmol, world, dt / ke), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d // ke), "d2h_bytes_per_step": int(d2h // ke),
                "steps": ke, "timing": "wall clock over the steps, max over ranks",
                "step_ms": [round(1e3 * (b - a_), 1) for a_, b in zip(marks[:-1], marks[1:])],
+               "step_host_ms": host, "gc_gen2_pauses_ms": gc_pauses,
                "api": "b200dft.engine.run_batches (plan of the next batch prefetched on a worker thread)"}
 
     if rank == 0:

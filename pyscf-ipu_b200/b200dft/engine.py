@@ -363,8 +363,12 @@ class RKSEngine:
 
     def run(self, its=20, use_diis=True, log=True):
         """Fixed-iteration SCF as in the reference (no convergence test, fori_loop of `its`)."""
+        import time
+        tm = {"initial": 0.0, "capture": 0.0, "graph_its": 0.0, "eager_its": 0.0, "restarts": 0}
+        t = time.perf_counter()
         self.prepare()
         self.initial()
+        tm["initial"] = 1e3 * (time.perf_counter() - t)
         nm = self.plan.nmol
         E = torch.zeros((its, nm, 5), dtype=torch.float64, device=self.device)
         mo = torch.zeros((its, nm, NMO), dtype=torch.float64, device=self.device)
@@ -401,8 +405,12 @@ class RKSEngine:
         is still iterating, the J/K and XC launches are compacted to those molecules (eager mode).
         Returns per-molecule energies, iterations (counted from the first start), flags and
         the energies of each molecule's last 5 iterations (``last5``, NaN where fewer ran)."""
+        import time
+        tm = {"initial": 0.0, "capture": 0.0, "graph_its": 0.0, "eager_its": 0.0, "restarts": 0}
+        t = time.perf_counter()
         self.prepare()
         self.initial()
+        tm["initial"] = 1e3 * (time.perf_counter() - t)
         nm = self.plan.nmol
         dev = self.device
         e_prev = torch.full((nm,), float("inf"), dtype=torch.float64, device=dev)
@@ -413,6 +421,7 @@ class RKSEngine:
         err_prev = torch.full((nm,), float("inf"), dtype=torch.float64, device=dev)
         hist = torch.full((nm, 5), float("nan"), dtype=torch.float64, device=dev)   # last 5 energies
         g = None
+        t = time.perf_counter()
         if graph:
             # capture one iteration (all launches go to the capture stream); replay per step
             st = torch.cuda.Stream()
@@ -433,6 +442,8 @@ class RKSEngine:
             self.graph_kernels_per_step = launch_count() - c0
             self._captured += self.graph_kernels_per_step
             # the capture did not execute the step: state is unchanged
+        tm["capture"] = 1e3 * (time.perf_counter() - t)
+        t = time.perf_counter()
         for i in range(max_its):
             if g is not None:
                 g.replay()
@@ -451,6 +462,7 @@ class RKSEngine:
                        & (err > rise * err_prev))
                 err_prev = torch.where(self.active > 0, err, err_prev)
                 if bool(bad.any()):
+                    tm["restarts"] += 1
                     self._restart_from_minao(bad)
                     fell_back |= bad
                     e_prev = torch.where(bad, torch.full_like(e_prev, float("inf")), e_prev)
@@ -464,10 +476,15 @@ class RKSEngine:
                     check(lib().b2_plan_set_subset(self.plan.h, ptr(np.ascontiguousarray(idx)), len(idx)),
                           "b2_plan_set_subset")
                     sub_n = n_act
+                    if g is not None:
+                        tm["graph_its"] = 1e3 * (time.perf_counter() - t)
+                        t = time.perf_counter()
                     g = None                                 # graph holds full-batch launches
+        tm["graph_its" if g is not None else "eager_its"] = 1e3 * (time.perf_counter() - t)
         if sub_n <= nm:
             check(lib().b2_plan_set_subset(self.plan.h, None, 0), "b2_plan_set_subset")
         E = self.energy.view(nm, 5)[:, 0].clone()
+        self.host_ms = tm                                # host wall time of the parts (ms)
         return dict(energy=E, iterations=conv_it, converged=conv_it > 0, mo_energy=self.mo_energy.view(nm, NMO),
                     diis_err=self.diis_err.clone(), its_run=i + 1, fell_back=fell_back, last5=hist)
 
@@ -496,16 +513,25 @@ def _run_one(mols, plan, level, precision, guess, net, run_kw, after_prepare=Non
     """one batch to convergence; returns host arrays, the engine's device memory released
     (back to the allocator cache, where the next batch's engine finds it).  ``after_prepare``
     runs once the batch's setup and ERI work is queued."""
+    import time
+    t0 = time.perf_counter()
     eng = RKSEngine(mols, level=level, precision=precision, guess=guess, net=net, plan=plan)
     try:
+        t1 = time.perf_counter()
         eng.prepare()
         if after_prepare is not None:
             after_prepare()
+        t2 = time.perf_counter()
         r = eng.run_converged(**run_kw)
         out = {k: r[k].cpu().numpy() for k in ("energy", "iterations", "converged", "mo_energy",
                                                "last5", "diis_err")}
+        t3 = time.perf_counter()
         out["its_run"] = r["its_run"]
         out["h2d_bytes"] = plan.h2d_bytes + getattr(getattr(eng, "_nn_batch", None), "h2d_bytes", 0)
+        # host wall time of the batch's parts (ms): engine set-up, setup + ERI launch, SCF to results
+        out["host_ms"] = {"engine": 1e3 * (t1 - t0), "prepare": 1e3 * (t2 - t1), "scf": 1e3 * (t3 - t2)}
+        out["host_ms"].update({"scf_" + k: v for k, v in getattr(eng, "host_ms", {}).items()})
+        out["its_run"] = r["its_run"]
         return out
     finally:
         eng.close()
@@ -533,8 +559,11 @@ def run_batches(batches, level=0, precision="mixed", guess="learned", net=None, 
 
     ex = ThreadPoolExecutor(1) if prefetch else None
     try:
+        import time
+        tw = time.perf_counter()
         first = next(it, None)
         cur = None if first is None else make(first)
+        wait_ms = 1e3 * (time.perf_counter() - tw)      # building the plan the next batch waited for
         while cur is not None:
             mols, plan = cur
             nxt = next(it, None)
@@ -543,11 +572,14 @@ def run_batches(batches, level=0, precision="mixed", guess="learned", net=None, 
             # queued, so they do not hold up the kernels this batch waits on first
             start = (lambda: fut.append(ex.submit(make, nxt))) if (ex and nxt is not None) else None
             out = _run_one(mols, plan, level, precision, guess, net, run_kw, after_prepare=start)
+            out["host_ms"]["plan_wait"] = wait_ms
             del plan                      # the engine and plan are released before the next batch
+            tw = time.perf_counter()
             if nxt is None:
                 cur = None
             else:
                 cur = fut[0].result() if fut else make(nxt)
+            wait_ms = 1e3 * (time.perf_counter() - tw)
             yield mols, out
     finally:
         if ex:
