@@ -3,13 +3,16 @@
 // (direct.py:584-707), and writes straight into the tril-of-tril s8 layout of
 // ``mol.intor('int2e_sph', aosym='s8')`` (nanoDFT.py:285).
 //
-// Decomposition: a host-built task list (plan) assigns each warp one bra shell pair IJ of one
+// Decomposition: a task list (built on the device from the plan's class counts, or on the host
+// for the allocation-free single-molecule entry) assigns each warp one bra shell pair IJ of one
 // molecule and a chunk of ket shell pairs KL of a single angular class (ss, ps, sp, pp), all
-// with KL <= (I,I) (32 kets per task for batch plans: warps stay full; 4 tasks per CTA); the
-// bra's primitive pairs are staged in the warp's shared-memory slot and every lane evaluates
-// all components of one shell quartet (float32 form) or of one bra component (float64 form,
-// p bras split over 3 lanes), looping over the chunk's kets.  Every s8 entry is written exactly once, by the
-// CTA whose bra shell pair owns its row ij.
+// with KL <= (I,I) (32 kets per task for batch plans, 128 for the single-molecule entry; 4 tasks
+// per CTA); the bra's primitive pairs are staged in the warp's shared-memory slot.  Batch plans
+// run the float32 classes with at most 27 components in the flattened kernel k_eri_fl (lanes
+// over the chunk's (ket, ket primitive pair) entries); otherwise (k_eri_sq) every lane evaluates
+// all components of one shell quartet (float32) or of one bra component (float64, p bras split
+// over 3 lanes), looping over the chunk's kets.  Every s8 entry is written exactly once, by the
+// warp whose bra shell pair owns its row ij.
 #include <type_traits>
 #include "eri_sq.cuh"
 #include "device_plan.cuh"
