@@ -1,0 +1,243 @@
+// Two-electron part of the RKS nuclear gradient for s / p shells (host and device code).
+//
+// The reference's gradient (nanoDFT.py:403-426) contracts int2e_ip1 = (d/dA_x i j|k l) with the
+// density: vj = -sum (d_i j|k l) D_lk, vk = -sum (d_i j|k l) D_jk, de_A += 2 <vj - hyb/2 vk,
+// D>_{i on A}.  Over all ordered index quartets that is
+//
+//   dE_2e / dR = sum_{ijkl} d(ij|kl)/dR  Gamma_ijkl,   Gamma = 1/2 D_ij D_kl - hyb/4 D_il D_jk,
+//
+// the derivative at fixed D of E_2e = 1/2 <D, J> - hyb/4 <D, K>.  For one shell quartet
+// (I J | K L) this file evaluates the derivatives with respect to the centres of I, J and K and
+// takes the fourth from translation invariance (the four sum to zero).  A primitive's
+// derivative is d/dA_x g_a = 2 alpha g_{a+1x} - a_x g_{a-1x}; the integrals over Cartesian
+// Gaussians come from the Obara-Saika vertical recursion (Obara & Saika, J. Chem. Phys. 84,
+// 3963 (1986)) for [e 0 | f 0], contracted with weights 1, 2 alpha, 2 beta, 2 gamma, then the
+// Head-Gordon-Pople horizontal recursion (J. Chem. Phys. 89, 5777 (1988)) moves angular
+// momentum to the second centre of each pair.  Shells are s or p (l <= 1), so Cartesian
+// components up to l = 3 occur.
+#pragma once
+#include "common.cuh"
+#include "boys.cuh"
+#include "plan_host.hpp"
+
+#define B2G_NC 20                  // Cartesian components of l = 0..3
+#define B2G_MMAX 6                 // Boys orders 0..5
+
+B2_HD int b2g_cstart(int l) { return l * (l + 1) * (l + 2) / 6; }
+B2_HD int b2g_ncart(int l) { return (l + 1) * (l + 2) * (l + 3) / 6; }   // components of 0..l
+// index of the Cartesian (x, y, z) among all components of l = 0..3 (order within a shell:
+// x descending, then y descending)
+B2_HD int b2g_cidx(int x, int y, int z) {
+  const int l = x + y + z;
+  return b2g_cstart(l) + (l - x) * (l - x + 1) / 2 + z;
+}
+B2_HD void b2g_cart(int idx, int &x, int &y, int &z) {
+  int l = 0;
+  while (b2g_cstart(l + 1) <= idx) ++l;
+  int r = idx - b2g_cstart(l);
+  int lx = l;                                    // r = (l - x)(l - x + 1)/2 + z
+  while (true) {
+    const int k = l - lx, base = k * (k + 1) / 2;
+    if (r < base + k + 1) { z = r - base; x = lx; y = l - x - z; return; }
+    --lx;
+  }
+}
+
+B2_HD double b2g_binom(int n, int k) { return (n == 2 && k == 1) ? 2.0 : 1.0; }   // n <= 2 here
+template <typename T> B2_HD T b2g_pow(T x, int n) { T r = (T)1; for (int i = 0; i < n; ++i) r *= x; return r; }
+
+// Boys F_0..F_L (L <= 5) from the float64 table (same scheme as b2_boys)
+template <typename T>
+B2_HD void b2g_boys(int L, T t, const T *btab, T *F) {
+  switch (L) {
+    case 0: b2_boys<T, 0, T>(t, btab, F); break;
+    case 1: b2_boys<T, 1, T>(t, btab, F); break;
+    case 2: b2_boys<T, 2, T>(t, btab, F); break;
+    case 3: b2_boys<T, 3, T>(t, btab, F); break;
+    case 4: b2_boys<T, 4, T>(t, btab, F); break;
+    default: b2_boys<T, 5, T>(t, btab, F); break;
+  }
+}
+
+// contracted [e 0 | f 0] for e over l <= le, f over l <= lf, with four weightings:
+// w = 0: plain, 1: x 2 alpha (first bra primitive), 2: x 2 beta (second bra), 3: x 2 gamma
+// (first ket).  Shells a, b, c, d (their coefficients include the angular factors).
+template <typename T>
+B2_HD void b2g_e0f0(const B2Shell &a, const B2Shell &b, const B2Shell &c, const B2Shell &d, int le, int lf,
+                    const T *btab, T (*acc)[B2G_NC][B2G_NC]) {
+  const int ne = b2g_ncart(le), nf = b2g_ncart(lf), L = le + lf;
+  for (int w = 0; w < 4; ++w)
+    for (int i = 0; i < ne; ++i)
+      for (int j = 0; j < nf; ++j) acc[w][i][j] = (T)0;
+  T AB2 = 0, CD2 = 0;
+  for (int x = 0; x < 3; ++x) {
+    AB2 += (T)((a.R[x] - b.R[x]) * (a.R[x] - b.R[x]));
+    CD2 += (T)((c.R[x] - d.R[x]) * (c.R[x] - d.R[x]));
+  }
+  for (int pa = 0; pa < a.nprim; ++pa)
+    for (int pb = 0; pb < b.nprim; ++pb) {
+      const T al = (T)a.exp[pa], be = (T)b.exp[pb], z = al + be;
+      T P[3], PA[3];
+      for (int x = 0; x < 3; ++x) {
+        P[x] = (al * (T)a.R[x] + be * (T)b.R[x]) / z;
+        PA[x] = P[x] - (T)a.R[x];
+      }
+      const T Kab = exp(-al * be / z * AB2) * (T)a.coef[pa] * (T)b.coef[pb];
+      for (int pc = 0; pc < c.nprim; ++pc)
+        for (int pd = 0; pd < d.nprim; ++pd) {
+          const T ga = (T)c.exp[pc], de = (T)d.exp[pd], e = ga + de;
+          T Q[3], QC[3], WP[3], WQ[3], PQ2 = 0;
+          for (int x = 0; x < 3; ++x) {
+            Q[x] = (ga * (T)c.R[x] + de * (T)d.R[x]) / e;
+            QC[x] = Q[x] - (T)c.R[x];
+            const T W = (z * P[x] + e * Q[x]) / (z + e);
+            WP[x] = W - P[x];
+            WQ[x] = W - Q[x];
+            PQ2 += (P[x] - Q[x]) * (P[x] - Q[x]);
+          }
+          const T rho = z * e / (z + e);
+          const T Kcd = exp(-ga * de / e * CD2) * (T)c.coef[pc] * (T)d.coef[pd];
+          // 2 pi^(5/2) / (z e sqrt(z + e))
+          const T pref = (T)34.98683665524972 / (z * e * sqrt(z + e)) * Kab * Kcd;
+          T F[B2G_MMAX];
+          b2g_boys<T>(L, rho * PQ2, btab, F);
+          T v[B2G_NC][B2G_NC][B2G_MMAX];
+          for (int m = 0; m <= L; ++m) v[0][0][m] = pref * F[m];
+          for (int l1 = 1; l1 <= le; ++l1)                // bra vertical recursion
+            for (int ie = b2g_cstart(l1); ie < b2g_cstart(l1 + 1); ++ie) {
+              int ex, ey, ez;
+              b2g_cart(ie, ex, ey, ez);
+              const int dd = ex ? 0 : (ey ? 1 : 2);
+              int e1[3] = {ex, ey, ez};
+              e1[dd]--;
+              const int i1 = b2g_cidx(e1[0], e1[1], e1[2]);
+              int i2 = -1;
+              if (e1[dd] > 0) {
+                int e2[3] = {e1[0], e1[1], e1[2]};
+                e2[dd]--;
+                i2 = b2g_cidx(e2[0], e2[1], e2[2]);
+              }
+              for (int m = 0; m <= L - l1; ++m) {
+                T t = PA[dd] * v[i1][0][m] + WP[dd] * v[i1][0][m + 1];
+                if (i2 >= 0) t += (T)e1[dd] / (2 * z) * (v[i2][0][m] - rho / z * v[i2][0][m + 1]);
+                v[ie][0][m] = t;
+              }
+            }
+          for (int l2 = 1; l2 <= lf; ++l2)                // ket vertical recursion
+            for (int jf = b2g_cstart(l2); jf < b2g_cstart(l2 + 1); ++jf) {
+              int fx, fy, fz;
+              b2g_cart(jf, fx, fy, fz);
+              const int dd = fx ? 0 : (fy ? 1 : 2);
+              int f1[3] = {fx, fy, fz};
+              f1[dd]--;
+              const int j1 = b2g_cidx(f1[0], f1[1], f1[2]);
+              int j2 = -1;
+              if (f1[dd] > 0) {
+                int f2[3] = {f1[0], f1[1], f1[2]};
+                f2[dd]--;
+                j2 = b2g_cidx(f2[0], f2[1], f2[2]);
+              }
+              for (int ie = 0; ie < ne; ++ie) {
+                int ex, ey, ez;
+                b2g_cart(ie, ex, ey, ez);
+                const int ec[3] = {ex, ey, ez};
+                const int l1 = ex + ey + ez;
+                int i3 = -1;
+                if (ec[dd] > 0) {
+                  int e3[3] = {ex, ey, ez};
+                  e3[dd]--;
+                  i3 = b2g_cidx(e3[0], e3[1], e3[2]);
+                }
+                for (int m = 0; m <= L - l1 - l2; ++m) {
+                  T t = QC[dd] * v[ie][j1][m] + WQ[dd] * v[ie][j1][m + 1];
+                  if (j2 >= 0) t += (T)f1[dd] / (2 * e) * (v[ie][j2][m] - rho / e * v[ie][j2][m + 1]);
+                  if (i3 >= 0) t += (T)ec[dd] / (2 * (z + e)) * v[i3][j1][m + 1];
+                  v[ie][jf][m] = t;
+                }
+              }
+            }
+          const T wt[4] = {(T)1, 2 * al, 2 * be, 2 * ga};
+          for (int w = 0; w < 4; ++w)
+            for (int i = 0; i < ne; ++i)
+              for (int j = 0; j < nf; ++j) acc[w][i][j] += wt[w] * v[i][j][0];
+        }
+    }
+}
+
+// (a b | c d) over Cartesian exponent triplets (a, b on the bra centres A, B; c, d on C, D) from
+// contracted [e 0 | f 0] (weighting w): horizontal recursion (a b+1_x| = (a+1_x b| + AB_x (a b|
+template <typename T>
+B2_HD T b2g_hrr(const T (*acc)[B2G_NC][B2G_NC], int w, const int *ea, const int *eb, const int *ec, const int *ed,
+                const T *AB, const T *CD) {
+  // expand b onto a: sum over binomial terms of (a + b')|, with weight AB^(b - b')
+  T s = 0;
+  for (int bx = 0; bx <= eb[0]; ++bx)
+    for (int by = 0; by <= eb[1]; ++by)
+      for (int bz = 0; bz <= eb[2]; ++bz) {
+        const T cb = (T)b2g_binom(eb[0], bx) * b2g_binom(eb[1], by) * b2g_binom(eb[2], bz) *
+                     b2g_pow(AB[0], eb[0] - bx) * b2g_pow(AB[1], eb[1] - by) * b2g_pow(AB[2], eb[2] - bz);
+        const int ie = b2g_cidx(ea[0] + bx, ea[1] + by, ea[2] + bz);
+        for (int dx = 0; dx <= ed[0]; ++dx)
+          for (int dy = 0; dy <= ed[1]; ++dy)
+            for (int dz = 0; dz <= ed[2]; ++dz) {
+              const T cd = (T)b2g_binom(ed[0], dx) * b2g_binom(ed[1], dy) * b2g_binom(ed[2], dz) *
+                           b2g_pow(CD[0], ed[0] - dx) * b2g_pow(CD[1], ed[1] - dy) * b2g_pow(CD[2], ed[2] - dz);
+              const int jf = b2g_cidx(ec[0] + dx, ec[1] + dy, ec[2] + dz);
+              s += cb * cd * acc[w][ie][jf];
+            }
+      }
+  return s;
+}
+
+// Cartesian exponents of component k of a shell with l <= 1 (s; p_x, p_y, p_z)
+B2_HD void b2g_comp(int l, int k, int *e) {
+  e[0] = e[1] = e[2] = 0;
+  if (l) e[k] = 1;
+}
+
+// Gradient contributions of the shell quartet (a b | c d) contracted with gam[ia][ib][ic][id]
+// (component order of each shell, flattened): g[s][x] = sum gam d(ab|cd)/dR_x of the centre of
+// shell s (s = 0..3; the fourth from translation invariance).
+template <typename T>
+B2_HD void b2g_quartet_grad(const B2Shell &a, const B2Shell &b, const B2Shell &c, const B2Shell &d,
+                            const T *btab, const T *gam, T g[4][3]) {
+  const int la = a.l, lb = b.l, lc = c.l, ld = d.l;
+  const int na = 2 * la + 1, nb = 2 * lb + 1, nc = 2 * lc + 1, nd = 2 * ld + 1;
+  T accB[4][B2G_NC][B2G_NC], accK[4][B2G_NC][B2G_NC];
+  b2g_e0f0<T>(a, b, c, d, la + lb + 1, lc + ld, btab, accB);   // bra raised by one (dA, dB)
+  b2g_e0f0<T>(a, b, c, d, la + lb, lc + ld + 1, btab, accK);   // ket raised by one (dC)
+  T AB[3], CD[3];
+  for (int x = 0; x < 3; ++x) {
+    AB[x] = (T)(a.R[x] - b.R[x]);
+    CD[x] = (T)(c.R[x] - d.R[x]);
+  }
+  for (int s = 0; s < 4; ++s) for (int x = 0; x < 3; ++x) g[s][x] = (T)0;
+  for (int ia = 0; ia < na; ++ia)
+    for (int ib = 0; ib < nb; ++ib)
+      for (int ic = 0; ic < nc; ++ic)
+        for (int id = 0; id < nd; ++id) {
+          const T gm = gam[((ia * nb + ib) * nc + ic) * nd + id];
+          if (gm == (T)0) continue;
+          int ea[3], eb[3], ec[3], ed[3];
+          b2g_comp(la, ia, ea); b2g_comp(lb, ib, eb); b2g_comp(lc, ic, ec); b2g_comp(ld, id, ed);
+          for (int x = 0; x < 3; ++x) {
+            int up[3], dn[3];
+            // d/dA_x: 2 alpha (a+1x b| - a_x (a-1x b|
+            for (int k = 0; k < 3; ++k) { up[k] = ea[k] + (k == x); dn[k] = ea[k] - (k == x); }
+            T dA = b2g_hrr<T>(accB, 1, up, eb, ec, ed, AB, CD);
+            if (ea[x]) dA -= (T)ea[x] * b2g_hrr<T>(accB, 0, dn, eb, ec, ed, AB, CD);
+            // d/dB_x: 2 beta (a b+1x| - b_x (a b-1x|
+            for (int k = 0; k < 3; ++k) { up[k] = eb[k] + (k == x); dn[k] = eb[k] - (k == x); }
+            T dB = b2g_hrr<T>(accB, 2, ea, up, ec, ed, AB, CD);
+            if (eb[x]) dB -= (T)eb[x] * b2g_hrr<T>(accB, 0, ea, dn, ec, ed, AB, CD);
+            // d/dC_x: 2 gamma (ab|c+1x d) - c_x (ab|c-1x d)
+            for (int k = 0; k < 3; ++k) { up[k] = ec[k] + (k == x); dn[k] = ec[k] - (k == x); }
+            T dC = b2g_hrr<T>(accK, 3, ea, eb, up, ed, AB, CD);
+            if (ec[x]) dC -= (T)ec[x] * b2g_hrr<T>(accK, 0, ea, eb, dn, ed, AB, CD);
+            g[0][x] += gm * dA;
+            g[1][x] += gm * dB;
+            g[2][x] += gm * dC;
+          }
+        }
+  for (int x = 0; x < 3; ++x) g[3][x] = -(g[0][x] + g[1][x] + g[2][x]);
+}

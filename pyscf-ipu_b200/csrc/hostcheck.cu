@@ -4,6 +4,7 @@
 // It is never loaded by the product path (libb200dft.so has no CPU fallback).
 #include "eri_row.cuh"
 #include "eri_sq.cuh"
+#include "grad_math.cuh"
 #include "xc_math.cuh"
 #include <vector>
 
@@ -89,6 +90,39 @@ int b2hc_plan_classes(int nmol, const int *natm, const int *nbas, const int *atm
       const int last = md.nsp ? R.cls_cnt[4ll * md.sp_off + (long long)c * md.nsp + md.nsp - 1] : 0;
       if (last != md.cls_start[c + 1] - md.cls_start[c]) return -100 - c;
     }
+  }
+  return 0;
+}
+
+// two-electron gradient of one molecule at fixed density D (nao x nao): g[natm][3] =
+// sum over all ordered shell quartets of d(ij|kl)/dR Gamma_ijkl, Gamma = 1/2 D_ij D_kl - hyb/4
+// D_il D_jk (the two-electron part of the reference's grad_elec, nanoDFT.py:403-426)
+int b2hc_grad_2e(int natm, int nbas, const int *atm, const int *bas, const double *env, const double *D,
+                 double hyb, double *g) {
+  B2PlanHost P;
+  const long long eo = 0;
+  int rc = b2_plan_build(P, 1, &natm, &nbas, atm, bas, env, &eo);
+  if (rc) return rc;
+  const int N = P.mols[0].nao;
+  std::vector<double> tab(B2_BOYS_NT * B2_BOYS_NM);
+  b2_boys_fill_table(tab.data());
+  for (int i = 0; i < 3 * natm; ++i) g[i] = 0;
+  const B2Shell *S = P.shells.data();
+  std::vector<double> gam(81);
+  for (int I = 0; I < nbas; ++I) for (int J = 0; J < nbas; ++J)
+  for (int K = 0; K < nbas; ++K) for (int L = 0; L < nbas; ++L) {
+    const B2Shell *q[4] = {&S[I], &S[J], &S[K], &S[L]};
+    const int n[4] = {2 * q[0]->l + 1, 2 * q[1]->l + 1, 2 * q[2]->l + 1, 2 * q[3]->l + 1};
+    for (int a = 0; a < n[0]; ++a) for (int b = 0; b < n[1]; ++b)
+    for (int c = 0; c < n[2]; ++c) for (int d = 0; d < n[3]; ++d) {
+      const int i = q[0]->ao0 + a, j = q[1]->ao0 + b, k = q[2]->ao0 + c, l = q[3]->ao0 + d;
+      gam[((a * n[1] + b) * n[2] + c) * n[3] + d] =
+          0.5 * D[i * N + j] * D[k * N + l] - 0.25 * hyb * D[i * N + l] * D[j * N + k];
+    }
+    double g4[4][3];
+    b2g_quartet_grad<double>(*q[0], *q[1], *q[2], *q[3], tab.data(), gam.data(), g4);
+    for (int s = 0; s < 4; ++s)
+      for (int x = 0; x < 3; ++x) g[3 * q[s]->atom + x] += g4[s][x];
   }
   return 0;
 }

@@ -105,3 +105,35 @@ def test_plan_class_starts_without_pair_tables():
     np.testing.assert_array_equal(fast, ref)
     nsp = nbas.astype(np.int64) * (nbas + 1) // 2
     np.testing.assert_array_equal(fast.reshape(-1, 5)[:, 4], nsp)
+
+
+def test_two_electron_gradient_vs_finite_differences():
+    """the two-electron gradient math (grad_math.cuh, host build) against central differences
+    of E_2e = sum (ij|kl) Gamma_ijkl at fixed density, Gamma = 1/2 D_ij D_kl - hyb/4 D_il D_jk,
+    with the ERI oracle at the displaced geometries"""
+    from oracle import grad as ograd
+    hc = _hc()
+    for mol in (Mole("O 0 0 0.1173; H 0 0.7572 -0.4692; H 0 -0.7532 -0.4792"), Mole(methane(1.05))):
+        N, hyb = mol.nao, 0.2
+        rng = np.random.default_rng(4)
+        D = rng.normal(size=(N, N)) * 0.3
+        D = np.ascontiguousarray(D + D.T)
+        gam = 0.5 * np.einsum("ij,kl->ijkl", D, D) - hyb / 4 * np.einsum("il,jk->ijkl", D, D)
+        g = np.zeros((mol.natm, 3))
+        atm = np.ascontiguousarray(mol._atm, np.int32)
+        bas = np.ascontiguousarray(mol._bas, np.int32)
+        env = np.ascontiguousarray(mol._env, np.float64)
+        rc = hc.b2hc_grad_2e(mol.natm, len(bas), _p(atm, ctypes.c_int), _p(bas, ctypes.c_int),
+                             _p(env, ctypes.c_double), _p(D, ctypes.c_double), ctypes.c_double(hyb),
+                             _p(g, ctypes.c_double))
+        assert rc == 0
+        h = 1e-4
+        fd = np.zeros_like(g)
+        for a in range(mol.natm):
+            for x in range(3):
+                e = [float((eri.unpack_s8(eri.eri_s8(ograd._displaced(mol, a, x, s * h)), N) * gam).sum())
+                     for s in (1, -1)]
+                fd[a, x] = (e[0] - e[1]) / (2 * h)
+        assert np.abs(fd).max() > 1e-2
+        np.testing.assert_allclose(g, fd, atol=1e-7 * max(1.0, np.abs(fd).max()), rtol=0)
+        np.testing.assert_allclose(g.sum(0), 0.0, atol=1e-9)    # translation invariance (exact)
