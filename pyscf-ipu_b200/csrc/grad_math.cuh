@@ -241,3 +241,144 @@ B2_HD void b2g_quartet_grad(const B2Shell &a, const B2Shell &b, const B2Shell &c
         }
   for (int x = 0; x < 3; ++x) g[3][x] = -(g[0][x] + g[1][x] + g[2][x]);
 }
+
+// ---------------------------------------------------------------- one-electron part
+// d/dR of <D, T + V_nuc> - <W, S> at fixed D and W (the h1aos and s1 terms of the reference's
+// grad_elec, nanoDFT.py:414-424), per ordered shell pair (a, b): overlap and kinetic integrals
+// from Obara-Saika one-dimensional overlap tables (kinetic energy by the Laplacian acting on the
+// ket function), nuclear attraction by the Obara-Saika vertical recursion in (a|1/r_C|0) and the
+// same binomial horizontal recursion as above; the derivative with respect to a nucleus C
+// follows from translation invariance of <a|1/|r - C||b>.
+
+// 1D overlap factors s[i][j] (up to 2 x 4) of a primitive pair: i on centre A, j on centre B
+template <typename T>
+B2_HD void b2g_ovl1d(T PA, T PB, T oz, int ni, int nj, T s[3][5]) {
+  s[0][0] = (T)1;
+  for (int i = 1; i <= ni; ++i) s[i][0] = PA * s[i - 1][0] + (i > 1 ? (T)(i - 1) * oz * s[i - 2][0] : (T)0);
+  for (int j = 1; j <= nj; ++j)
+    for (int i = 0; i <= ni; ++i)
+      s[i][j] = PB * s[i][j - 1] + oz * ((i > 0 ? (T)i * s[i - 1][j - 1] : (T)0) +
+                                         (j > 1 ? (T)(j - 1) * s[i][j - 2] : (T)0));
+}
+
+// g[0], g[1]: gradient on the centres of a and b; gC[atom] (natm x 3): on the nuclei.
+// D and W are the molecule's nao x nao matrices (row-major, stride N); Z / RC the nuclei.
+template <typename T>
+B2_HD void b2g_pair_grad_1e(const B2Shell &a, const B2Shell &b, const T *D, const T *Wm, int N, int natm,
+                            const T *Z, const T *RC, const T *btab, T g[2][3], T *gC) {
+  const int la = a.l, lb = b.l, na = 2 * la + 1, nb = 2 * lb + 1;
+  T AB[3], AB2 = 0;
+  for (int x = 0; x < 3; ++x) { AB[x] = (T)(a.R[x] - b.R[x]); AB2 += AB[x] * AB[x]; }
+  for (int s = 0; s < 2; ++s) for (int x = 0; x < 3; ++x) g[s][x] = (T)0;
+  // nuclear attraction: contracted Theta[w][e], e up to la + lb + 1, per nucleus
+  const int le = la + lb + 1, ne = b2g_ncart(le);
+  for (int pa = 0; pa < a.nprim; ++pa)
+    for (int pb = 0; pb < b.nprim; ++pb) {
+      const T al = (T)a.exp[pa], be = (T)b.exp[pb], z = al + be, oz = (T)0.5 / z;
+      T P[3], PA[3], PB[3];
+      for (int x = 0; x < 3; ++x) {
+        P[x] = (al * (T)a.R[x] + be * (T)b.R[x]) / z;
+        PA[x] = P[x] - (T)a.R[x];
+        PB[x] = P[x] - (T)b.R[x];
+      }
+      const T cab = (T)a.coef[pa] * (T)b.coef[pb] * exp(-al * be / z * AB2);
+      const T pref3 = cab * pow((T)3.141592653589793 / z, (T)1.5);
+      T s1[3][3][5];
+      for (int x = 0; x < 3; ++x) b2g_ovl1d<T>(PA[x], PB[x], oz, la + 1, lb + 3, s1[x]);
+      auto S3 = [&](const int *ea, const int *eb) -> T {
+        return pref3 * s1[0][ea[0]][eb[0]] * s1[1][ea[1]][eb[1]] * s1[2][ea[2]][eb[2]];
+      };
+      auto T3 = [&](const int *ea, const int *eb) -> T {   // -1/2 <a| lap |b>
+        T t = 0;
+        for (int x = 0; x < 3; ++x) {
+          int e2[3] = {eb[0], eb[1], eb[2]};
+          T u = -(T)2 * be * (T)(2 * eb[x] + 1) * S3(ea, eb);
+          e2[x] = eb[x] + 2;
+          u += (T)4 * be * be * S3(ea, e2);
+          if (eb[x] >= 2) { e2[x] = eb[x] - 2; u += (T)(eb[x] * (eb[x] - 1)) * S3(ea, e2); }
+          t += u;
+        }
+        return (T)-0.5 * t;
+      };
+      for (int ia = 0; ia < na; ++ia)
+        for (int ib = 0; ib < nb; ++ib) {
+          int ea[3], eb[3];
+          b2g_comp(la, ia, ea);
+          b2g_comp(lb, ib, eb);
+          const int i = a.ao0 + ia, j = b.ao0 + ib;
+          const T dij = D[i * N + j], wij = Wm[i * N + j];
+          for (int x = 0; x < 3; ++x) {
+            int up[3] = {ea[0], ea[1], ea[2]}, dn[3] = {ea[0], ea[1], ea[2]};
+            up[x]++; dn[x]--;
+            T dS = (T)2 * al * S3(up, eb), dT = (T)2 * al * T3(up, eb);
+            if (ea[x]) { dS -= (T)ea[x] * S3(dn, eb); dT -= (T)ea[x] * T3(dn, eb); }
+            g[0][x] += dij * dT - wij * dS;
+            int ub[3] = {eb[0], eb[1], eb[2]}, db[3] = {eb[0], eb[1], eb[2]};
+            ub[x]++; db[x]--;
+            dS = (T)2 * be * S3(ea, ub); dT = (T)2 * be * T3(ea, ub);
+            if (eb[x]) { dS -= (T)eb[x] * S3(ea, db); dT -= (T)eb[x] * T3(ea, db); }
+            g[1][x] += dij * dT - wij * dS;
+          }
+        }
+      // nuclear attraction, nucleus by nucleus
+      for (int c = 0; c < natm; ++c) {
+        T PC[3], PC2 = 0;
+        for (int x = 0; x < 3; ++x) { PC[x] = P[x] - RC[3 * c + x]; PC2 += PC[x] * PC[x]; }
+        T F[B2G_MMAX];
+        b2g_boys<T>(le, z * PC2, btab, F);
+        T th[B2G_NC][B2G_MMAX];
+        const T p0 = -Z[c] * (T)6.283185307179586 / z * cab;
+        for (int m = 0; m <= le; ++m) th[0][m] = p0 * F[m];
+        for (int l1 = 1; l1 <= le; ++l1)
+          for (int ie = b2g_cstart(l1); ie < b2g_cstart(l1 + 1); ++ie) {
+            int ex, ey, ez;
+            b2g_cart(ie, ex, ey, ez);
+            const int dd = ex ? 0 : (ey ? 1 : 2);
+            int e1[3] = {ex, ey, ez};
+            e1[dd]--;
+            const int i1 = b2g_cidx(e1[0], e1[1], e1[2]);
+            int i2 = -1;
+            if (e1[dd] > 0) {
+              int e2[3] = {e1[0], e1[1], e1[2]};
+              e2[dd]--;
+              i2 = b2g_cidx(e2[0], e2[1], e2[2]);
+            }
+            for (int m = 0; m <= le - l1; ++m) {
+              T t = PA[dd] * th[i1][m] - PC[dd] * th[i1][m + 1];
+              if (i2 >= 0) t += (T)e1[dd] * oz * (th[i2][m] - th[i2][m + 1]);
+              th[ie][m] = t;
+            }
+          }
+        auto V3 = [&](const int *ea, const int *eb) -> T {    // binomial horizontal recursion
+          T s = 0;
+          for (int bx = 0; bx <= eb[0]; ++bx)
+            for (int by = 0; by <= eb[1]; ++by)
+              for (int bz = 0; bz <= eb[2]; ++bz)
+                s += (T)(b2g_binom(eb[0], bx) * b2g_binom(eb[1], by) * b2g_binom(eb[2], bz)) *
+                     b2g_pow(AB[0], eb[0] - bx) * b2g_pow(AB[1], eb[1] - by) * b2g_pow(AB[2], eb[2] - bz) *
+                     th[b2g_cidx(ea[0] + bx, ea[1] + by, ea[2] + bz)][0];
+          return s;
+        };
+        for (int ia = 0; ia < na; ++ia)
+          for (int ib = 0; ib < nb; ++ib) {
+            int ea[3], eb[3];
+            b2g_comp(la, ia, ea);
+            b2g_comp(lb, ib, eb);
+            const T dij = D[(a.ao0 + ia) * N + b.ao0 + ib];
+            for (int x = 0; x < 3; ++x) {
+              int up[3] = {ea[0], ea[1], ea[2]}, dn[3] = {ea[0], ea[1], ea[2]};
+              up[x]++; dn[x]--;
+              T dA = (T)2 * al * V3(up, eb);
+              if (ea[x]) dA -= (T)ea[x] * V3(dn, eb);
+              int ub[3] = {eb[0], eb[1], eb[2]}, db[3] = {eb[0], eb[1], eb[2]};
+              ub[x]++; db[x]--;
+              T dB = (T)2 * be * V3(ea, ub);
+              if (eb[x]) dB -= (T)eb[x] * V3(ea, db);
+              g[0][x] += dij * dA;
+              g[1][x] += dij * dB;
+              gC[3 * c + x] -= dij * (dA + dB);
+            }
+          }
+      }
+    }
+}

@@ -127,6 +127,36 @@ int b2hc_grad_2e(int natm, int nbas, const int *atm, const int *bas, const doubl
   return 0;
 }
 
+// one-electron gradient of one molecule at fixed D and W (nao x nao): g[natm][3] = d/dR of
+// <D, T + V_nuc> - <W, S> (nuclear repulsion not included)
+int b2hc_grad_1e(int natm, int nbas, const int *atm, const int *bas, const double *env, const double *D,
+                 const double *W, double *g) {
+  B2PlanHost P;
+  const long long eo = 0;
+  int rc = b2_plan_build(P, 1, &natm, &nbas, atm, bas, env, &eo);
+  if (rc) return rc;
+  const int N = P.mols[0].nao;
+  std::vector<double> tab(B2_BOYS_NT * B2_BOYS_NM);
+  b2_boys_fill_table(tab.data());
+  std::vector<double> Z(natm), RC(3 * natm);
+  for (int c = 0; c < natm; ++c) {
+    Z[c] = P.atom_z[c];
+    for (int x = 0; x < 3; ++x) RC[3 * c + x] = P.atom_xyz[3 * c + x];
+  }
+  for (int i = 0; i < 3 * natm; ++i) g[i] = 0;
+  const B2Shell *S = P.shells.data();
+  for (int I = 0; I < nbas; ++I)
+    for (int J = 0; J < nbas; ++J) {
+      double g2[2][3];
+      b2g_pair_grad_1e<double>(S[I], S[J], D, W, N, natm, Z.data(), RC.data(), tab.data(), g2, g);
+      for (int x = 0; x < 3; ++x) {
+        g[3 * S[I].atom + x] += g2[0][x];
+        g[3 * S[J].atom + x] += g2[1][x];
+      }
+    }
+  return 0;
+}
+
 int b2hc_b3lyp(int n, const double *rho, double *exc, double *vrho, double *vgamma) {
   for (int g = 0; g < n; ++g) {
     double r[4] = {rho[g], rho[n + g], rho[2 * n + g], rho[3 * n + g]};

@@ -137,3 +137,37 @@ def test_two_electron_gradient_vs_finite_differences():
         assert np.abs(fd).max() > 1e-2
         np.testing.assert_allclose(g, fd, atol=1e-7 * max(1.0, np.abs(fd).max()), rtol=0)
         np.testing.assert_allclose(g.sum(0), 0.0, atol=1e-9)    # translation invariance (exact)
+
+
+def test_one_electron_gradient_vs_finite_differences():
+    """the one-electron gradient math (host build) against central differences of
+    <D, T + V_nuc> - <W, S> at fixed D and W, with the host 1e integrals at displaced geometries"""
+    from oracle import grad as ograd
+    from b200dft.int1e import int1e
+    hc = _hc()
+    for mol in (Mole("O 0 0 0.1173; H 0 0.7572 -0.4692; H 0 -0.7532 -0.4792"), Mole(methane(1.05))):
+        N = mol.nao
+        rng = np.random.default_rng(6)
+        D = rng.normal(size=(N, N)) * 0.3
+        D = np.ascontiguousarray(D + D.T)
+        W = rng.normal(size=(N, N)) * 0.3
+        W = np.ascontiguousarray(W + W.T)
+        g = np.zeros((mol.natm, 3))
+        atm = np.ascontiguousarray(mol._atm, np.int32)
+        bas = np.ascontiguousarray(mol._bas, np.int32)
+        env = np.ascontiguousarray(mol._env, np.float64)
+        rc = hc.b2hc_grad_1e(mol.natm, len(bas), _p(atm, ctypes.c_int), _p(bas, ctypes.c_int),
+                             _p(env, ctypes.c_double), _p(D, ctypes.c_double), _p(W, ctypes.c_double),
+                             _p(g, ctypes.c_double))
+        assert rc == 0
+        h = 1e-4
+        fd = np.zeros_like(g)
+        for a in range(mol.natm):
+            for x in range(3):
+                e = []
+                for s in (1, -1):
+                    S, T, V = int1e(ograd._displaced(mol, a, x, s * h))
+                    e.append(float((D * (T + V)).sum() - (W * S).sum()))
+                fd[a, x] = (e[0] - e[1]) / (2 * h)
+        assert np.abs(fd).max() > 1e-2
+        np.testing.assert_allclose(g, fd, atol=1e-7 * max(1.0, np.abs(fd).max()), rtol=0)
