@@ -19,6 +19,7 @@
 #include "common.cuh"
 #include "boys.cuh"
 #include "plan_host.hpp"
+#include "xc_math.cuh"
 
 #define B2G_NC 20                  // Cartesian components of l = 0..3
 #define B2G_MMAX 6                 // Boys orders 0..5
@@ -381,4 +382,44 @@ B2_HD void b2g_pair_grad_1e(const B2Shell &a, const B2Shell &b, const T *D, cons
           }
       }
     }
+}
+
+// ---------------------------------------------------------------- exchange-correlation part
+// d/dR of E_xc at fixed D on a fixed grid (the V_xc terms of the reference's grad_elec,
+// nanoDFT.py:408-415; the grid does not move with the atoms, as there).  Moving atom A moves its
+// orbitals (d phi_i / dR_A = -grad phi_i), so with u = D phi, u_k = D d_k phi, g = grad rho:
+//   dE/dR_A,x = -2 sum_g w sum_{i on A} [vrho d_x phi_i u_i
+//                                        + 2 vgamma sum_k g_k (d_x d_k phi_i u_i + d_x phi_i u_k,i)]
+
+// values, gradients and Hessians (xx, xy, xz, yy, yz, zz) of the components of shell S at r
+template <typename T>
+B2_HD void b2g_ao2(const B2Shell &S, const T *r, T *f, T (*df)[3], T (*hf)[6]) {
+  T d[3], r2 = 0;
+  for (int x = 0; x < 3; ++x) { d[x] = r[x] - (T)S.R[x]; r2 += d[x] * d[x]; }
+  T g0 = 0, g1 = 0, g2 = 0;                    // sum c e, sum c (-2a) e, sum c 4a^2 e
+  for (int k = 0; k < S.nprim; ++k) {
+    const T al = (T)S.exp[k], e = (T)S.coef[k] * exp(-al * r2);
+    g0 += e;
+    g1 += (T)-2 * al * e;
+    g2 += (T)4 * al * al * e;
+  }
+  const int hk[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+  if (S.l == 0) {
+    f[0] = g0;
+    for (int x = 0; x < 3; ++x) df[0][x] = g1 * d[x];
+    for (int h = 0; h < 6; ++h) {
+      const int p = hk[h][0], q = hk[h][1];
+      hf[0][h] = g2 * d[p] * d[q] + (p == q ? g1 : (T)0);
+    }
+    return;
+  }
+  for (int c = 0; c < 3; ++c) {
+    f[c] = d[c] * g0;
+    for (int x = 0; x < 3; ++x) df[c][x] = (x == c ? g0 : (T)0) + d[c] * d[x] * g1;
+    for (int h = 0; h < 6; ++h) {
+      const int p = hk[h][0], q = hk[h][1];
+      hf[c][h] = (p == c ? g1 * d[q] : (T)0) + (q == c ? g1 * d[p] : (T)0) +
+                 d[c] * ((p == q ? g1 : (T)0) + d[p] * d[q] * g2);
+    }
+  }
 }

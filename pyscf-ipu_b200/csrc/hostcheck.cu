@@ -157,6 +157,59 @@ int b2hc_grad_1e(int natm, int nbas, const int *atm, const int *bas, const doubl
   return 0;
 }
 
+// exchange-correlation gradient of one molecule at fixed D on the grid (coords G x 3, w):
+// g[natm][3] = dE_xc/dR with the grid held fixed (B3LYP of xc_math.cuh)
+int b2hc_grad_xc(int natm, int nbas, const int *atm, const int *bas, const double *env, const double *D,
+                 long long G, const double *coords, const double *w, double *g) {
+  B2PlanHost P;
+  const long long eo = 0;
+  int rc = b2_plan_build(P, 1, &natm, &nbas, atm, bas, env, &eo);
+  if (rc) return rc;
+  const int N = P.mols[0].nao;
+  const B2Shell *S = P.shells.data();
+  std::vector<double> f(N), u(N), uk(3 * N), df(3 * N), hf(6 * N);
+  std::vector<int> own(N);
+  for (int s = 0; s < nbas; ++s)
+    for (int c = 0; c < 2 * S[s].l + 1; ++c) own[S[s].ao0 + c] = S[s].atom;
+  for (int i = 0; i < 3 * natm; ++i) g[i] = 0;
+  for (long long p = 0; p < G; ++p) {
+    for (int s = 0; s < nbas; ++s) {
+      double ff[3], dd[3][3], hh[3][6];
+      b2g_ao2<double>(S[s], coords + 3 * p, ff, dd, hh);
+      for (int c = 0; c < 2 * S[s].l + 1; ++c) {
+        const int i = S[s].ao0 + c;
+        f[i] = ff[c];
+        for (int x = 0; x < 3; ++x) df[3 * i + x] = dd[c][x];
+        for (int h = 0; h < 6; ++h) hf[6 * i + h] = hh[c][h];
+      }
+    }
+    double rho = 0, r1[3] = {0, 0, 0};
+    for (int i = 0; i < N; ++i) {
+      double a = 0, b[3] = {0, 0, 0};
+      for (int j = 0; j < N; ++j) {
+        a += D[i * N + j] * f[j];
+        for (int x = 0; x < 3; ++x) b[x] += D[i * N + j] * df[3 * j + x];
+      }
+      u[i] = a;
+      for (int x = 0; x < 3; ++x) uk[3 * i + x] = b[x];
+      rho += f[i] * a;
+      for (int x = 0; x < 3; ++x) r1[x] += df[3 * i + x] * a;
+    }
+    const B2XcPoint<double> o = b2_b3lyp_point<double>(rho, r1[0], r1[1], r1[2]);
+    const double gr[3] = {2 * r1[0], 2 * r1[1], 2 * r1[2]};       // grad rho
+    const int hidx[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    for (int i = 0; i < N; ++i)
+      for (int x = 0; x < 3; ++x) {
+        double t = o.vrho * df[3 * i + x] * u[i];
+        double q = 0;
+        for (int k = 0; k < 3; ++k) q += gr[k] * (hf[6 * i + hidx[x][k]] * u[i] + df[3 * i + x] * uk[3 * i + k]);
+        t += 2 * o.vgamma * q;
+        g[3 * own[i] + x] -= 2 * w[p] * t;
+      }
+  }
+  return 0;
+}
+
 int b2hc_b3lyp(int n, const double *rho, double *exc, double *vrho, double *vgamma) {
   for (int g = 0; g < n; ++g) {
     double r[4] = {rho[g], rho[n + g], rho[2 * n + g], rho[3 * n + g]};

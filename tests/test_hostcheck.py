@@ -171,3 +171,35 @@ def test_one_electron_gradient_vs_finite_differences():
                 fd[a, x] = (e[0] - e[1]) / (2 * h)
         assert np.abs(fd).max() > 1e-2
         np.testing.assert_allclose(g, fd, atol=1e-7 * max(1.0, np.abs(fd).max()), rtol=0)
+
+
+def test_xc_gradient_vs_finite_differences():
+    """the exchange-correlation gradient math (host build) against central differences of the
+    oracle's E_xc at fixed density on a fixed grid (the grid does not move with the atoms, as in
+    the reference's gradient)"""
+    from oracle import grad as ograd
+    from b200dft.grids import build_grid
+    from b200dft.guess import minao
+    hc = _hc()
+    mol = Mole("O 0 0 0.1173; H 0 0.7572 -0.4692; H 0 -0.7532 -0.4792")
+    grid = build_grid(mol, 0)
+    coords = np.ascontiguousarray(grid.coords, np.float64)
+    w = np.ascontiguousarray(grid.weights, np.float64)
+    D = np.ascontiguousarray(minao(mol), np.float64)
+    g = np.zeros((mol.natm, 3))
+    atm = np.ascontiguousarray(mol._atm, np.int32)
+    bas = np.ascontiguousarray(mol._bas, np.int32)
+    env = np.ascontiguousarray(mol._env, np.float64)
+    rc = hc.b2hc_grad_xc(mol.natm, len(bas), _p(atm, ctypes.c_int), _p(bas, ctypes.c_int),
+                         _p(env, ctypes.c_double), _p(D, ctypes.c_double), ctypes.c_longlong(len(w)),
+                         _p(coords, ctypes.c_double), _p(w, ctypes.c_double), _p(g, ctypes.c_double))
+    assert rc == 0
+    h = 1e-4
+    fd = np.zeros_like(g)
+    for a in range(mol.natm):
+        for x in range(3):
+            e = [rks.exchange_correlation(D, rks.ao_values(ograd._displaced(mol, a, x, s * h), coords), w)[0]
+                 for s in (1, -1)]
+            fd[a, x] = (e[0] - e[1]) / (2 * h)
+    assert np.abs(fd).max() > 1e-2
+    np.testing.assert_allclose(g, fd, atol=1e-6 * max(1.0, np.abs(fd).max()), rtol=0)
