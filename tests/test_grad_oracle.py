@@ -60,3 +60,36 @@ def test_gradient_methane_symmetry():
     np.testing.assert_allclose(along, along[0], atol=1e-6, rtol=0)
     np.testing.assert_allclose(g[1:] - along[:, None] * u, 0.0, atol=1e-6)
     assert along[0] > 1e-3                           # stretched C-H bonds pull inwards: dE/dr > 0
+
+
+def test_analytic_gradient_parts_sum_to_the_oracle():
+    """one-electron + two-electron + exchange-correlation gradient math (grad_math.cuh, host
+    build) plus the nuclear-repulsion derivative (nanoDFT.py:428-438) reproduce the oracle's
+    gradient of a converged SCF"""
+    import ctypes
+    from test_hostcheck import _hc, _p
+    hc = _hc()
+    mol = Mole("O 0 0 0.1173; H 0 0.7572 -0.4692; H 0 -0.7532 -0.4792")
+    coords, w = _grid(mol)
+    r = _scf(mol, coords, w)
+    nocc = mol.nelectron // 2
+    C = r["mo_coeff"][:, :nocc]
+    dm0 = np.ascontiguousarray(2 * C @ C.T)
+    dme0 = np.ascontiguousarray(2 * (C * r["mo_energy"][:nocc]) @ C.T)
+    atm = np.ascontiguousarray(mol._atm, np.int32)
+    bas = np.ascontiguousarray(mol._bas, np.int32)
+    env = np.ascontiguousarray(mol._env, np.float64)
+    args = (mol.natm, len(bas), _p(atm, ctypes.c_int), _p(bas, ctypes.c_int), _p(env, ctypes.c_double))
+    g1, g2, gx = (np.zeros((mol.natm, 3)) for _ in range(3))
+    assert hc.b2hc_grad_1e(*args, _p(dm0, ctypes.c_double), _p(dme0, ctypes.c_double), _p(g1, ctypes.c_double)) == 0
+    assert hc.b2hc_grad_2e(*args, _p(dm0, ctypes.c_double), ctypes.c_double(rks.HYB), _p(g2, ctypes.c_double)) == 0
+    assert hc.b2hc_grad_xc(*args, _p(dm0, ctypes.c_double), ctypes.c_longlong(len(w)), _p(coords, ctypes.c_double),
+                           _p(w, ctypes.c_double), _p(gx, ctypes.c_double)) == 0
+    Z = mol.charges.astype(np.float64)
+    dR = mol.coords[:, None, :] - mol.coords[None, :, :]
+    dist = np.linalg.norm(dR, axis=2)
+    np.fill_diagonal(dist, np.inf)
+    gn = -(Z[:, None, None] * Z[None, :, None] * dR / dist[:, :, None] ** 3).sum(1)
+    g = g1 + g2 + gx + gn
+    ref = ograd.gradient(mol, r["mo_coeff"], r["mo_energy"], coords, w)
+    np.testing.assert_allclose(g, ref, atol=1e-7, rtol=0)
