@@ -203,3 +203,28 @@ def test_xc_gradient_vs_finite_differences():
             fd[a, x] = (e[0] - e[1]) / (2 * h)
     assert np.abs(fd).max() > 1e-2
     np.testing.assert_allclose(g, fd, atol=1e-6 * max(1.0, np.abs(fd).max()), rtol=0)
+
+
+def test_gradient_math_compiles_for_sm100a(tmp_path):
+    """the gradient math is host and device code: it must also build as sm_100a device code"""
+    import shutil
+    import subprocess
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(nvcc):
+        pytest.skip("nvcc not available")
+    csrc = os.path.join(os.path.dirname(os.path.dirname(HOSTCHECK_PATH)), "..", "csrc")
+    src = tmp_path / "k.cu"
+    src.write_text(
+        '#include "grad_math.cuh"\n'
+        "__global__ void k(const B2Shell *s, const double *t, const double *gam, const double *D,\n"
+        "                  const double *W, const double *Z, const double *RC, const double *r, double *o) {\n"
+        "  double g4[4][3], g2[2][3], f[3], df[3][3], hf[3][6];\n"
+        "  b2g_quartet_grad<double>(s[0], s[1], s[2], s[3], t, gam, g4);\n"
+        "  b2g_pair_grad_1e<double>(s[0], s[1], D, W, 9, 5, Z, RC, t, g2, o);\n"
+        "  b2g_ao2<double>(s[0], r, f, df, hf);\n"
+        "  o[0] += g4[0][0] + g2[0][0] + f[0] + df[0][0] + hf[0][0];\n"
+        "}\n")
+    r = subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++17", "-O1",
+                        "--expt-relaxed-constexpr", "-I", csrc, "-c", str(src), "-o", str(tmp_path / "k.o")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
