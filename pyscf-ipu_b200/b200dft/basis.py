@@ -14,6 +14,7 @@ rescaled so the contracted radial function R(r) = sum_i c'_i r^l exp(-a_i r^2)
 has int R^2 r^2 dr = 1; the angular factor 1/sqrt(4 pi) (s) or sqrt(3/(4 pi)) (p)
 is applied by the integral code (cpu_int2e_sph.cpp, CINTcommon_fac_sp).
 """
+import functools
 import math
 import numpy as np
 
@@ -53,13 +54,20 @@ def gto_norm(l, a):
 
 
 def normalized_coefficients(l, exps, coefs):
-    """libcint-convention contracted coefficients (radial part normalised to 1)."""
+    """libcint-convention contracted coefficients (radial part normalised to 1); cached per
+    shell (a basis has few distinct shells, every molecule reuses them)"""
+    return np.array(_normalized_coefficients(int(l), tuple(float(a) for a in exps),
+                                             tuple(float(c) for c in coefs)))
+
+
+@functools.lru_cache(maxsize=None)
+def _normalized_coefficients(l, exps, coefs):
     exps = np.asarray(exps, dtype=np.float64)
     cs = np.asarray(coefs, dtype=np.float64) * np.array([gto_norm(l, a) for a in exps])
     ee = exps[:, None] + exps[None, :]
     ovl = np.vectorize(lambda a: gaussian_int(2 * l + 2, a))(ee)
     s = cs @ ovl @ cs
-    return cs / math.sqrt(s)
+    return tuple((cs / math.sqrt(s)).tolist())
 
 
 def get_basis(name):

@@ -17,10 +17,15 @@ def _unit(v):
     return v / np.linalg.norm(v)
 
 
+def _cross(a, b):
+    """cross product of 3-vectors (the same arithmetic as np.cross, without its generality)"""
+    return np.array([a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]])
+
+
 def _perp(u, rng):
     a = np.array([1.0, 0, 0]) if abs(u[0]) < 0.9 else np.array([0, 1.0, 0])
-    p = _unit(np.cross(u, a))
-    q = np.cross(u, p)
+    p = _unit(_cross(u, a))
+    q = _cross(u, p)
     phi = rng.uniform(0, 2 * np.pi)
     return np.cos(phi) * p + np.sin(phi) * q, -np.sin(phi) * p + np.cos(phi) * q
 
@@ -42,7 +47,7 @@ def free_directions(bonds, rng):
         return out
     if len(b) == 2:
         m = -_unit(b[0] + b[1])
-        n = _unit(np.cross(b[0], b[1]))
+        n = _unit(_cross(b[0], b[1]))
         be = np.radians(TET / 2)
         return [np.cos(be) * m + np.sin(be) * n, np.cos(be) * m - np.sin(be) * n]
     if len(b) == 3:
