@@ -17,12 +17,16 @@ the GDB-11 SMILES + RDKit conformers the reference reads, which are not availabl
 
 Pipelining (the reference overlaps host preparation with device compute the same way): a
 ``spawn`` process pool generates and parses molecules in chunks of one batch; a host thread
-keeps the next batch ready, its plan already built and on the device, while the GPU runs the
-current one; a writer thread converts and appends finished batches.  Each batch is one ``RKSEngine`` run to convergence: molecules retire
-individually as they converge (their kernels skip them, and the J/K and XC launches are
-compacted to the stragglers), so a batch ends when its slowest molecule converges.
+keeps the next batch ready while the GPU runs the current one (the workers also make each
+molecule's static row columns); ``engine.run_batches`` runs the batches, building each next plan
+on its worker thread once the current batch's ERI work is queued; a writer thread converts and
+appends finished batches (result columns by numpy).  Each batch is one ``RKSEngine`` run to
+convergence: molecules retire individually as they converge (their kernels skip them, and the
+J/K and XC launches are compacted to the stragglers), so a batch ends when its slowest molecule
+converges.
 """
 import argparse
+import collections
 import json
 import multiprocessing as mp
 import os
@@ -35,7 +39,7 @@ import numpy as np
 import torch
 
 from .constants import HARTREE_TO_EV
-from .engine import Plan, RKSEngine
+from .engine import run_batches
 from .molgen import stream_chunk
 
 QM1B_COLUMNS = ("smile", "atoms", "z", "energy", "homo", "lumo", "N", "std", "y", "pos")
@@ -46,32 +50,55 @@ def _formula(symbols):
     return "".join(f"{e}{c[e] if c[e] > 1 else ''}" for e in sorted(c, key=lambda e: (e != "C", e != "H", e)))
 
 
+def static_columns(idx, m, seed):
+    """the columns of one molecule that do not depend on its SCF (computed where the molecule is
+    generated, in the worker processes)"""
+    return {"smile": f"gen:{seed}:{idx}:{_formula(m.symbols)}", "atoms": "".join(m.symbols),
+            "z": [int(z) for z in m.charges], "pos": [float(x) for x in m.coords.reshape(-1)]}
+
+
+def _low_priority():
+    """worker initialiser: generation yields the cores to the process that drives the GPU"""
+    try:
+        os.nice(10)
+    except OSError:
+        pass
+
+
+def prepare_chunk(args):
+    """worker: molecules of one chunk of the stream with their static columns"""
+    items = stream_chunk(args)
+    return [(i, s, m, static_columns(i, m, args[0])) for i, s, m in items]
+
+
 def batch_rows(items, res, seed):
-    """rows (dict of columns) of one finished batch"""
-    E = res["energy"].cpu().numpy() * HARTREE_TO_EV
-    mo = res["mo_energy"].cpu().numpy()
-    last5 = res["last5"].cpu().numpy() * HARTREE_TO_EV
-    its = res["iterations"].cpu().numpy()
-    conv = res["converged"].cpu().numpy()
-    cols = {k: [] for k in QM1B_COLUMNS + ("iterations", "converged", "last5")}
-    for j, (idx, _, m) in enumerate(items):
-        nocc = m.nelectron // 2
-        homo = float(mo[j, nocc - 1]) * HARTREE_TO_EV
-        lumo = float(mo[j, nocc]) * HARTREE_TO_EV if nocc < m.nao else float("nan")
-        l5 = last5[j][np.isfinite(last5[j])]
-        cols["smile"].append(f"gen:{seed}:{idx}:{_formula(m.symbols)}")
-        cols["atoms"].append("".join(m.symbols))
-        cols["z"].append([int(z) for z in m.charges])
-        cols["energy"].append(float(E[j]))
-        cols["homo"].append(homo)
-        cols["lumo"].append(lumo)
-        cols["N"].append(int(m.nao))
-        cols["std"].append(float(np.std(l5)) if len(l5) else float("nan"))
-        cols["y"].append(abs(lumo - homo))
-        cols["pos"].append([float(x) for x in m.coords.reshape(-1)])
-        cols["iterations"].append(int(its[j]))
-        cols["converged"].append(bool(conv[j]))
-        cols["last5"].append([float(x) for x in l5])
+    """rows (dict of columns) of one finished batch; the per-molecule static columns come with
+    the items when the workers made them, else they are made here"""
+    n = len(items)
+    h = lambda x: x.cpu().numpy() if torch.is_tensor(x) else np.asarray(x)
+    E = h(res["energy"]) * HARTREE_TO_EV
+    mo = h(res["mo_energy"]).reshape(n, -1)
+    last5 = h(res["last5"]) * HARTREE_TO_EV
+    its = h(res["iterations"])
+    conv = h(res["converged"])
+    mols = [it[2] for it in items]
+    nocc = np.array([m.nelectron // 2 for m in mols], np.int64)
+    nao = np.array([m.nao for m in mols], np.int64)
+    r = np.arange(n)
+    homo = mo[r, nocc - 1] * HARTREE_TO_EV
+    lumo = np.where(nocc < nao, mo[r, np.minimum(nocc, mo.shape[1] - 1)] * HARTREE_TO_EV, np.nan)
+    fin = np.isfinite(last5)
+    cnt = fin.sum(1)
+    l5 = np.where(fin, last5, 0.0)
+    mean = l5.sum(1) / np.maximum(cnt, 1)
+    std = np.sqrt((np.where(fin, last5 - mean[:, None], 0.0) ** 2).sum(1) / np.maximum(cnt, 1))
+    std = np.where(cnt > 0, std, np.nan)
+    stat = [it[3] if len(it) > 3 else static_columns(it[0], it[2], seed) for it in items]
+    cols = {k: [st[k] for st in stat] for k in ("smile", "atoms", "z", "pos")}
+    cols.update({"energy": E.tolist(), "homo": homo.tolist(), "lumo": lumo.tolist(), "N": nao.tolist(),
+                 "std": std.tolist(), "y": np.abs(lumo - homo).tolist(), "iterations": its.astype(int).tolist(),
+                 "converged": conv.astype(bool).tolist(),
+                 "last5": [row[f].tolist() for row, f in zip(last5, fin)]})
     return cols
 
 
@@ -123,7 +150,7 @@ def run_stream(n_total, batch=4096, seed=0, level=0, precision="mixed", guess="l
     from .shard import shard_indices
     chunks = [(seed, s, min(batch, n_total - s), max_heavy) for s in shard_indices(n_total, batch, rank, world)]
     ctx = mp.get_context("spawn")
-    pool = ctx.Pool(workers)
+    pool = ctx.Pool(workers, initializer=_low_priority)
     ready = queue.Queue(maxsize=2)        # generated batches waiting for the GPU
     done = queue.Queue(maxsize=4)         # finished batches waiting for the writer
     writer = RowWriter(out, fmt)
@@ -134,24 +161,17 @@ def run_stream(n_total, batch=4096, seed=0, level=0, precision="mixed", guess="l
         # one batch split over every worker
         seed_, start, n, mh = c
         step = max(1, -(-n // workers))
-        return [pool.apply_async(stream_chunk, ((seed_, s0, min(step, start + n - s0), mh),))
+        return [pool.apply_async(prepare_chunk, ((seed_, s0, min(step, start + n - s0), mh),))
                 for s0 in range(start, start + n, step)]
-
-    dev = torch.cuda.current_device()
 
     def produce():
         try:
-            torch.cuda.set_device(dev)      # plans are built on this thread
-
             pending = [submit(c) for c in chunks[:2]]
             for k in range(len(chunks)):
                 parts = pending.pop(0)
                 if k + 2 < len(chunks):
                     pending.append(submit(chunks[k + 2]))
-                items = [x for p in parts for x in p.get()]
-                # the batch's plan (host tables, upload, device tables) is built here, off the
-                # GPU thread, while the previous batch runs
-                ready.put((items, Plan([m for _, _, m in items])))
+                ready.put([x for p in parts for x in p.get()])
         except Exception as e:          # surfaced by the main loop
             err.append(e)
         ready.put(None)
@@ -172,21 +192,25 @@ def run_stream(n_total, batch=4096, seed=0, level=0, precision="mixed", guess="l
     t0 = time.perf_counter()
     tp.start()
     tw.start()
-    try:
+    queued = collections.deque()          # items of the batches handed to run_batches, in order
+
+    def batches():
         while True:
-            got = ready.get()
-            if got is None or err:
-                break
-            items, plan = got
-            g0 = time.perf_counter()
-            eng = RKSEngine([m for _, _, m in items], level=level, precision=precision, guess=guess, net=net,
-                            plan=plan)
-            res = eng.run_converged(e_tol=e_tol, diis_tol=diis_tol)
-            res = {k: (v.clone() if torch.is_tensor(v) else v) for k, v in res.items()}
-            torch.cuda.synchronize()
-            eng.close()
-            stats["gpu_s"] += time.perf_counter() - g0
-            its = res["iterations"].cpu().numpy()
+            items = ready.get()
+            if items is None or err:
+                return
+            queued.append(items)
+            yield [it[2] for it in items]
+
+    try:
+        # run_batches builds each next plan on its worker thread once the current batch's ERI
+        # work is queued, and reuses the engine memory from batch to batch
+        for _, res in run_batches(batches(), level=level, precision=precision, guess=guess, net=net,
+                                  e_tol=e_tol, diis_tol=diis_tol):
+            items = queued.popleft()
+            h = res["host_ms"]
+            stats["gpu_s"] += 1e-3 * (h["engine"] + h["prepare"] + h["scf"])
+            its = res["iterations"]
             stats["iterations"].append(its)
             stats["converged"] += int((its > 0).sum())
             stats["batches"] += 1
