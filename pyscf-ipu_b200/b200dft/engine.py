@@ -574,13 +574,14 @@ def run_batches(batches, level=0, precision="mixed", guess="learned", net=None, 
             out = _run_one(mols, plan, level, precision, guess, net, run_kw, after_prepare=start)
             out["host_ms"]["plan_wait"] = wait_ms
             del plan                      # the engine and plan are released before the next batch
+            cur = None
+            # the result goes out before the next plan is awaited: the caller's handling of it
+            # overlaps the plan build, and a failing plan does not hold back a finished batch
+            yield mols, out
             tw = time.perf_counter()
-            if nxt is None:
-                cur = None
-            else:
+            if nxt is not None:
                 cur = fut[0].result() if fut else make(nxt)
             wait_ms = 1e3 * (time.perf_counter() - tw)
-            yield mols, out
     finally:
         if ex:
             ex.shutdown(wait=True)

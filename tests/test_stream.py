@@ -104,3 +104,64 @@ def test_run_batches_prefetch_matches_serial():
     E = eng.run_converged()["energy"].cpu().numpy()
     eng.close()
     np.testing.assert_allclose(pre[1][1]["energy"], E, rtol=0, atol=1e-9)
+
+
+def _fake_engine(monkeypatch, fail_at=None):
+    """run_batches with Plan and the per-batch SCF replaced by host stand-ins that record the
+    order of events (no GPU)"""
+    import threading
+    from b200dft import engine
+    log, lock = [], threading.Lock()
+
+    class FakePlan:
+        def __init__(self, mols):
+            if fail_at is not None and mols[0] == fail_at:
+                raise RuntimeError(f"plan {fail_at} failed")
+            with lock:
+                log.append(("plan", mols[0], threading.current_thread() is threading.main_thread()))
+            self.first = mols[0]
+
+    def fake_run_one(mols, plan, level, precision, guess, net, run_kw, after_prepare=None):
+        assert plan.first == mols[0]
+        with lock:
+            log.append(("prepare", mols[0]))
+        if after_prepare is not None:
+            after_prepare()
+        with lock:
+            log.append(("scf", mols[0]))
+        return {"energy": np.array([float(mols[0])]), "host_ms": {}, "kw": dict(run_kw)}
+
+    monkeypatch.setattr(engine, "Plan", FakePlan)
+    monkeypatch.setattr(engine, "_run_one", fake_run_one)
+    monkeypatch.setattr(torch.cuda, "current_device", lambda: 0)
+    monkeypatch.setattr(torch.cuda, "set_device", lambda d: None)
+    return engine, log
+
+
+@pytest.mark.parametrize("prefetch", [True, False])
+def test_run_batches_order_and_prefetch_points(monkeypatch, prefetch):
+    engine, log = _fake_engine(monkeypatch)
+    batches = [[k, k] for k in range(5)]
+    out = list(engine.run_batches(iter(batches), guess="minao", prefetch=prefetch, e_tol=1e-7))
+    assert [m for m, _ in out] == batches                       # in order, one result per batch
+    assert [float(r["energy"][0]) for _, r in out] == [0, 1, 2, 3, 4]
+    assert all(r["kw"] == {"e_tol": 1e-7} and "plan_wait" in r["host_ms"] for _, r in out)
+    plans = [e for e in log if e[0] == "plan"]
+    assert [e[1] for e in plans] == [0, 1, 2, 3, 4]
+    assert plans[0][2]                                          # the first plan is made in place
+    # with prefetch the later plans are made on the worker thread, each only after the previous
+    # batch's setup and ERI work was queued; without it every plan is made on the caller's thread
+    assert all(not e[2] for e in plans[1:]) if prefetch else all(e[2] for e in plans)
+    for k in range(1, 5):
+        assert log.index(("prepare", k - 1)) < log.index(plans[k])
+        assert log.index(plans[k]) < log.index(("prepare", k))
+
+
+def test_run_batches_empty_and_plan_errors(monkeypatch):
+    engine, _ = _fake_engine(monkeypatch, fail_at=2)
+    assert list(engine.run_batches(iter([]), guess="minao")) == []
+    got = []
+    with pytest.raises(RuntimeError, match="plan 2 failed"):
+        for mols, _ in engine.run_batches(iter([[0], [1], [2], [3]]), guess="minao"):
+            got.append(mols[0])
+    assert got == [0, 1]     # the batches before the failing plan are all delivered
