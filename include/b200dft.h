@@ -182,6 +182,21 @@ int b2_guess(b2_plan_t plan, double *D, void *stream);
 /* Nuclear repulsion per molecule (mol.energy_nuc(), dft.py:202); device float64 [nmol]. */
 int b2_enuc(b2_plan_t plan, double *enuc, void *stream);
 
+/* Nuclear gradient of converged SCFs, float64 (replaces grad(mol, coords, weight, mo_coeff,
+ * mo_energy) = grad_elec + grad_nuc, nanoDFT.py:403-477, with the grid held fixed as there).
+ * With C (device float64 matrices at the plan's matrix offsets, column k = orbital k) and
+ * mo_energy (device float64 nmol x 72), D and W (caller-owned device matrices) receive
+ * dm0 = 2 C_occ C_occ^T and dme0 = 2 C_occ eps_occ C_occ^T; with C NULL they are inputs.
+ * grad (device float64, 3 per atom, each molecule's atoms from its atom offset = the sum of
+ * natm of the molecules before it) is overwritten with the sum of the parts selected by
+ * `parts`: bit 0 one-electron (kinetic, nuclear attraction, -<dme0, dS>), bit 1 two-electron
+ * (Coulomb and hyb-scaled exchange), bit 2 exchange-correlation (B3LYP on coords / weights, the
+ * layout registered with b2_grid_set), bit 3 nuclear repulsion; 15 = the full gradient.
+ * hyb: exact-exchange fraction (0.2 for B3LYP). */
+int b2_grad(b2_plan_t plan, int parts, double hyb, const double *C, const double *mo_energy,
+            const double *coords, const double *weights, double *D, double *W, double *grad,
+            void *stream);
+
 /* Single-molecule convenience mirroring the reference's native entry int2e_sph
  * (int2e_sph.cpp:6750): host libcint arrays in, all s8 ERIs of the molecule out (device). */
 int b2_int2e_sph_s8(const int *atm, int natm, const int *bas, int nbas, const double *env,

@@ -55,6 +55,7 @@ SIGNATURES = {
     "b2_grid_build": [_P, _I, _P, _P, _P, _P, _P],
     "b2_guess": [_P, _P, _P],
     "b2_enuc": [_P, _P, _P],
+    "b2_grad": [_P, _I, _D, _P, _P, _P, _P, _P, _P, _P, _P],
 }
 
 

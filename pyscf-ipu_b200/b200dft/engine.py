@@ -500,6 +500,12 @@ class RKSEngine:
         self.xc(active=act)
         self.jk(active=act)
 
+    def gradient(self, parts=15, hyb=HYB_B3LYP, stream=None):
+        """Nuclear gradients [Ha/Bohr] of the converged molecules from the final orbitals, on the
+        engine's grid (``nuclear_gradient``): device float64 (sum of natm, 3)."""
+        return nuclear_gradient(self.plan, self.C, self.mo_energy, self.coords, self.weights, parts=parts,
+                                hyb=hyb, stream=stream)
+
     def kernels_launched(self, since):
         """library kernels executed since the launch_count() value ``since`` (graph replays included;
         the capture itself launches nothing)"""
@@ -507,6 +513,27 @@ class RKSEngine:
 
     def close(self):
         self.plan.close()
+
+
+def nuclear_gradient(plan, C, mo_energy, coords, weights, parts=15, hyb=HYB_B3LYP, stream=None, out_dm=None):
+    """Nuclear gradients [Ha/Bohr] of converged SCFs, float64 on the device (b2_grad): the
+    reference's grad = grad_elec + grad_nuc (nanoDFT.py:403-477) with the grid held fixed as
+    there.  C (column k = orbital k) and mo_energy (``NMO`` per molecule) are laid out by
+    ``plan``; coords / weights follow the grid registered with ``plan.set_grid``.  ``parts``
+    selects terms (1 one-electron, 2 two-electron, 4 exchange-correlation, 8 nuclear
+    repulsion).  Returns (sum of natm, 3), each molecule's atoms after those of the molecules
+    before it; ``out_dm`` (a list) receives the dm0 and dme0 device matrices."""
+    dev = C.device
+    f64 = dict(dtype=torch.float64, device=dev)
+    n_atm = sum(m.natm for m in plan.mols)
+    D = torch.empty(max(1, plan.n_mat), **f64)
+    W = torch.empty(max(1, plan.n_mat), **f64)
+    g = torch.empty((max(1, n_atm), 3), **f64)
+    check(lib().b2_grad(plan.h, int(parts), float(hyb), ptr(C), ptr(mo_energy), ptr(coords), ptr(weights),
+                        ptr(D), ptr(W), ptr(g), stream_handle(stream)), "b2_grad")
+    if out_dm is not None:
+        out_dm.extend([D, W])
+    return g[:n_atm]
 
 
 def _run_one(mols, plan, level, precision, guess, net, run_kw, after_prepare=None):

@@ -14,7 +14,7 @@ from .mole import Mole, build_mol, methane
 from .grids import Grids
 from .engine import RKSEngine, HostSetup
 
-__all__ = ["nanoDFT", "nanoDFT_options", "build_mol", "energy", "hlgap", "process_mol_str"]
+__all__ = ["nanoDFT", "nanoDFT_options", "build_mol", "energy", "hlgap", "process_mol_str", "grad"]
 
 NAMED = {
     "methane": methane(),
@@ -94,6 +94,28 @@ def nanoDFT(mol, opts):
     mo_coeff = res["C"][:N * N].reshape(N, N)
     energies, logged, hlgaps = [a * HARTREE_TO_EV for a in (energies, logged, hlgaps)]
     return energies, (logged, hlgaps, mo_energy, mo_coeff, setup.coords, setup.weights)
+
+
+def grad(mol, coords, weight, mo_coeff, mo_energy):
+    """Nuclear gradient [Ha/Bohr], (natm, 3), of a converged SCF from its orbitals (mo_coeff,
+    column k = orbital k, ascending mo_energy) on its grid (coords, weight): drop-in for
+    nanoDFT.grad (nanoDFT.py:440-477; grad_elec + grad_nuc, no grid response).  Every term is
+    evaluated on the B200 (b2_grad)."""
+    import torch
+    from .engine import NMO, Plan, _require_cuda, nuclear_gradient
+    _require_cuda()
+    N = mol.nao
+    dev = torch.device("cuda")
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a, np.float64).reshape(-1)).to(dev)
+    plan = Plan([mol])
+    try:
+        plan.set_grid([len(weight)])
+        eps = torch.zeros(NMO, dtype=torch.float64, device=dev)
+        eps[:N] = t(np.asarray(mo_energy)[:N])
+        g = nuclear_gradient(plan, t(np.asarray(mo_coeff)[:N, :N]), eps, t(coords), t(weight))
+        return g.cpu().numpy().reshape(mol.natm, 3)
+    finally:
+        plan.close()
 
 
 def main(argv=None):

@@ -488,4 +488,12 @@ int b2_enuc(void *plan, double *enuc, void *stream) {
   return b2_launch_enuc(*(B2PlanDev *)plan, enuc, (cudaStream_t)stream);
 }
 
+int b2_grad(void *plan, int parts, double hyb, const double *C, const double *mo_energy, const double *coords,
+            const double *weights, double *D, double *W, double *grad, void *stream) {
+  if (!plan) return B2_ERR_ARG;
+  B2PlanDev *P = (B2PlanDev *)plan;
+  if (P->h.max_natm > B2_MAXNAO) return B2_ERR_SIZE;
+  return b2_launch_grad(*P, parts, hyb, C, mo_energy, coords, weights, D, W, grad, (cudaStream_t)stream);
+}
+
 }  // extern "C"

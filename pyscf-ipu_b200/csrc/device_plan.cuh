@@ -69,6 +69,12 @@ struct B2PlanDev {
 };
 
 int b2_launch_eri_s8(B2PlanDev &P, int precision, void *out, cudaStream_t st);
+// the ERI work list of `precision` (32: canonical shell quartets grouped by class combination,
+// up to 32 kets per task; 64: p-shell bras split by component), built once per plan
+int b2_eri_tasks_ready(B2PlanDev &P, int precision, cudaStream_t st);
+int b2_launch_grad(B2PlanDev &P, int parts, double hyb, const double *C, const double *mo_energy,
+                   const double *coords, const double *weights, double *D, double *W, double *grad,
+                   cudaStream_t st);
 int b2_build_pairs(B2PlanDev &P, cudaStream_t st);
 int b2_launch_exch_build(const B2PlanDev &P, int precision, const void *eri, void *exch, cudaStream_t st);
 int b2_launch_jk_symv(const B2PlanDev &P, int precision, const int *active, const void *eri,

@@ -385,6 +385,11 @@ static int b2_eri_task_upload(B2PlanDev &P, int precision, cudaStream_t st) {
   return B2_OK;
 }
 
+int b2_eri_tasks_ready(B2PlanDev &P, int precision, cudaStream_t st) {
+  if (precision != 64 && precision != 32) return B2_ERR_ARG;
+  return b2_eri_task_upload(P, precision, st);
+}
+
 int b2_launch_eri_s8(B2PlanDev &P, int precision, void *out, cudaStream_t st) {
   if (precision != 64 && precision != 32) return B2_ERR_ARG;
   int rc = b2_eri_task_upload(P, precision, st);

@@ -24,8 +24,8 @@
 #define B2G_NC 20                  // Cartesian components of l = 0..3
 #define B2G_MMAX 6                 // Boys orders 0..5
 
-B2_HD int b2g_cstart(int l) { return l * (l + 1) * (l + 2) / 6; }
-B2_HD int b2g_ncart(int l) { return (l + 1) * (l + 2) * (l + 3) / 6; }   // components of 0..l
+B2_HD constexpr int b2g_cstart(int l) { return l * (l + 1) * (l + 2) / 6; }
+B2_HD constexpr int b2g_ncart(int l) { return (l + 1) * (l + 2) * (l + 3) / 6; }   // components of 0..l
 // index of the Cartesian (x, y, z) among all components of l = 0..3 (order within a shell:
 // x descending, then y descending)
 B2_HD int b2g_cidx(int x, int y, int z) {
@@ -60,14 +60,17 @@ B2_HD void b2g_boys(int L, T t, const T *btab, T *F) {
   }
 }
 
-// contracted [e 0 | f 0] for e over l <= le, f over l <= lf, with four weightings:
-// w = 0: plain, 1: x 2 alpha (first bra primitive), 2: x 2 beta (second bra), 3: x 2 gamma
-// (first ket).  Shells a, b, c, d (their coefficients include the angular factors).
-template <typename T>
-B2_HD void b2g_e0f0(const B2Shell &a, const B2Shell &b, const B2Shell &c, const B2Shell &d, int le, int lf,
-                    const T *btab, T (*acc)[B2G_NC][B2G_NC]) {
-  const int ne = b2g_ncart(le), nf = b2g_ncart(lf), L = le + lf;
-  for (int w = 0; w < 4; ++w)
+// contracted [e 0 | f 0] for e over l <= LE, f over l <= LF, with the weightings of the bra
+// pass (KET false; w = 0: plain, 1: x 2 alpha of the first bra primitive, 2: x 2 beta of the
+// second) or of the ket pass (KET true; w = 0: plain, 1: x 2 gamma of the first ket
+// primitive).  Shells a, b, c, d (their coefficients include the angular factors).  The
+// array sizes follow the class, so a GPU thread holds no more than the class needs.
+template <typename T, int LE, int LF, bool KET>
+B2_HD void b2g_e0f0(const B2Shell &a, const B2Shell &b, const B2Shell &c, const B2Shell &d,
+                    const T *btab, T (*acc)[b2g_ncart(LE)][b2g_ncart(LF)]) {
+  constexpr int ne = b2g_ncart(LE), nf = b2g_ncart(LF), L = LE + LF, NW = KET ? 2 : 3;
+  const int le = LE, lf = LF;
+  for (int w = 0; w < NW; ++w)
     for (int i = 0; i < ne; ++i)
       for (int j = 0; j < nf; ++j) acc[w][i][j] = (T)0;
   T AB2 = 0, CD2 = 0;
@@ -102,7 +105,7 @@ B2_HD void b2g_e0f0(const B2Shell &a, const B2Shell &b, const B2Shell &c, const 
           const T pref = (T)34.98683665524972 / (z * e * sqrt(z + e)) * Kab * Kcd;
           T F[B2G_MMAX];
           b2g_boys<T>(L, rho * PQ2, btab, F);
-          T v[B2G_NC][B2G_NC][B2G_MMAX];
+          T v[ne][nf][L + 1];
           for (int m = 0; m <= L; ++m) v[0][0][m] = pref * F[m];
           for (int l1 = 1; l1 <= le; ++l1)                // bra vertical recursion
             for (int ie = b2g_cstart(l1); ie < b2g_cstart(l1 + 1); ++ie) {
@@ -157,8 +160,8 @@ B2_HD void b2g_e0f0(const B2Shell &a, const B2Shell &b, const B2Shell &c, const 
                 }
               }
             }
-          const T wt[4] = {(T)1, 2 * al, 2 * be, 2 * ga};
-          for (int w = 0; w < 4; ++w)
+          const T wt[3] = {(T)1, KET ? 2 * ga : 2 * al, 2 * be};
+          for (int w = 0; w < NW; ++w)
             for (int i = 0; i < ne; ++i)
               for (int j = 0; j < nf; ++j) acc[w][i][j] += wt[w] * v[i][j][0];
         }
@@ -167,8 +170,8 @@ B2_HD void b2g_e0f0(const B2Shell &a, const B2Shell &b, const B2Shell &c, const 
 
 // (a b | c d) over Cartesian exponent triplets (a, b on the bra centres A, B; c, d on C, D) from
 // contracted [e 0 | f 0] (weighting w): horizontal recursion (a b+1_x| = (a+1_x b| + AB_x (a b|
-template <typename T>
-B2_HD T b2g_hrr(const T (*acc)[B2G_NC][B2G_NC], int w, const int *ea, const int *eb, const int *ec, const int *ed,
+template <typename T, int NE, int NF>
+B2_HD T b2g_hrr(const T (*acc)[NE][NF], int w, const int *ea, const int *eb, const int *ec, const int *ed,
                 const T *AB, const T *CD) {
   // expand b onto a: sum over binomial terms of (a + b')|, with weight AB^(b - b')
   T s = 0;
@@ -196,17 +199,17 @@ B2_HD void b2g_comp(int l, int k, int *e) {
   if (l) e[k] = 1;
 }
 
-// Gradient contributions of the shell quartet (a b | c d) contracted with gam[ia][ib][ic][id]
-// (component order of each shell, flattened): g[s][x] = sum gam d(ab|cd)/dR_x of the centre of
-// shell s (s = 0..3; the fourth from translation invariance).
-template <typename T>
-B2_HD void b2g_quartet_grad(const B2Shell &a, const B2Shell &b, const B2Shell &c, const B2Shell &d,
-                            const T *btab, const T *gam, T g[4][3]) {
-  const int la = a.l, lb = b.l, lc = c.l, ld = d.l;
-  const int na = 2 * la + 1, nb = 2 * lb + 1, nc = 2 * lc + 1, nd = 2 * ld + 1;
-  T accB[4][B2G_NC][B2G_NC], accK[4][B2G_NC][B2G_NC];
-  b2g_e0f0<T>(a, b, c, d, la + lb + 1, lc + ld, btab, accB);   // bra raised by one (dA, dB)
-  b2g_e0f0<T>(a, b, c, d, la + lb, lc + ld + 1, btab, accK);   // ket raised by one (dC)
+// Gradient contributions of the shell quartet (a b | c d) of class (LA LB | LC LD) contracted
+// with gam[ia][ib][ic][id] (component order of each shell, flattened): g[s][x] = sum gam
+// d(ab|cd)/dR_x of the centre of shell s (s = 0..3; the fourth from translation invariance).
+template <typename T, int LA, int LB, int LC, int LD>
+B2_HD void b2g_quartet_grad_t(const B2Shell &a, const B2Shell &b, const B2Shell &c, const B2Shell &d,
+                              const T *btab, const T *gam, T g[4][3]) {
+  constexpr int na = 2 * LA + 1, nb = 2 * LB + 1, nc = 2 * LC + 1, nd = 2 * LD + 1;
+  constexpr int LEB = LA + LB + 1, LFB = LC + LD, LEK = LA + LB, LFK = LC + LD + 1;
+  T accB[3][b2g_ncart(LEB)][b2g_ncart(LFB)], accK[2][b2g_ncart(LEK)][b2g_ncart(LFK)];
+  b2g_e0f0<T, LEB, LFB, false>(a, b, c, d, btab, accB);   // bra raised by one (dA, dB)
+  b2g_e0f0<T, LEK, LFK, true>(a, b, c, d, btab, accK);    // ket raised by one (dC)
   T AB[3], CD[3];
   for (int x = 0; x < 3; ++x) {
     AB[x] = (T)(a.R[x] - b.R[x]);
@@ -220,27 +223,72 @@ B2_HD void b2g_quartet_grad(const B2Shell &a, const B2Shell &b, const B2Shell &c
           const T gm = gam[((ia * nb + ib) * nc + ic) * nd + id];
           if (gm == (T)0) continue;
           int ea[3], eb[3], ec[3], ed[3];
-          b2g_comp(la, ia, ea); b2g_comp(lb, ib, eb); b2g_comp(lc, ic, ec); b2g_comp(ld, id, ed);
+          b2g_comp(LA, ia, ea); b2g_comp(LB, ib, eb); b2g_comp(LC, ic, ec); b2g_comp(LD, id, ed);
           for (int x = 0; x < 3; ++x) {
             int up[3], dn[3];
             // d/dA_x: 2 alpha (a+1x b| - a_x (a-1x b|
             for (int k = 0; k < 3; ++k) { up[k] = ea[k] + (k == x); dn[k] = ea[k] - (k == x); }
-            T dA = b2g_hrr<T>(accB, 1, up, eb, ec, ed, AB, CD);
-            if (ea[x]) dA -= (T)ea[x] * b2g_hrr<T>(accB, 0, dn, eb, ec, ed, AB, CD);
+            T dA = b2g_hrr(accB, 1, up, eb, ec, ed, AB, CD);
+            if (ea[x]) dA -= (T)ea[x] * b2g_hrr(accB, 0, dn, eb, ec, ed, AB, CD);
             // d/dB_x: 2 beta (a b+1x| - b_x (a b-1x|
             for (int k = 0; k < 3; ++k) { up[k] = eb[k] + (k == x); dn[k] = eb[k] - (k == x); }
-            T dB = b2g_hrr<T>(accB, 2, ea, up, ec, ed, AB, CD);
-            if (eb[x]) dB -= (T)eb[x] * b2g_hrr<T>(accB, 0, ea, dn, ec, ed, AB, CD);
+            T dB = b2g_hrr(accB, 2, ea, up, ec, ed, AB, CD);
+            if (eb[x]) dB -= (T)eb[x] * b2g_hrr(accB, 0, ea, dn, ec, ed, AB, CD);
             // d/dC_x: 2 gamma (ab|c+1x d) - c_x (ab|c-1x d)
             for (int k = 0; k < 3; ++k) { up[k] = ec[k] + (k == x); dn[k] = ec[k] - (k == x); }
-            T dC = b2g_hrr<T>(accK, 3, ea, eb, up, ed, AB, CD);
-            if (ec[x]) dC -= (T)ec[x] * b2g_hrr<T>(accK, 0, ea, eb, dn, ed, AB, CD);
+            T dC = b2g_hrr(accK, 1, ea, eb, up, ed, AB, CD);
+            if (ec[x]) dC -= (T)ec[x] * b2g_hrr(accK, 0, ea, eb, dn, ed, AB, CD);
             g[0][x] += gm * dA;
             g[1][x] += gm * dB;
             g[2][x] += gm * dC;
           }
         }
   for (int x = 0; x < 3; ++x) g[3][x] = -(g[0][x] + g[1][x] + g[2][x]);
+}
+
+// the same for shells of any class (l <= 1), dispatched at run time
+template <typename T>
+B2_HD void b2g_quartet_grad(const B2Shell &a, const B2Shell &b, const B2Shell &c, const B2Shell &d,
+                            const T *btab, const T *gam, T g[4][3]) {
+  switch (a.l * 8 + b.l * 4 + c.l * 2 + d.l) {
+#define B2G_Q(A, B, C, D) case A * 8 + B * 4 + C * 2 + D: b2g_quartet_grad_t<T, A, B, C, D>(a, b, c, d, btab, gam, g); break;
+    B2G_Q(0, 0, 0, 0) B2G_Q(0, 0, 0, 1) B2G_Q(0, 0, 1, 0) B2G_Q(0, 0, 1, 1)
+    B2G_Q(0, 1, 0, 0) B2G_Q(0, 1, 0, 1) B2G_Q(0, 1, 1, 0) B2G_Q(0, 1, 1, 1)
+    B2G_Q(1, 0, 0, 0) B2G_Q(1, 0, 0, 1) B2G_Q(1, 0, 1, 0) B2G_Q(1, 0, 1, 1)
+    B2G_Q(1, 1, 0, 0) B2G_Q(1, 1, 0, 1) B2G_Q(1, 1, 1, 0) B2G_Q(1, 1, 1, 1)
+#undef B2G_Q
+    default: break;
+  }
+}
+
+// Work-list group g = bra class * 4 + ket class (class = l_first + 2 l_second) to the shells'
+// angular momenta: k = 0..3 gives l of I, J, K, L.
+B2_HD constexpr int b2g_group_l(int g, int k) {
+  return k == 0 ? (g >> 2) & 1 : k == 1 ? (g >> 3) & 1 : k == 2 ? g & 1 : (g >> 1) & 1;
+}
+
+// One canonical shell quartet (a b | c d) (pair index IJ >= KL, I >= J, K >= L) of a molecule
+// with density Dm (N x N): summed over all ordered index quartets, dE_2e/dR = sum d(ij|kl)/dR
+// Gamma_ijkl, Gamma = 1/2 D_ij D_kl - hyb/4 D_il D_jk; over the eight orderings of a quartet
+// that is the symmetrised Gamma = 1/2 D_ij D_kl - hyb/8 (D_il D_jk + D_ik D_jl) times the number
+// of distinct shell orderings (2 for I != J, 2 for K != L, 2 for IJ != KL).
+template <int LA, int LB, int LC, int LD>
+B2_HD void b2g_canonical_quartet(const B2Shell &a, const B2Shell &b, const B2Shell &c, const B2Shell &d,
+                                 bool ij_same, bool kl_same, bool braket_same, const double *Dm, int N,
+                                 double hyb, const double *btab, double g4[4][3]) {
+  constexpr int na = 2 * LA + 1, nb = 2 * LB + 1, nc = 2 * LC + 1, nd = 2 * LD + 1;
+  const double deg = (ij_same ? 1.0 : 2.0) * (kl_same ? 1.0 : 2.0) * (braket_same ? 1.0 : 2.0);
+  double gam[na * nb * nc * nd];
+  for (int ia = 0; ia < na; ++ia)
+    for (int ib = 0; ib < nb; ++ib)
+      for (int ic = 0; ic < nc; ++ic)
+        for (int id = 0; id < nd; ++id) {
+          const int i = a.ao0 + ia, j = b.ao0 + ib, k = c.ao0 + ic, l = d.ao0 + id;
+          gam[((ia * nb + ib) * nc + ic) * nd + id] =
+              deg * (0.5 * Dm[i * N + j] * Dm[k * N + l] -
+                     0.125 * hyb * (Dm[i * N + l] * Dm[j * N + k] + Dm[i * N + k] * Dm[j * N + l]));
+        }
+  b2g_quartet_grad_t<double, LA, LB, LC, LD>(a, b, c, d, btab, gam, g4);
 }
 
 // ---------------------------------------------------------------- one-electron part
@@ -262,11 +310,12 @@ B2_HD void b2g_ovl1d(T PA, T PB, T oz, int ni, int nj, T s[3][5]) {
                                          (j > 1 ? (T)(j - 1) * s[i][j - 2] : (T)0));
 }
 
-// g[0], g[1]: gradient on the centres of a and b; gC[atom] (natm x 3): on the nuclei.
+// g[0], g[1]: gradient on the centres of a and b; the terms on the nuclei go to addC(atom, x,
+// value) (the caller's accumulator: a plain sum on the host, atomics on the GPU).
 // D and W are the molecule's nao x nao matrices (row-major, stride N); Z / RC the nuclei.
-template <typename T>
+template <typename T, typename AddC>
 B2_HD void b2g_pair_grad_1e(const B2Shell &a, const B2Shell &b, const T *D, const T *Wm, int N, int natm,
-                            const T *Z, const T *RC, const T *btab, T g[2][3], T *gC) {
+                            const T *Z, const T *RC, const T *btab, T g[2][3], AddC &&addC) {
   const int la = a.l, lb = b.l, na = 2 * la + 1, nb = 2 * lb + 1;
   T AB[3], AB2 = 0;
   for (int x = 0; x < 3; ++x) { AB[x] = (T)(a.R[x] - b.R[x]); AB2 += AB[x] * AB[x]; }
@@ -377,7 +426,7 @@ B2_HD void b2g_pair_grad_1e(const B2Shell &a, const B2Shell &b, const T *D, cons
               if (eb[x]) dB -= (T)eb[x] * V3(ea, db);
               g[0][x] += dij * dA;
               g[1][x] += dij * dB;
-              gC[3 * c + x] -= dij * (dA + dB);
+              addC(c, x, -dij * (dA + dB));
             }
           }
       }

@@ -8,6 +8,37 @@
 #include "xc_math.cuh"
 #include <vector>
 
+// The two-electron gradient kernel's traversal on the host: the float32 ERI work list (32 kets
+// per task, grouped by class combination), canonical quartets only, each lane's quartet through
+// b2g_canonical_quartet with the class its group fixes.  bad counts quartets whose shells do not
+// have the group's angular momenta.
+template <int G>
+static void b2hc_2e_group(const B2PlanHost &P, const std::vector<B2EriTask> &tasks, const std::vector<long long> &goff,
+                          const double *D, double hyb, const double *tab, double *g, int *bad) {
+  for (long long t = goff[G]; t < goff[G + 1]; ++t) {
+    const B2EriTask &tk = tasks[t];
+    const B2MolDev &md = P.mols[tk.mol];
+    const B2PairInfo &bp = P.pinfo[md.sp_off + tk.IJ];
+    const B2Shell *S = &P.shells[md.sh_off];
+    for (int lane = 0; lane < 32; ++lane) {
+      if (lane >= tk.count) continue;
+      const int KL = P.cls_list[md.sp_off + md.cls_start[tk.cls] + tk.start + lane];
+      if (KL > tk.IJ) continue;
+      const B2PairInfo &kp = P.pinfo[md.sp_off + KL];
+      const B2Shell *q[4] = {&S[bp.I], &S[bp.J], &S[kp.I], &S[kp.J]};
+      for (int k = 0; k < 4; ++k)
+        if (q[k]->l != b2g_group_l(G, k)) ++*bad;
+      double g4[4][3];
+      b2g_canonical_quartet<b2g_group_l(G, 0), b2g_group_l(G, 1), b2g_group_l(G, 2), b2g_group_l(G, 3)>(
+          *q[0], *q[1], *q[2], *q[3], bp.I == bp.J, kp.I == kp.J, KL == tk.IJ, D + md.mat_off, md.nao, hyb,
+          tab, g4);
+      for (int s = 0; s < 4; ++s)
+        for (int x = 0; x < 3; ++x) g[3 * (md.atm_off + q[s]->atom) + x] += g4[s][x];
+    }
+  }
+  if constexpr (G < 15) b2hc_2e_group<G + 1>(P, tasks, goff, D, hyb, tab, g, bad);
+}
+
 extern "C" {
 
 int b2hc_boys(int L, double t, double *F) {
@@ -127,6 +158,25 @@ int b2hc_grad_2e(int natm, int nbas, const int *atm, const int *bas, const doubl
   return 0;
 }
 
+// two-electron gradient of a batch (D: the molecules' matrices back to back, nao x nao each;
+// g: 3 per atom, molecules back to back) by the GPU kernel's traversal
+int b2hc_grad_2e_tasks(int nmol, const int *natm, const int *nbas, const int *atm, const int *bas,
+                       const double *env, const long long *env_off, const double *D, double hyb, double *g,
+                       int *bad) {
+  B2PlanHost P;
+  int rc = b2_plan_build(P, nmol, natm, nbas, atm, bas, env, env_off);
+  if (rc) return rc;
+  std::vector<double> tab(B2_BOYS_NT * B2_BOYS_NM);
+  b2_boys_fill_table(tab.data());
+  std::vector<B2EriTask> tasks;
+  std::vector<long long> goff;
+  b2_eri_tasks(P, 32, false, tasks, &goff);
+  for (int i = 0; i < 3 * P.n_atm; ++i) g[i] = 0;
+  *bad = 0;
+  b2hc_2e_group<0>(P, tasks, goff, D, hyb, tab.data(), g, bad);
+  return 0;
+}
+
 // one-electron gradient of one molecule at fixed D and W (nao x nao): g[natm][3] = d/dR of
 // <D, T + V_nuc> - <W, S> (nuclear repulsion not included)
 int b2hc_grad_1e(int natm, int nbas, const int *atm, const int *bas, const double *env, const double *D,
@@ -148,7 +198,8 @@ int b2hc_grad_1e(int natm, int nbas, const int *atm, const int *bas, const doubl
   for (int I = 0; I < nbas; ++I)
     for (int J = 0; J < nbas; ++J) {
       double g2[2][3];
-      b2g_pair_grad_1e<double>(S[I], S[J], D, W, N, natm, Z.data(), RC.data(), tab.data(), g2, g);
+      b2g_pair_grad_1e<double>(S[I], S[J], D, W, N, natm, Z.data(), RC.data(), tab.data(), g2,
+                               [&](int c, int x, double v) { g[3 * c + x] += v; });
       for (int x = 0; x < 3; ++x) {
         g[3 * S[I].atom + x] += g2[0][x];
         g[3 * S[J].atom + x] += g2[1][x];

@@ -1,0 +1,87 @@
+"""Nuclear gradients on the B200 (b2_grad): every kernel against the host build of the same
+math on the same densities, batched over uneven molecules, and the nanoDFT.grad drop-in against
+the gradient oracle."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from b200dft.mole import Mole, methane
+
+pytestmark = pytest.mark.gpu
+
+HYB = 0.2
+
+
+def _mols():
+    return [Mole("O 0 0 0.1173; H 0 0.7572 -0.4692; H 0 -0.7532 -0.4792"), Mole(methane(1.05)),
+            Mole("N 0 0 0; C 0 0 2.6; O 2.1 0 3.9; H 0 1.9 -0.8", unit="Bohr")]
+
+
+def _host_parts(hc, mol, D, W, coords, w):
+    """one-electron, two-electron, exchange-correlation and nuclear parts by the host build"""
+    from test_hostcheck import _p
+    atm = np.ascontiguousarray(mol._atm, np.int32)
+    bas = np.ascontiguousarray(mol._bas, np.int32)
+    env = np.ascontiguousarray(mol._env, np.float64)
+    args = (mol.natm, len(bas), _p(atm, ctypes.c_int), _p(bas, ctypes.c_int), _p(env, ctypes.c_double))
+    D, W = np.ascontiguousarray(D), np.ascontiguousarray(W)
+    coords, w = np.ascontiguousarray(coords), np.ascontiguousarray(w)
+    g1, g2, gx = (np.zeros((mol.natm, 3)) for _ in range(3))
+    assert hc.b2hc_grad_1e(*args, _p(D, ctypes.c_double), _p(W, ctypes.c_double), _p(g1, ctypes.c_double)) == 0
+    assert hc.b2hc_grad_2e(*args, _p(D, ctypes.c_double), ctypes.c_double(HYB), _p(g2, ctypes.c_double)) == 0
+    assert hc.b2hc_grad_xc(*args, _p(D, ctypes.c_double), ctypes.c_longlong(len(w)), _p(coords, ctypes.c_double),
+                           _p(w, ctypes.c_double), _p(gx, ctypes.c_double)) == 0
+    Z = mol.charges.astype(np.float64)
+    dR = mol.coords[:, None, :] - mol.coords[None, :, :]
+    dist = np.linalg.norm(dR, axis=2)
+    np.fill_diagonal(dist, np.inf)
+    gn = -(Z[:, None, None] * Z[None, :, None] * dR / dist[:, :, None] ** 3).sum(1)
+    return {1: g1, 2: g2, 4: gx, 8: gn}
+
+
+def test_gradient_kernels_match_host_math_batched():
+    from test_hostcheck import _hc
+    from b200dft.engine import RKSEngine, nuclear_gradient
+    mols = _mols()
+    eng = RKSEngine(mols, precision="fp64", guess="minao")
+    try:
+        r = eng.run_converged()
+        assert bool(r["converged"].all())
+        dm = []
+        full = nuclear_gradient(eng.plan, eng.C, eng.mo_energy, eng.coords, eng.weights, parts=15,
+                                hyb=HYB, out_dm=dm).cpu().numpy()
+        parts = {p: eng.gradient(parts=p, hyb=HYB).cpu().numpy() for p in (1, 2, 4, 8)}
+        P = eng.plan
+        D, W = (x.cpu().numpy() for x in dm)
+        # dm0 from the final orbitals is the final density of the SCF
+        np.testing.assert_allclose(D[:P.n_mat], eng.D.cpu().numpy(), atol=1e-12, rtol=0)
+        coords = eng.coords.cpu().numpy().reshape(-1, 3)
+        w = eng.weights.cpu().numpy()
+    finally:
+        eng.close()
+    np.testing.assert_allclose(sum(parts.values()), full, atol=1e-10, rtol=0)
+    hc = _hc()
+    a0 = 0
+    for m, mol in enumerate(mols):
+        g0, g1 = P.grid_off[m], P.grid_off[m + 1]
+        ref = _host_parts(hc, mol, P.unpack(D, m), P.unpack(W, m), coords[g0:g1], w[g0:g1])
+        for p, gr in ref.items():
+            got = parts[p][a0:a0 + mol.natm]
+            np.testing.assert_allclose(got, gr, atol=1e-9 * max(1.0, np.abs(gr).max()), rtol=0,
+                                       err_msg=f"molecule {m} part {p}")
+        assert np.abs(full[a0:a0 + mol.natm].sum(0)).max() < 1e-5    # near translation invariance
+        a0 += mol.natm
+
+
+def test_nanodft_grad_drop_in_matches_oracle():
+    """nanoDFT(mol, opts) then grad(mol, coords, weight, mo_coeff, mo_energy) (nanoDFT.py:636)"""
+    from oracle import grad as ograd
+    from b200dft.nanodft import grad, nanoDFT, nanoDFT_options
+    mol = _mols()[0]
+    opts, _ = nanoDFT_options(its=30, mol_str="water")
+    _, (_, _, mo_energy, mo_coeff, coords, weights) = nanoDFT(mol, opts)
+    g = grad(mol, coords, weights, mo_coeff, mo_energy)
+    ref = ograd.gradient(mol, mo_coeff, mo_energy, coords, weights)
+    assert np.abs(ref).max() > 1e-2
+    np.testing.assert_allclose(g, ref, atol=1e-6, rtol=0)     # oracle truncation ~1e-8

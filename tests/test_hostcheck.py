@@ -139,6 +139,45 @@ def test_two_electron_gradient_vs_finite_differences():
         np.testing.assert_allclose(g.sum(0), 0.0, atol=1e-9)    # translation invariance (exact)
 
 
+def test_two_electron_gradient_kernel_traversal():
+    """the GPU kernel's traversal of the two-electron gradient (canonical shell quartets of the
+    float32 ERI work list, degeneracy weights, symmetrised Gamma, class fixed by the task group;
+    the same lane code as k_grad_2e) equals the sum over all ordered quartets, molecule by
+    molecule in a batch"""
+    hc = _hc()
+    mols = [Mole("O 0 0 0.1173; H 0 0.7572 -0.4692; H 0 -0.7532 -0.4792"), Mole(methane(1.05)),
+            Mole("N 0 0 0; C 0 0 2.6; O 2.1 0 3.9; H 0 1.9 -0.8", unit="Bohr")]
+    rng = np.random.default_rng(7)
+    Ds, hyb = [], 0.2
+    for m in mols:
+        X = rng.normal(size=(m.nao, m.nao)) * 0.3
+        Ds.append(np.ascontiguousarray(X + X.T))
+    atm = np.ascontiguousarray(np.concatenate([m._atm for m in mols]), np.int32)
+    bas = np.ascontiguousarray(np.concatenate([m._bas for m in mols]), np.int32)
+    env = np.concatenate([m._env for m in mols])
+    eo = np.cumsum([0] + [len(m._env) for m in mols[:-1]]).astype(np.int64)
+    natm = np.array([m.natm for m in mols], np.int32)
+    nbas = np.array([m.nbas for m in mols], np.int32)
+    Dp = np.ascontiguousarray(np.concatenate([D.reshape(-1) for D in Ds]))
+    g = np.full((int(natm.sum()), 3), np.nan)
+    bad = ctypes.c_int(-1)
+    rc = hc.b2hc_grad_2e_tasks(len(mols), _p(natm, ctypes.c_int), _p(nbas, ctypes.c_int), _p(atm, ctypes.c_int),
+                               _p(bas, ctypes.c_int), _p(env, ctypes.c_double), _p(eo, ctypes.c_longlong),
+                               _p(Dp, ctypes.c_double), ctypes.c_double(hyb), _p(g, ctypes.c_double),
+                               ctypes.byref(bad))
+    assert rc == 0 and bad.value == 0
+    a0 = 0
+    for m, D in zip(mols, Ds):
+        ref = np.zeros((m.natm, 3))
+        ma = np.ascontiguousarray(m._atm, np.int32)
+        mb = np.ascontiguousarray(m._bas, np.int32)
+        me = np.ascontiguousarray(m._env, np.float64)
+        assert hc.b2hc_grad_2e(m.natm, len(mb), _p(ma, ctypes.c_int), _p(mb, ctypes.c_int), _p(me, ctypes.c_double),
+                               _p(D, ctypes.c_double), ctypes.c_double(hyb), _p(ref, ctypes.c_double)) == 0
+        np.testing.assert_allclose(g[a0:a0 + m.natm], ref, atol=1e-10 * max(1.0, np.abs(ref).max()), rtol=0)
+        a0 += m.natm
+
+
 def test_one_electron_gradient_vs_finite_differences():
     """the one-electron gradient math (host build) against central differences of
     <D, T + V_nuc> - <W, S> at fixed D and W, with the host 1e integrals at displaced geometries"""
@@ -220,7 +259,8 @@ def test_gradient_math_compiles_for_sm100a(tmp_path):
         "                  const double *W, const double *Z, const double *RC, const double *r, double *o) {\n"
         "  double g4[4][3], g2[2][3], f[3], df[3][3], hf[3][6];\n"
         "  b2g_quartet_grad<double>(s[0], s[1], s[2], s[3], t, gam, g4);\n"
-        "  b2g_pair_grad_1e<double>(s[0], s[1], D, W, 9, 5, Z, RC, t, g2, o);\n"
+        "  b2g_pair_grad_1e<double>(s[0], s[1], D, W, 9, 5, Z, RC, t, g2,\n"
+        "                           [&](int c, int x, double v) { atomicAdd(o + 3 * c + x, v); });\n"
         "  b2g_ao2<double>(s[0], r, f, df, hf);\n"
         "  o[0] += g4[0][0] + g2[0][0] + f[0] + df[0][0] + hf[0][0];\n"
         "}\n")
