@@ -70,7 +70,10 @@ def test_gradient_kernels_match_host_math_batched():
             got = parts[p][a0:a0 + mol.natm]
             np.testing.assert_allclose(got, gr, atol=1e-9 * max(1.0, np.abs(gr).max()), rtol=0,
                                        err_msg=f"molecule {m} part {p}")
-        assert np.abs(full[a0:a0 + mol.natm].sum(0)).max() < 1e-5    # near translation invariance
+        # translation invariance holds for the integral terms; the XC term is taken on a grid that
+        # does not move with the atoms (no grid response, as in the reference), so it breaks it
+        analytic = sum(parts[p][a0:a0 + mol.natm] for p in (1, 2, 8))
+        assert np.abs(analytic.sum(0)).max() < 1e-8
         a0 += mol.natm
 
 
