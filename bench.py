@@ -154,6 +154,33 @@ def run_reference(a):
 
 
 # ------------------------------------------------------------------ B200 arm
+def gradient_timing(mols, a, net):
+    """Nuclear gradients (b2_grad) of a converged batch: CUDA-event time of the full gradient and
+    of each term (one-electron, two-electron, exchange-correlation, nuclear), after one warm-up
+    call; the orbitals and grid stay resident between calls."""
+    import torch
+    from b200dft.engine import RKSEngine
+    eng = RKSEngine(mols, level=a.level, precision=a.precision, guess=a.guess, net=net)
+    try:
+        r = eng.run_converged()
+        ms = {}
+        for name, parts in (("full", 15), ("one_electron", 1), ("two_electron", 2), ("xc", 4), ("nuclear", 8)):
+            eng.gradient(parts=parts)
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            t0.record()
+            for _ in range(3):
+                eng.gradient(parts=parts)
+            t1.record()
+            torch.cuda.synchronize()
+            ms[name] = t0.elapsed_time(t1) / 3
+        return {"molecules": len(mols), "converged": int(r["converged"].sum().item()), "ms_per_call": ms,
+                "molecules_per_s": len(mols) / (ms["full"] / 1000.0), "dtype": "f64",
+                "timing": "CUDA events, mean of 3 calls after one warm-up call"}
+    finally:
+        eng.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -169,6 +196,8 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=8)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-mode", action="store_true", help="timed steps only (for ncu captures)")
+    ap.add_argument("--grad", type=int, default=0,
+                    help="also time the nuclear gradient (b2_grad) of the first N converged molecules (0: off)")
     a = ap.parse_args()
     if a.impl == "reference":
         return run_reference(a)
@@ -284,6 +313,10 @@ def main():
                 "traffic_source": "ncu 256-molecule capture scaled by list size",
                 "algorithmic_bytes_per_launch": jk_bytes, "ms_per_launch": jk_ms}
 
+    grad = None
+    if a.grad > 0 and rank == 0:
+        grad = gradient_timing(mols[:a.grad], a, net)
+
     if a.profile_mode:
         a.plain_sample = 0
         a.no_cpu = True
@@ -373,6 +406,8 @@ def main():
                     "p99_its": float(np.percentile(iters[conv], 99)) if conv.any() else None},
             "plain_fp64_per_molecule": plain,
         }
+        if grad is not None:
+            out["gradient"] = grad
         print(json.dumps(out))
     if world > 1:
         dist.destroy_process_group()

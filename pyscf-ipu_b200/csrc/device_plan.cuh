@@ -13,7 +13,6 @@ struct B2GridDev {             // grid layout registered with b2_grid_set
   long long *xblk32 = nullptr, *xblk64 = nullptr;   // fused-XC CTA prefix per precision
   long long *xblk_tc = nullptr;                     // tensor-core XC CTA prefix (128-point tiles)
   int tpc32 = 1, tpc64 = 1, tpc_tc = 1;             // tiles per CTA
-  double *rt = nullptr;        // unused (kept for layout compatibility)
   double *tmpl = nullptr;      // atomic grid templates (x, y, z, w)
   long long *tmpl_off = nullptr, *atom_pt_off = nullptr;
   std::vector<long long> grid_off_h, ao_off_h, xblk32_h, xblk64_h, xblk_tc_h;

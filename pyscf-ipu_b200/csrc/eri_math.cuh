@@ -20,7 +20,7 @@
 // bra primitive data with the row's bra components folded in (per CTA)
 template <typename T>
 struct B2BraPrim {
-  T zeta, Px, Py, Pz, K, E0, Ea, Eb, Eab, xsel;   // xsel unused padding
+  T zeta, Px, Py, Pz, K, E0, Ea, Eb, Eab, xsel;   // xsel: padding to 80 bytes (float64)
 };
 
 template <typename T>
