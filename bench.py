@@ -38,6 +38,66 @@ def _peaks():
     return 6650.0, "fallback"
 
 
+def _tensor_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        return json.load(open(p)).get("bf16_tflops", 1590.0), "measured"
+    return 1590.0, "fallback"
+
+
+def quartet_counts(mols):
+    """canonical shell quartets (IJ >= KL over shell pairs I >= J) of the molecules and their
+    primitive quartets before screening"""
+    quartets = prim = 0
+    for m in mols:
+        npr = np.asarray(m._bas)[:, 2].astype(np.int64)            # libcint NPRIM_OF slot
+        pp = (npr[:, None] * npr[None, :])[np.tril_indices(len(npr))]
+        s = int(pp.sum())
+        quartets += len(pp) * (len(pp) + 1) // 2
+        prim += (s * s + int((pp * pp).sum())) // 2
+    return quartets, prim
+
+
+def kernel_figures(eng, precision):
+    """Throughput of the ERI and XC entry points on the resident batch (CUDA events around
+    repeated calls, after one warm-up call): shell quartets/s and primitive quartets/s of the s8
+    ERI generation (b2_eri_s8; float32 SIMT, no measured peak to divide by) and the XC grid
+    products' algorithmic TFLOP/s (b2_xc_direct; 4 G N^2 per molecule: rho and V_xc products)."""
+    import torch
+    from b200dft._lib import lib, check, ptr, stream_handle
+    P = eng.plan
+
+    def timed(fn, n):
+        fn()
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(n):
+            fn()
+        t1.record()
+        torch.cuda.synchronize()
+        return t0.elapsed_time(t1) / n
+
+    quartets, prim = quartet_counts(eng.mols)
+    prec = 64 if precision == "fp64" else 32
+    eri_ms = timed(lambda: check(lib().b2_eri_s8(P.h, prec, ptr(eng.eri), stream_handle()), "b2_eri_s8"), 3)
+    G = np.diff(P.grid_off).astype(np.float64)
+    N = P.nao.astype(np.float64)
+    flops = float((4.0 * G * N * N).sum())
+    xc_ms = timed(lambda: eng.xc(active=None), 5)
+    tf = flops / (xc_ms / 1e3) / 1e12
+    peak, kind = _tensor_peak()
+    return {
+        "eri": {"entry": "b2_eri_s8", "ms_per_call": eri_ms, "shell_quartets": quartets,
+                "primitive_quartets_unscreened": prim, "shell_quartets_per_s": quartets / (eri_ms / 1e3),
+                "primitive_quartets_per_s": prim / (eri_ms / 1e3), "bound": "float32 SIMT compute"},
+        "xc": {"entry": "b2_xc_direct", "ms_per_call": xc_ms, "algorithmic_flops": flops, "tflops": tf,
+               "peak_tflops": peak, "peak_kind": f"{kind} bf16 dense", "frac": tf / peak,
+               "note": "tf32 operands (nominal tf32 peak is half the bf16 peak); AO values are generated on "
+                       "chip, so the kernel also spends CUDA-core time per point"},
+    }
+
+
 class Clocks:
     """nvidia-smi sampler during the timed region."""
 
@@ -313,6 +373,16 @@ def main():
                 "traffic_source": "ncu 256-molecule capture scaled by list size",
                 "algorithmic_bytes_per_launch": jk_bytes, "ms_per_launch": jk_ms}
 
+    # per-kernel figures beside the roofline; a failure here is recorded in the line, it does
+    # not void it
+    kernels = {}
+    if not a.profile_mode:
+        try:
+            kernels = kernel_figures(eng, a.precision)
+        except Exception as e:  # noqa: BLE001
+            kernels = {"error": f"{type(e).__name__}: {e}"}
+    kernels["jk"] = {"entry": "b2_jk_pairs", "ms_per_call": jk_ms, "gbs": achieved, "frac": achieved / hbm}
+
     grad = None
     if a.grad > 0 and rank == 0:
         grad = gradient_timing(mols[:a.grad], a, net)
@@ -397,7 +467,7 @@ def main():
                        "nmol_per_gpu": a.nmol, "precision": a.precision, "guess": a.guess,
                        "l2": "inputs (s8 ERIs, AO values) larger than L2 between iterations",
                        "convergence": "|dE|<1e-6 Ha and DIIS err<1e-4, retire converged"},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+            "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
             "gpu_launches": gpu_launches,
             "phases_ms_per_step": {k: v / a.steps for k, v in phase.items()},
             "scf": {"converged": int(conv.sum()), "of": int(len(conv)),
