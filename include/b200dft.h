@@ -182,6 +182,10 @@ int b2_guess(b2_plan_t plan, double *D, void *stream);
 /* Nuclear repulsion per molecule (mol.energy_nuc(), dft.py:202); device float64 [nmol]. */
 int b2_enuc(b2_plan_t plan, double *enuc, void *stream);
 
+/* ERI threshold (nanoDFT.py:280-288, option eri_threshold): every entry of the s8 list with
+ * |v| <= threshold becomes 0.  Apply before b2_jk_exchange, which reads the thresholded list. */
+int b2_eri_threshold(b2_plan_t plan, int precision, void *eri, double threshold, void *stream);
+
 /* Nuclear gradient of converged SCFs, float64 (replaces grad(mol, coords, weight, mo_coeff,
  * mo_energy) = grad_elec + grad_nuc, nanoDFT.py:403-477, with the grid held fixed as there).
  * With C (device float64 matrices at the plan's matrix offsets, column k = orbital k) and

@@ -56,6 +56,7 @@ SIGNATURES = {
     "b2_guess": [_P, _P, _P],
     "b2_enuc": [_P, _P, _P],
     "b2_grad": [_P, _I, _D, _P, _P, _P, _P, _P, _P, _P, _P],
+    "b2_eri_threshold": [_P, _I, _P, _D, _P],
 }
 
 

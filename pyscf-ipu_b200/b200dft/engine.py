@@ -111,9 +111,12 @@ def _require_cuda():
 
 
 class HostSetup:
-    """Per-molecule host inputs (the reference's PySCF-side setup, numpy)."""
+    """Per-molecule host inputs (the reference's PySCF-side setup, numpy).  With
+    ``ao_threshold`` > 0 the AO values are evaluated here, thresholded and the grid points left
+    without any AO value are dropped (nanoDFT.py:221-230); ``ao`` then holds the (4, G, nao)
+    values the SCF uses in place of on-the-fly ones."""
 
-    def __init__(self, mol, level=0, grid=None, D0=None):
+    def __init__(self, mol, level=0, grid=None, D0=None, ao_threshold=0.0):
         self.mol = mol
         S, T, V = int1e(mol)
         self.S, self.T, self.V = S, T, V
@@ -123,6 +126,11 @@ class HostSetup:
             grid = Grids(mol, level).build()
         self.coords = np.ascontiguousarray(grid.coords, np.float64)
         self.weights = np.ascontiguousarray(grid.weights, np.float64)
+        self.ao = None
+        if ao_threshold and ao_threshold > 0.0:
+            from .ao import eval_ao, threshold_grid
+            self.ao, self.coords, self.weights = threshold_grid(eval_ao(mol, self.coords), self.coords,
+                                                                self.weights, ao_threshold)
         self.D0 = minao(mol) if D0 is None else np.asarray(D0, np.float64)
         self.E_nuc = mol.energy_nuc()
 
@@ -154,7 +162,7 @@ class RKSEngine:
     """
 
     def __init__(self, mols, level=0, precision="fp64", setups=None, device=None, jk_chunk=None,
-                 plan=None, guess="minao", net=None):
+                 plan=None, guess="minao", net=None, eri_threshold=0.0):
         _require_cuda()
         self.mols = list(mols)
         self.level = level
@@ -199,7 +207,19 @@ class RKSEngine:
         self.eri = torch.empty(max(1, P.n_eri), dtype=rdt, device=dev)
         self.eri_x = torch.empty(max(1, P.n_eri), dtype=rdt, device=dev)   # exchange list for J/K
         self.jk_impl = "pairs"      # "pairs": two products over the s8 and exchange lists; "s8"
+        self.eri_threshold = float(eri_threshold or 0.0)   # > 0: |ERI| <= it become 0 (nanoDFT.py:280)
         self.ao = None          # (4, G, nao) AO tensor, only for the AO-input XC entry
+        self.ao_stored = False  # the SCF's XC reads self.ao (thresholded host AO values)
+        self._ao_done = False
+        if setups is not None and any(getattr(s, "ao", None) is not None for s in setups):
+            if not all(getattr(s, "ao", None) is not None for s in setups):
+                raise ValueError("either every HostSetup of a batch carries AO values or none does")
+            self.ao = torch.zeros(max(1, P.n_ao), dtype=rdt, device=dev)
+            for m, s in enumerate(setups):
+                o = int(P.ao_off[m])
+                self.ao[o:o + s.ao.size] = torch.from_numpy(np.ascontiguousarray(s.ao).reshape(-1)).to(dev, rdt)
+            self._ao_done = True
+            self.ao_stored = True
         self.D, self.J, self.K, self.Vxc = z(nmat), z(nmat), z(nmat), z(nmat)
         self.H, self.diffJK = z(nmat), z(nmat)
         self.ring_err, self.ring_h = z(9 * nmat), z(9 * nmat)
@@ -214,7 +234,6 @@ class RKSEngine:
         self.active = torch.ones(nm, dtype=torch.int32, device=dev)
         self.sweeps = torch.zeros(nm, dtype=torch.int32, device=dev)
         self._eri_done = False
-        self._ao_done = False
         self._graph = None
         self.guess = guess                  # "minao" or "learned"
         self.net = net
@@ -280,6 +299,9 @@ class RKSEngine:
     # --- kernels -----------------------------------------------------------------------
     def compute_eri(self, stream=None):
         check(lib().b2_eri_s8(self.plan.h, self.prec, ptr(self.eri), stream_handle(stream)), "b2_eri_s8")
+        if self.eri_threshold > 0.0:
+            check(lib().b2_eri_threshold(self.plan.h, self.prec, ptr(self.eri), self.eri_threshold,
+                                         stream_handle(stream)), "b2_eri_threshold")
         check(lib().b2_jk_exchange(self.plan.h, self.prec, ptr(self.eri), ptr(self.eri_x), stream_handle(stream)),
               "b2_jk_exchange")
         self._eri_done = True
@@ -308,6 +330,14 @@ class RKSEngine:
         D = self.D if D is None else D
         check(lib().b2_xc_direct(self.plan.h, self.prec, ptr(active), ptr(self.coords), ptr(self.weights),
                                  ptr(D), ptr(self.Vxc), ptr(self.exc), stream_handle(stream)), "b2_xc_direct")
+
+    def scf_xc(self, active=None, stream=None):
+        """the SCF's XC step: stored (thresholded) AO values when the setups carry them, else AO
+        values generated per grid tile"""
+        if self.ao_stored:
+            self.xc_from_ao(active=active, stream=stream)
+        else:
+            self.xc(active=active, stream=stream)
 
     def xc_from_ao(self, D=None, active=None, stream=None):
         """E_xc and V_xc from the stored AO tensor (compute_ao first)."""
@@ -347,7 +377,7 @@ class RKSEngine:
         self.D.copy_(self.D0)
         self.iter.zero_()
         self.active.fill_(1)
-        self.xc()
+        self.scf_xc()
         self.jk()
 
     def step(self, use_diis=True):
@@ -355,7 +385,7 @@ class RKSEngine:
         a = self.active
         self.fock_diis(use_diis)
         self.eigh_density()
-        self.xc(active=a)
+        self.scf_xc(active=a)
         self.jk(active=a)
         torch.add(self.J, self.K, alpha=-0.5 * HYB_B3LYP, out=self.diffJK)
         self.energies()
@@ -497,7 +527,7 @@ class RKSEngine:
             self.D[o:o + n].copy_(self.D0_minao[o:o + n])
         self.iter.masked_fill_(mask, 0)
         act = mask.to(torch.int32)
-        self.xc(active=act)
+        self.scf_xc(active=act)
         self.jk(active=act)
 
     def gradient(self, parts=15, hyb=HYB_B3LYP, stream=None):

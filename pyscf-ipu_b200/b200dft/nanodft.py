@@ -69,11 +69,12 @@ def nanoDFT(mol, opts):
     """Run the SCF for ``mol`` on the B200 (nanoDFT.py:259-336)."""
     if opts.structure_optimization:
         raise NotImplementedError("structure optimisation is outside the SCF hot path")
-    setup = HostSetup(mol, level=opts.level)
-    if opts.ao_threshold and opts.ao_threshold > 0:
-        # nanoDFT.py:221-230 drops grid points whose AO values are all below the threshold
-        from .grids import Grids as _G  # noqa: F401
-    eng = RKSEngine([mol], precision="mixed" if opts.float32 else "fp64", setups=[setup])
+    # ao_threshold > 0: AO values below it are zeroed and grid points left without any are
+    # dropped (nanoDFT.py:221-230); the SCF then reads those stored AO values
+    setup = HostSetup(mol, level=opts.level, ao_threshold=opts.ao_threshold or 0.0)
+    # eri_threshold > 0: s8 entries with |v| <= it are zeroed before J/K (nanoDFT.py:280-288)
+    eng = RKSEngine([mol], precision="mixed" if opts.float32 else "fp64", setups=[setup],
+                    eri_threshold=opts.eri_threshold or 0.0)
     try:
         res = eng.run(its=opts.its, use_diis=opts.diis, log=True)
     finally:

@@ -488,6 +488,11 @@ int b2_enuc(void *plan, double *enuc, void *stream) {
   return b2_launch_enuc(*(B2PlanDev *)plan, enuc, (cudaStream_t)stream);
 }
 
+int b2_eri_threshold(void *plan, int precision, void *eri, double threshold, void *stream) {
+  if (!plan) return B2_ERR_ARG;
+  return b2_launch_eri_threshold(*(B2PlanDev *)plan, precision, eri, threshold, (cudaStream_t)stream);
+}
+
 int b2_grad(void *plan, int parts, double hyb, const double *C, const double *mo_energy, const double *coords,
             const double *weights, double *D, double *W, double *grad, void *stream) {
   if (!plan) return B2_ERR_ARG;

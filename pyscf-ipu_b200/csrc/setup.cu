@@ -4,6 +4,7 @@
 // minao dft.py:223, energy_nuc dft.py:202) and follow the same formulas as the package's
 // host versions (b200dft/int1e.py, b200dft/grids.py, b200dft/guess.py), so the device
 // setup reproduces the host setup to rounding.
+#include <algorithm>
 #include <vector>
 #include "device_plan.cuh"
 #include "devmem.cuh"
@@ -207,6 +208,27 @@ __global__ void k_add(long long n, const double *__restrict__ a, const double *_
                       double *__restrict__ c) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) c[i] = a[i] + b[i];
+}
+
+// s8 entries with |v| <= threshold become 0 (the ERI threshold of nanoDFT.py:280-288); the
+// molecules' padding entries are never read, so the whole buffer is swept
+template <typename T>
+__global__ void k_threshold(long long n, T *__restrict__ x, double thr) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    if (fabs((double)x[i]) <= thr) x[i] = (T)0;
+}
+
+int b2_launch_eri_threshold(const B2PlanDev &P, int precision, void *eri, double thr, cudaStream_t st) {
+  if (!eri || (precision != 32 && precision != 64) || !(thr >= 0.0)) return B2_ERR_ARG;
+  const long long n = P.h.n_eri;
+  if (n > 0) {
+    const unsigned nb = (unsigned)std::min<long long>((n + 255) / 256, 148ll * 32);
+    if (precision == 64) k_threshold<double><<<nb, 256, 0, st>>>(n, (double *)eri, thr);
+    else k_threshold<float><<<nb, 256, 0, st>>>(n, (float *)eri, thr);
+    b2_count_launches(1);
+  }
+  B2_CUDA_TRY(cudaGetLastError());
+  return B2_OK;
 }
 
 int b2_launch_int1e(const B2PlanDev &P, double *S, double *T, double *V, cudaStream_t st) {

@@ -80,3 +80,42 @@ def test_kinetic_fd_identity():
     m = Mole("O 0 0 0.1173; H 0 0.7572 -0.4692; H 0 -0.7572 -0.4692")
     S, T, V = int1e(m)
     assert np.linalg.eigvalsh(T).min() > 0
+
+
+def test_host_ao_values_match_oracle():
+    from oracle import rks
+    from b200dft.ao import eval_ao
+    m = Mole("N 0 0 0; C 0 0 2.6; O 2.1 0 3.9; H 0 1.9 -0.8", unit="Bohr")
+    g = grids.Grids(m, 0).build()
+    a = eval_ao(m, g.coords)
+    np.testing.assert_allclose(a, rks.ao_values(m, g.coords), atol=1e-13, rtol=0)
+
+
+def test_ao_threshold_as_nanodft():
+    """b200dft.ao.threshold_grid against the reference's steps, nanoDFT.py:221-230, written out"""
+    from oracle import rks
+    from b200dft.ao import threshold_grid
+    m = Mole(methane())
+    g = grids.Grids(m, 0).build()
+    coords, w = np.asarray(g.coords), np.asarray(g.weights)
+    ao = rks.ao_values(m, coords)
+    for thr in (1e-6, 1e-3, 1e-2):
+        A = ao.copy()
+        A[np.abs(A) < thr] = 0
+        sparsity_mask = np.where(np.all(A == 0, axis=0), 0, 1)
+        sparse_rows = np.where(np.all(sparsity_mask == 0, axis=1), 0, 1).reshape(-1, 1)
+        drop = np.where(sparse_rows == 0)[0]
+        ref = (np.delete(A, drop, axis=1), np.delete(coords, drop, axis=0), np.delete(w, drop, axis=0))
+        got = threshold_grid(ao, coords, w, thr)
+        for x, y in zip(got, ref):
+            np.testing.assert_array_equal(x, y)
+    assert len(got[2]) < len(w)                  # the largest threshold drops points
+
+
+def test_host_setup_with_ao_threshold():
+    from b200dft.engine import HostSetup
+    m = Mole(methane())
+    s0 = HostSetup(m, level=0)
+    s1 = HostSetup(m, level=0, ao_threshold=1e-2)
+    assert s0.ao is None and s1.ao.shape == (4, len(s1.weights), m.nao)
+    assert 0 < len(s1.weights) < len(s0.weights) and s1.coords.shape == (len(s1.weights), 3)
