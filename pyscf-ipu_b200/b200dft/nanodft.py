@@ -53,7 +53,10 @@ def nanoDFT_options(its: int = 20, mol_str: str = "benzene", float32: bool = Fal
                     ndevices: int = 1, dense_ERI: bool = False, v: bool = False,
                     profile: bool = False, vis_num_error: bool = False, molecule_name: str = None):
     """Same fields as the reference's nanoDFT_options (nanoDFT.py:548-618); returns
-    (immutable options, processed mol_str)."""
+    (immutable options, processed mol_str).  its, float32, level, diis, eri_threshold and
+    ao_threshold shape the B200 run; the IPU scheduling knobs (multv, intv, threads,
+    threads_int, batches, ndevices) and dense_ERI (the dense and s8 ERI forms give the same J/K)
+    leave it unchanged, and v / profile / vis_num_error (plots) are accepted and unused."""
     if xc.lower() != "b3lyp":
         raise ValueError("only B3LYP is supported (as in the reference, nanoDFT.py:627)")
     if molecule_name is None:
