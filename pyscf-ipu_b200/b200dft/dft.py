@@ -49,6 +49,11 @@ def density_functional_theory(atom_positions, args, mf_diis_space=9):
         raise ValueError("the device DIIS ring holds 9 entries (as the reference's IPU path)")
     if args.xc.lower() != "b3lyp":
         raise ValueError("only B3LYP is supported")
+    # the reference's timing switches that skip or randomise work (dft.py:127-133, 827) change
+    # the results; they are refused rather than ignored
+    for flag in ("skiperi", "randeri", "skipeigh", "float16"):
+        if getattr(args, flag, False):
+            raise ValueError(f"-{flag} (a timing switch that skips or randomises work) is not supported")
     if mol is None:
         raise RuntimeError("set b200dft.dft.mol (jax_dft does) before calling")
     setup = HostSetup(mol, level=args.level)

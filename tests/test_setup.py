@@ -119,3 +119,13 @@ def test_host_setup_with_ao_threshold():
     s1 = HostSetup(m, level=0, ao_threshold=1e-2)
     assert s0.ao is None and s1.ao.shape == (4, len(s1.weights), m.nao)
     assert 0 < len(s1.weights) < len(s0.weights) and s1.coords.shape == (len(s1.weights), 3)
+
+
+def test_dft_dropin_refuses_work_skipping_switches():
+    import types
+    import pytest
+    from b200dft import dft
+    for flag in ("skiperi", "randeri", "skipeigh", "float16"):
+        args = types.SimpleNamespace(xc="b3lyp", its=2, level=0, float32=False, skipdiis=False, **{flag: True})
+        with pytest.raises(ValueError, match=flag):
+            dft.density_functional_theory(None, args)
