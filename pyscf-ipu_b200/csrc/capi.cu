@@ -395,7 +395,7 @@ int b2_xc(void *plan, int precision, const int *active, const void *ao, const do
           const double *D, double *Vxc, double *Exc, void *stream) {
   if (!plan || !ao || !weights || !D || !Vxc || !Exc) return B2_ERR_ARG;
   B2PlanDev *P = (B2PlanDev *)plan;
-  return b2_launch_xc(*P, precision, active, ao, weights, D, Vxc, Exc, nullptr, (cudaStream_t)stream);
+  return b2_launch_xc(*P, precision, active, ao, weights, D, Vxc, Exc, (cudaStream_t)stream);
 }
 
 int b2_xc_direct(void *plan, int precision, const int *active, const double *coords,

@@ -350,10 +350,8 @@ static int b2_xc_impl(const B2PlanDev &P, const int *active, const T *ao, const 
 }
 
 int b2_launch_xc(const B2PlanDev &P, int precision, const int *active, const void *ao,
-                 const double *w, const double *D, double *V, double *exc, void *rt_scratch,
-                 cudaStream_t st) {
+                 const double *w, const double *D, double *V, double *exc, cudaStream_t st) {
   if (!P.g.grid_off) return B2_ERR_ARG;
-  (void)rt_scratch;
   if (precision == 64)
     return b2_xc_impl<double, 32>(P, active, (const double *)ao, w, D, V, exc, P.g.xblk64,
                                   P.g.n_xblk64, P.g.tpc64, st);

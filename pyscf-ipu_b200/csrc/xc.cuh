@@ -4,8 +4,7 @@ int b2_grid_setup(B2PlanDev &P, const long long *grid_off_host);
 void b2_grid_free(B2PlanDev &P);
 int b2_launch_ao_eval(const B2PlanDev &P, int precision, const double *coords, void *ao, cudaStream_t st);
 int b2_launch_xc(const B2PlanDev &P, int precision, const int *active, const void *ao,
-                 const double *w, const double *D, double *V, double *exc, void *rt_scratch,
-                 cudaStream_t st);
+                 const double *w, const double *D, double *V, double *exc, cudaStream_t st);
 int b2_launch_xc_direct(const B2PlanDev &P, int precision, const int *active, const double *coords,
                         const double *w, const double *D, double *V, double *exc, cudaStream_t st);
 int b2_launch_xc_tc(const B2PlanDev &P, const int *active, const double *coords, const double *w,
