@@ -204,12 +204,6 @@ __global__ void k_enuc(const B2MolDev *__restrict__ mols, int nmol, const double
   enuc[m] = e;
 }
 
-__global__ void k_add(long long n, const double *__restrict__ a, const double *__restrict__ b,
-                      double *__restrict__ c) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) c[i] = a[i] + b[i];
-}
-
 // s8 entries with |v| <= threshold become 0 (the ERI threshold of nanoDFT.py:280-288); the
 // molecules' padding entries are never read, so the whole buffer is swept
 template <typename T>
@@ -296,11 +290,3 @@ int b2_launch_enuc(const B2PlanDev &P, double *enuc, cudaStream_t st) {
   return B2_OK;
 }
 
-int b2_launch_add(long long n, const double *a, const double *b, double *c, cudaStream_t st) {
-  if (n > 0) {
-    k_add<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, a, b, c);
-    b2_count_launches(1);
-  }
-  B2_CUDA_TRY(cudaGetLastError());
-  return B2_OK;
-}

@@ -5,5 +5,4 @@ int b2_launch_grid_build(B2PlanDev &P, int nz, const double *tmpl_host, const lo
                          double *coords, double *weights, cudaStream_t st);
 int b2_launch_guess(const B2PlanDev &P, double *D, cudaStream_t st);
 int b2_launch_enuc(const B2PlanDev &P, double *enuc, cudaStream_t st);
-int b2_launch_add(long long n, const double *a, const double *b, double *c, cudaStream_t st);
 int b2_launch_eri_threshold(const B2PlanDev &P, int precision, void *eri, double thr, cudaStream_t st);
