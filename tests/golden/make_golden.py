@@ -9,6 +9,8 @@
   full) the reference's values at 4096 seeded positions plus sum and sum of squares.
 * scf_oracle_<name>.npz: FP64 oracle SCF trajectory (energies per iteration, final
   mo_energy) on this project's level-0 grid; used to pin later changes of the oracle.
+* scf_oracle_config2_level3.npz: the same for the seeded 9-heavy-atom molecule on the level-3
+  grid (426 762 points), plus the final density, for the single-molecule precision comparison.
 """
 import os
 import sys
@@ -58,6 +60,20 @@ def main():
         np.savez_compressed(os.path.join(HERE, f"scf_oracle_{name}.npz"), energies=r["energies"],
                             mo_energy=r["mo_energy"], atom=s, unit=unit, level=0)
         print(name, r["energies"][-1, 0])
+    scf_config2_level3()
+
+
+def scf_config2_level3():
+    m = Mole(config2_molecule(0))
+    g = build_grid(m, 3)
+    S, T, V = int1e(m)
+    ao = rks.ao_values(m, g.coords)
+    r = rks.scf(S, T, V, minao(m), eri.ref_eri_s8(m), ao, g.weights, m.nelectron // 2, m.energy_nuc(),
+                its=20)
+    np.savez_compressed(os.path.join(HERE, "scf_oracle_config2_level3.npz"), energies=r["energies"],
+                        mo_energy=r["mo_energy"], D=r["logs"][-1, 0], atom=config2_molecule(0),
+                        unit="Angstrom", level=3, npoints=len(g.weights))
+    print("config2 level 3", r["energies"][-1, 0], len(g.weights))
 
 
 if __name__ == "__main__":

@@ -140,3 +140,33 @@ def test_converged_graph_equals_eager(cuda):
     b = RKSEngine(mols, level=0, precision="fp64").run_converged(graph=False)
     np.testing.assert_allclose(a["energy"].cpu().numpy(), b["energy"].cpu().numpy(), atol=1e-10)
     assert (a["iterations"].cpu().numpy() == b["iterations"].cpu().numpy()).all()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_config2_level3_per_precision(cuda, precision):
+    """the seeded 9-heavy-atom molecule (nao 62) on the level-3 grid (426 762 points), plain FP64
+    and mixed precision against the FP64 oracle: J/K on the oracle's converged density and the
+    energies of 20 iterations from the same guess (its ERIs: test_eri_config2_full)"""
+    g = golden("scf_oracle_config2_level3.npz")
+    m = Mole(str(g["atom"]), unit=str(g["unit"]))
+    setup = HostSetup(m, 3)
+    assert len(setup.weights) == int(g["npoints"])
+    eng = RKSEngine([m], level=3, precision=precision, setups=[setup])
+    try:
+        res = eng.run(its=20, log=False)
+        D = g["D"]
+        eng.jk(D=torch.from_numpy(eng.plan.pack([D])).to(cuda))
+        torch.cuda.synchronize()
+        J = eng.plan.unpack(eng.J.cpu().numpy(), 0)
+        K = eng.plan.unpack(eng.K.cpu().numpy(), 0)
+    finally:
+        eng.close()
+    _, Jr, Kr = rks.jk_from_s8(D, oeri.eri_s8(m), m.nao)
+    tol = 1e-9 if precision == "fp64" else 2e-5 * max(1.0, np.abs(Jr).max())
+    np.testing.assert_allclose(J, Jr, atol=tol, rtol=0)
+    np.testing.assert_allclose(K, Kr, atol=tol, rtol=0)
+    E = res["energies"][:, 0, 0]
+    if precision == "fp64":
+        assert np.abs(E - g["energies"][:, 0]).max() <= 1e-6          # every iteration
+    else:
+        assert abs(E[-1] - g["energies"][-1, 0]) <= 1e-4              # north-star: 0.1 mHa
