@@ -566,10 +566,11 @@ def nuclear_gradient(plan, C, mo_energy, coords, weights, parts=15, hyb=HYB_B3LY
     return g[:n_atm]
 
 
-def _run_one(mols, plan, level, precision, guess, net, run_kw, after_prepare=None):
+def _run_one(mols, plan, level, precision, guess, net, run_kw, after_prepare=None, gradient=False):
     """one batch to convergence; returns host arrays, the engine's device memory released
     (back to the allocator cache, where the next batch's engine finds it).  ``after_prepare``
-    runs once the batch's setup and ERI work is queued."""
+    runs once the batch's setup and ERI work is queued; with ``gradient`` the result also holds
+    the nuclear gradients of the final orbitals (sum of natm x 3, Ha/Bohr)."""
     import time
     t0 = time.perf_counter()
     eng = RKSEngine(mols, level=level, precision=precision, guess=guess, net=net, plan=plan)
@@ -583,10 +584,14 @@ def _run_one(mols, plan, level, precision, guess, net, run_kw, after_prepare=Non
         out = {k: r[k].cpu().numpy() for k in ("energy", "iterations", "converged", "mo_energy",
                                                "last5", "diis_err")}
         t3 = time.perf_counter()
+        if gradient:
+            out["gradient"] = eng.gradient().cpu().numpy()
         out["its_run"] = r["its_run"]
         out["h2d_bytes"] = plan.h2d_bytes + getattr(getattr(eng, "_nn_batch", None), "h2d_bytes", 0)
         # host wall time of the batch's parts (ms): engine set-up, setup + ERI launch, SCF to results
         out["host_ms"] = {"engine": 1e3 * (t1 - t0), "prepare": 1e3 * (t2 - t1), "scf": 1e3 * (t3 - t2)}
+        if gradient:
+            out["host_ms"]["gradient"] = 1e3 * (time.perf_counter() - t3)
         out["host_ms"].update({"scf_" + k: v for k, v in getattr(eng, "host_ms", {}).items()})
         out["its_run"] = r["its_run"]
         return out
@@ -594,10 +599,12 @@ def _run_one(mols, plan, level, precision, guess, net, run_kw, after_prepare=Non
         eng.close()
 
 
-def run_batches(batches, level=0, precision="mixed", guess="learned", net=None, prefetch=True, **run_kw):
+def run_batches(batches, level=0, precision="mixed", guess="learned", net=None, prefetch=True, gradient=False,
+                **run_kw):
     """Run a sequence of molecule batches to convergence, one ``RKSEngine`` each, yielding
     ``(mols, result)`` per batch with the result's arrays on the host (energy, iterations,
-    converged, mo_energy, last5, diis_err).
+    converged, mo_energy, last5, diis_err; with ``gradient`` also the nuclear gradients, the
+    batch's atoms back to back).
 
     With ``prefetch`` the next batch's plan (host tables, upload and device table build on the
     plan's own stream) is made on a worker thread while the current batch runs on the GPU (from
@@ -628,7 +635,8 @@ def run_batches(batches, level=0, precision="mixed", guess="learned", net=None, 
             # the next plan's table kernels start once this batch's setup and ERI kernels are
             # queued, so they do not hold up the kernels this batch waits on first
             start = (lambda: fut.append(ex.submit(make, nxt))) if (ex and nxt is not None) else None
-            out = _run_one(mols, plan, level, precision, guess, net, run_kw, after_prepare=start)
+            out = _run_one(mols, plan, level, precision, guess, net, run_kw, after_prepare=start,
+                           gradient=gradient)
             out["host_ms"]["plan_wait"] = wait_ms
             del plan                      # the engine and plan are released before the next batch
             cur = None

@@ -99,6 +99,11 @@ def batch_rows(items, res, seed):
                  "std": std.tolist(), "y": np.abs(lumo - homo).tolist(), "iterations": its.astype(int).tolist(),
                  "converged": conv.astype(bool).tolist(),
                  "last5": [row[f].tolist() for row, f in zip(last5, fin)]})
+    if "gradient" in res:
+        # nuclear gradient dE/dR (Ha/Bohr) of each molecule, flattened like pos
+        g = h(res["gradient"]).reshape(-1, 3)
+        a0 = np.concatenate([[0], np.cumsum([m.natm for m in mols])])
+        cols["gradient"] = [g[a0[k]:a0[k + 1]].reshape(-1).tolist() for k in range(n)]
     return cols
 
 
@@ -116,7 +121,7 @@ class RowWriter:
         if self.fmt == "parquet":
             import pyarrow as pa
             import pyarrow.parquet as pq
-            keep = QM1B_COLUMNS + ("iterations", "converged")
+            keep = QM1B_COLUMNS + ("iterations", "converged") + (("gradient",) if "gradient" in cols else ())
             t = pa.table({k: cols[k] for k in keep})
             if self._pq is None:
                 self._pq = pq.ParquetWriter(self.path, t.schema)
@@ -128,6 +133,8 @@ class RowWriter:
                 "energies": cols["last5"], "std": cols["std"], "homo": cols["homo"],
                 "lumo": cols["lumo"], "hlgap": cols["y"], "N": cols["N"],
                 "basis": [self.basis] * len(cols["N"])})
+            if "gradient" in cols:
+                df["gradient"] = cols["gradient"]
             df.to_csv(self.path, mode="a", header=self._first, compression="gzip")
             self._first = False
 
@@ -139,10 +146,12 @@ class RowWriter:
 
 def run_stream(n_total, batch=4096, seed=0, level=0, precision="mixed", guess="learned", out=None,
                fmt="parquet", workers=None, max_heavy=9, net=None, e_tol=1e-6, diis_tol=1e-4,
-               rank=0, world=1):
+               rank=0, world=1, gradient=False):
     """Generate ``n_total`` molecules and write one row each; returns throughput and iteration
     statistics (the streaming configuration: molecules/s, p50/p99 iterations).  With
-    ``world`` > 1 this process handles the stream chunks of ``rank`` (round robin) only."""
+    ``world`` > 1 this process handles the stream chunks of ``rank`` (round robin) only.  With
+    ``gradient`` each row also carries the molecule's nuclear gradient (force labels, dE/dR in
+    Ha/Bohr, flattened like ``pos``; nanoDFT.py:440-477 on the SCF's final orbitals)."""
     if guess == "learned" and net is None:
         from .train_guess import load
         net = load()
@@ -206,10 +215,10 @@ def run_stream(n_total, batch=4096, seed=0, level=0, precision="mixed", guess="l
         # run_batches builds each next plan on its worker thread once the current batch's ERI
         # work is queued, and reuses the engine memory from batch to batch
         for _, res in run_batches(batches(), level=level, precision=precision, guess=guess, net=net,
-                                  e_tol=e_tol, diis_tol=diis_tol):
+                                  gradient=gradient, e_tol=e_tol, diis_tol=diis_tol):
             items = queued.popleft()
             h = res["host_ms"]
-            stats["gpu_s"] += 1e-3 * (h["engine"] + h["prepare"] + h["scf"])
+            stats["gpu_s"] += 1e-3 * (h["engine"] + h["prepare"] + h["scf"] + h.get("gradient", 0.0))
             its = res["iterations"]
             stats["iterations"].append(its)
             stats["converged"] += int((its > 0).sum())
@@ -246,10 +255,11 @@ def main(argv=None):
     ap.add_argument("--out", default=None, help="output file (.parquet or .csv.gz)")
     ap.add_argument("--format", default=None, choices=["parquet", "csv"])
     ap.add_argument("--workers", type=int, default=None)
+    ap.add_argument("--gradient", action="store_true", help="also write each molecule's nuclear gradient")
     a = ap.parse_args(argv)
     fmt = a.format or ("csv" if a.out and a.out.endswith((".csv", ".csv.gz", ".gz")) else "parquet")
     r = run_stream(a.n, batch=a.batch, seed=a.seed, level=a.level, precision=a.precision, guess=a.guess,
-                   out=a.out, fmt=fmt, workers=a.workers)
+                   out=a.out, fmt=fmt, workers=a.workers, gradient=a.gradient)
     print(json.dumps(r))
     return r
 

@@ -52,6 +52,29 @@ def test_rows_parquet_schema(tmp_path):
     assert abs(r["std"] - np.std((-40.0 + np.arange(3) * 1e-7) * HARTREE_TO_EV)) < 1e-12
 
 
+def test_rows_with_gradient(tmp_path):
+    """force labels: the batch's gradient rows (atoms back to back) split per molecule, written as
+    a flattened list beside pos"""
+    pq = pytest.importorskip("pyarrow.parquet")
+    items = stream_chunk((3, 0, 4, 5))
+    res = _fake_result(items)
+    nat = sum(it[2].natm for it in items)
+    res["gradient"] = torch.arange(3 * nat, dtype=torch.float64).reshape(nat, 3)
+    cols = batch_rows(items, res, seed=3)
+    a0 = 0
+    for k, it in enumerate(items):
+        n3 = 3 * it[2].natm
+        assert cols["gradient"][k] == list(np.arange(3 * a0, 3 * a0 + n3, dtype=float))
+        a0 += it[2].natm
+    path = str(tmp_path / "g.parquet")
+    w = RowWriter(path, "parquet")
+    w.write(cols)
+    w.close()
+    r = pq.read_table(path).to_pylist()
+    assert all(len(row["gradient"]) == len(row["pos"]) for row in r)
+    assert "gradient" not in batch_rows(items, _fake_result(items), seed=3)
+
+
 def test_rows_csv_schema(tmp_path):
     import pandas as pd
     items = stream_chunk((2, 0, 3, 3))
@@ -121,7 +144,7 @@ def _fake_engine(monkeypatch, fail_at=None):
                 log.append(("plan", mols[0], threading.current_thread() is threading.main_thread()))
             self.first = mols[0]
 
-    def fake_run_one(mols, plan, level, precision, guess, net, run_kw, after_prepare=None):
+    def fake_run_one(mols, plan, level, precision, guess, net, run_kw, after_prepare=None, gradient=False):
         assert plan.first == mols[0]
         with lock:
             log.append(("prepare", mols[0]))
@@ -129,7 +152,7 @@ def _fake_engine(monkeypatch, fail_at=None):
             after_prepare()
         with lock:
             log.append(("scf", mols[0]))
-        return {"energy": np.array([float(mols[0])]), "host_ms": {}, "kw": dict(run_kw)}
+        return {"energy": np.array([float(mols[0])]), "host_ms": {}, "kw": dict(run_kw), "gradient": gradient}
 
     monkeypatch.setattr(engine, "Plan", FakePlan)
     monkeypatch.setattr(engine, "_run_one", fake_run_one)
@@ -146,6 +169,7 @@ def test_run_batches_order_and_prefetch_points(monkeypatch, prefetch):
     assert [m for m, _ in out] == batches                       # in order, one result per batch
     assert [float(r["energy"][0]) for _, r in out] == [0, 1, 2, 3, 4]
     assert all(r["kw"] == {"e_tol": 1e-7} and "plan_wait" in r["host_ms"] for _, r in out)
+    assert all(r["gradient"] is False for _, r in out)
     plans = [e for e in log if e[0] == "plan"]
     assert [e[1] for e in plans] == [0, 1, 2, 3, 4]
     assert plans[0][2]                                          # the first plan is made in place
@@ -155,6 +179,12 @@ def test_run_batches_order_and_prefetch_points(monkeypatch, prefetch):
     for k in range(1, 5):
         assert log.index(("prepare", k - 1)) < log.index(plans[k])
         assert log.index(plans[k]) < log.index(("prepare", k))
+
+
+def test_run_batches_passes_gradient(monkeypatch):
+    engine, _ = _fake_engine(monkeypatch)
+    out = list(engine.run_batches(iter([[0], [1]]), guess="minao", gradient=True, e_tol=1e-7))
+    assert [r["gradient"] for _, r in out] == [True, True] and out[0][1]["kw"] == {"e_tol": 1e-7}
 
 
 def test_run_batches_empty_and_plan_errors(monkeypatch):
