@@ -245,7 +245,8 @@ def test_xc_gradient_vs_finite_differences():
 
 
 def test_gradient_math_compiles_for_sm100a(tmp_path):
-    """the gradient math is host and device code: it must also build as sm_100a device code"""
+    """the gradient math is host and device code: it must also build as sm_100a device code (one
+    class of the two-electron part here; the library build compiles all sixteen in grad.cu)"""
     import shutil
     import subprocess
     nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
@@ -258,7 +259,7 @@ def test_gradient_math_compiles_for_sm100a(tmp_path):
         "__global__ void k(const B2Shell *s, const double *t, const double *gam, const double *D,\n"
         "                  const double *W, const double *Z, const double *RC, const double *r, double *o) {\n"
         "  double g4[4][3], g2[2][3], f[3], df[3][3], hf[3][6];\n"
-        "  b2g_quartet_grad<double>(s[0], s[1], s[2], s[3], t, gam, g4);\n"
+        "  b2g_quartet_grad_t<double, 1, 0, 0, 1>(s[0], s[1], s[2], s[3], t, gam, g4);\n"
         "  b2g_pair_grad_1e<double>(s[0], s[1], D, W, 9, 5, Z, RC, t, g2,\n"
         "                           [&](int c, int x, double v) { atomicAdd(o + 3 * c + x, v); });\n"
         "  b2g_ao2<double>(s[0], r, f, df, hf);\n"
