@@ -163,6 +163,47 @@ class Mole:
         return f"Mole(natm={self.natm}, nao={self.nao}, nelectron={self.nelectron})"
 
 
+def pack_moles(mols):
+    """The molecules' arrays concatenated into a few flat arrays: the form in which generation
+    workers send a chunk of molecules (one pickle of a few arrays instead of several small
+    arrays per molecule; unpickling Mole objects cost 65 us each)."""
+    cat = lambda xs, dt: np.ascontiguousarray(np.concatenate(xs), dtype=dt) if xs else np.zeros(0, dt)
+    return {
+        "natm": np.array([m.natm for m in mols], np.int32),
+        "nbas": np.array([m.nbas for m in mols], np.int32),
+        "nenv": np.array([len(m._env) for m in mols], np.int64),
+        "charge": np.array([m.charge for m in mols], np.int32),
+        "basis": [m.basis for m in mols], "unit": [m.unit for m in mols],
+        "coords": cat([m.coords for m in mols], np.float64).reshape(-1, 3),
+        "charges": cat([m.charges for m in mols], np.int32),
+        "atm": cat([m._atm for m in mols], np.int32).reshape(-1, ATM_SLOTS),
+        "bas": cat([m._bas for m in mols], np.int32).reshape(-1, BAS_SLOTS),
+        "env": cat([m._env for m in mols], np.float64),
+        "ao_loc": cat([m.ao_loc for m in mols], np.int32),
+    }
+
+
+def unpack_moles(p):
+    """Mole objects whose arrays are views into the packed arrays (no parsing, no basis build)."""
+    out = []
+    a0 = b0 = e0 = 0
+    for k in range(len(p["natm"])):
+        na, nb, ne = int(p["natm"][k]), int(p["nbas"][k]), int(p["nenv"][k])
+        m = Mole.__new__(Mole)
+        m.basis, m.unit, m.charge, m.spin = p["basis"][k], p["unit"][k], int(p["charge"][k]), 0
+        m.coords = p["coords"][a0:a0 + na]
+        m.charges = p["charges"][a0:a0 + na]
+        m.symbols = [SYMBOLS[int(z)] for z in m.charges]
+        m.natm, m.nbas = na, nb
+        m._atm = p["atm"][a0:a0 + na]
+        m._bas = p["bas"][b0:b0 + nb]
+        m._env = p["env"][e0:e0 + ne]
+        m.ao_loc = p["ao_loc"][b0 + k:b0 + k + nb + 1]
+        out.append(m)
+        a0, b0, e0 = a0 + na, b0 + nb, e0 + ne
+    return out
+
+
 def build_mol(mol_str, basis_name="sto-3g", unit="Angstrom"):
     """Drop-in for ``build_mol`` (nanoDFT.py:543-546)."""
     return Mole(mol_str, basis=basis_name, unit=unit)

@@ -40,6 +40,7 @@ import torch
 
 from .constants import HARTREE_TO_EV
 from .engine import run_batches
+from .mole import pack_moles, unpack_moles
 from .molgen import stream_chunk
 
 QM1B_COLUMNS = ("smile", "atoms", "z", "energy", "homo", "lumo", "N", "std", "y", "pos")
@@ -66,9 +67,16 @@ def _low_priority():
 
 
 def prepare_chunk(args):
-    """worker: molecules of one chunk of the stream with their static columns"""
+    """worker: molecules of one chunk of the stream with their static columns; the molecules
+    travel packed (``unpack_chunk`` on the receiving side)"""
     items = stream_chunk(args)
-    return [(i, s, m, static_columns(i, m, args[0])) for i, s, m in items]
+    return [(i, s, static_columns(i, m, args[0])) for i, s, m in items], pack_moles([m for _, _, m in items])
+
+
+def unpack_chunk(chunk):
+    """(index, atom string, Mole, static columns) per molecule of a chunk from ``prepare_chunk``"""
+    meta, packed = chunk
+    return [(i, s, m, st) for (i, s, st), m in zip(meta, unpack_moles(packed))]
 
 
 def batch_rows(items, res, seed):
@@ -180,7 +188,7 @@ def run_stream(n_total, batch=4096, seed=0, level=0, precision="mixed", guess="l
                 parts = pending.pop(0)
                 if k + 2 < len(chunks):
                     pending.append(submit(chunks[k + 2]))
-                ready.put([x for p in parts for x in p.get()])
+                ready.put([x for p in parts for x in unpack_chunk(p.get())])
         except Exception as e:          # surfaced by the main loop
             err.append(e)
         ready.put(None)

@@ -195,3 +195,19 @@ def test_run_batches_empty_and_plan_errors(monkeypatch):
         for mols, _ in engine.run_batches(iter([[0], [1], [2], [3]]), guess="minao"):
             got.append(mols[0])
     assert got == [0, 1]     # the batches before the failing plan are all delivered
+
+
+def test_packed_chunk_round_trip():
+    """molecules sent packed between processes come back with identical arrays and accessors"""
+    import pickle
+    from b200dft.stream import prepare_chunk, unpack_chunk, static_columns
+    args = (5, 0, 7, 6)
+    ref = stream_chunk(args)
+    got = unpack_chunk(pickle.loads(pickle.dumps(prepare_chunk(args))))
+    assert [g[0] for g in got] == [r[0] for r in ref] and [g[1] for g in got] == [r[1] for r in ref]
+    for (i, s, m, st), (_, _, r) in zip(got, ref):
+        for name in ("coords", "charges", "_atm", "_bas", "_env", "ao_loc"):
+            np.testing.assert_array_equal(getattr(m, name), getattr(r, name))
+        assert (m.symbols, m.natm, m.nbas, m.nao, m.nelectron, m.basis, m.charge) == \
+            (r.symbols, r.natm, r.nbas, r.nao, r.nelectron, r.basis, r.charge)
+        assert m.energy_nuc() == r.energy_nuc() and st == static_columns(i, r, args[0])
