@@ -129,3 +129,11 @@ def test_dft_dropin_refuses_work_skipping_switches():
         args = types.SimpleNamespace(xc="b3lyp", its=2, level=0, float32=False, skipdiis=False, **{flag: True})
         with pytest.raises(ValueError, match=flag):
             dft.density_functional_theory(None, args)
+
+
+def test_double_factorial_known_values():
+    # the reference's known answers for factorial2 (test/test_special.py:27-34); the grid's
+    # sphere moments are built from this function
+    from b200dft.grids import _dfact
+    assert [_dfact(n) for n in range(1, 9)] == [1, 2, 3, 8, 15, 48, 105, 384]
+    assert _dfact(0) == 1 and _dfact(-1) == 1
