@@ -196,8 +196,9 @@ int b2_eri_threshold(b2_plan_t plan, int precision, void *eri, double threshold,
  * `parts`: bit 0 one-electron (kinetic, nuclear attraction, -<dme0, dS>), bit 1 two-electron
  * (Coulomb and hyb-scaled exchange), bit 2 exchange-correlation (B3LYP on coords / weights, the
  * layout registered with b2_grid_set), bit 3 nuclear repulsion; 15 = the full gradient.
- * hyb: exact-exchange fraction (0.2 for B3LYP).  The first call on a plan that has not built
- * its float32 ERI work list builds it and synchronises `stream` (not capturable then). */
+ * hyb: exact-exchange fraction (0.2 for B3LYP).  Not for graph capture: the exchange-correlation
+ * part copies a small host table per call, and the first call on a plan that has not built its
+ * float32 ERI work list builds it, synchronising `stream`. */
 int b2_grad(b2_plan_t plan, int parts, double hyb, const double *C, const double *mo_energy,
             const double *coords, const double *weights, double *D, double *W, double *grad,
             void *stream);
