@@ -69,22 +69,6 @@ def test_nanodft_dropin(cuda):
     assert hl[-1] > 0 and len(w) == len(coords)
 
 
-def test_nanodft_thresholds(cuda):
-    """ao_threshold and eri_threshold (nanoDFT.py:221-230, 280-288) against the oracle SCF on the
-    same thresholded AO values, grid and ERIs"""
-    thr_ao, thr_eri = 1e-2, 1e-6
-    opts, mol_str = nanodft.nanoDFT_options(its=12, mol_str="water", level=0, ao_threshold=thr_ao,
-                                            eri_threshold=thr_eri)
-    mol = nanodft.build_mol(mol_str, opts.basis)
-    E, (logged, hl, mo_e, mo_c, coords, w) = nanodft.nanoDFT(mol, opts)
-    s = HostSetup(mol, 0, ao_threshold=thr_ao)
-    assert len(w) == len(s.weights) < len(HostSetup(mol, 0).weights)
-    s8 = oeri.eri_s8(mol)
-    s8[np.abs(s8) <= thr_eri] = 0.0
-    ref = rks.scf(s.S, s.T, s.V, s.D0, s8, s.ao, s.weights, mol.nelectron // 2, s.E_nuc, its=12)
-    np.testing.assert_allclose(E[:, 0] / HARTREE_TO_EV, ref["energies"][:, 0], atol=1e-6)
-
-
 def test_dft_dropin(cuda):
     args = dft.get_args(["-its", "10", "-level", "0"])
     m = Mole(methane())
@@ -170,3 +154,19 @@ def test_config2_level3_per_precision(cuda, precision):
         assert np.abs(E - g["energies"][:, 0]).max() <= 1e-6          # every iteration
     else:
         assert abs(E[-1] - g["energies"][-1, 0]) <= 1e-4              # north-star: 0.1 mHa
+
+
+def test_nanodft_thresholds(cuda):
+    """ao_threshold and eri_threshold (nanoDFT.py:221-230, 280-288) against the oracle SCF on the
+    same thresholded AO values, grid and ERIs"""
+    thr_ao, thr_eri = 1e-2, 1e-6
+    opts, mol_str = nanodft.nanoDFT_options(its=12, mol_str="water", level=0, ao_threshold=thr_ao,
+                                            eri_threshold=thr_eri)
+    mol = nanodft.build_mol(mol_str, opts.basis)
+    E, (logged, hl, mo_e, mo_c, coords, w) = nanodft.nanoDFT(mol, opts)
+    s = HostSetup(mol, 0, ao_threshold=thr_ao)
+    assert len(w) == len(s.weights) < len(HostSetup(mol, 0).weights)
+    s8 = oeri.eri_s8(mol)
+    s8[np.abs(s8) <= thr_eri] = 0.0
+    ref = rks.scf(s.S, s.T, s.V, s.D0, s8, s.ao, s.weights, mol.nelectron // 2, s.E_nuc, its=12)
+    np.testing.assert_allclose(E[:, 0] / HARTREE_TO_EV, ref["energies"][:, 0], atol=1e-6)
