@@ -151,12 +151,16 @@ def stream_molecule(seed, index, max_heavy=9):
 
 
 def stream_chunk(args):
-    """(index, atom string, Mole) for molecules [start, start + n) of the stream; run in worker
-    processes (this module imports numpy only)"""
+    """(index, atom string, Mole) for molecules [start, start + n) of the stream, less the indices
+    in an optional fifth element (molecules already written); run in worker processes (this
+    module imports numpy only)"""
     from .mole import Mole
-    seed, start, n, max_heavy = args
+    seed, start, n, max_heavy = args[:4]
+    skip = set(args[4]) if len(args) > 4 else ()
     out = []
     for i in range(start, start + n):
+        if i in skip:
+            continue
         s = stream_molecule(seed, i, max_heavy)
         out.append((i, s, Mole(s)))
     return out

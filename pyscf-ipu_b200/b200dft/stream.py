@@ -66,6 +66,27 @@ def _low_priority():
         pass
 
 
+def done_indices(path, fmt, seed):
+    """indices of the molecules of stream ``seed`` whose rows ``path`` already holds (from the
+    rows' identifiers gen:<seed>:<index>:<formula>); the reference's generation loop skips the
+    molecules found in its output folder the same way (dft.py:247-283, option -resume)"""
+    import os
+    if not path or not os.path.exists(path):
+        return set()
+    if fmt == "parquet":
+        import pyarrow.parquet as pq
+        smiles = pq.read_table(path, columns=["smile"]).column("smile").to_pylist()
+    else:
+        import pandas as pd
+        smiles = pd.read_csv(path, compression="gzip", usecols=["smile"])["smile"].tolist()
+    out = set()
+    for s in smiles:
+        p = str(s).split(":")
+        if len(p) >= 3 and p[0] == "gen" and p[1] == str(seed):
+            out.add(int(p[2]))
+    return out
+
+
 def prepare_chunk(args):
     """worker: molecules of one chunk of the stream with their static columns; the molecules
     travel packed (``unpack_chunk`` on the receiving side)"""
@@ -118,10 +139,18 @@ def batch_rows(items, res, seed):
 class RowWriter:
     """Appends batches of rows to a Parquet file (QM1B schema) or a gzip CSV (reference schema)."""
 
-    def __init__(self, path, fmt="parquet", basis="sto-3g"):
+    def __init__(self, path, fmt="parquet", basis="sto-3g", append=False):
+        import os
         self.path, self.fmt, self.basis = path, fmt, basis
         self._pq = None
         self._first = True
+        self._prior = None                    # rows already in a Parquet file being appended to
+        if append and path and os.path.exists(path):
+            if fmt == "parquet":
+                import pyarrow.parquet as pq
+                self._prior = pq.read_table(path)
+            else:
+                self._first = False           # gzip CSV: append members, no second header
 
     def write(self, cols):
         if self.path is None:
@@ -132,6 +161,12 @@ class RowWriter:
             keep = QM1B_COLUMNS + ("iterations", "converged") + (("gradient",) if "gradient" in cols else ())
             t = pa.table({k: cols[k] for k in keep})
             if self._pq is None:
+                if self._prior is not None:
+                    # a Parquet file cannot be appended in place: rewrite its rows first
+                    if self._prior.schema.names != t.schema.names:
+                        raise ValueError(f"{self.path} has columns {self._prior.schema.names}, new rows {t.schema.names}")
+                    t = pa.concat_tables([self._prior.cast(t.schema), t])
+                    self._prior = None
                 self._pq = pq.ParquetWriter(self.path, t.schema)
             self._pq.write_table(t)
         else:
@@ -147,6 +182,7 @@ class RowWriter:
             self._first = False
 
     def close(self):
+        self._prior = None                           # nothing new written: the file is untouched
         if self._pq is not None:
             self._pq.close()
             self._pq = None
@@ -154,31 +190,45 @@ class RowWriter:
 
 def run_stream(n_total, batch=4096, seed=0, level=0, precision="mixed", guess="learned", out=None,
                fmt="parquet", workers=None, max_heavy=9, net=None, e_tol=1e-6, diis_tol=1e-4,
-               rank=0, world=1, gradient=False):
+               rank=0, world=1, gradient=False, resume=False):
     """Generate ``n_total`` molecules and write one row each; returns throughput and iteration
     statistics (the streaming configuration: molecules/s, p50/p99 iterations).  With
     ``world`` > 1 this process handles the stream chunks of ``rank`` (round robin) only.  With
     ``gradient`` each row also carries the molecule's nuclear gradient (force labels, dE/dR in
-    Ha/Bohr, flattened like ``pos``; nanoDFT.py:440-477 on the SCF's final orbitals)."""
+    Ha/Bohr, flattened like ``pos``; nanoDFT.py:440-477 on the SCF's final orbitals).  With
+    ``resume`` the molecules whose rows ``out`` already holds are not generated again and the new
+    rows are appended (dft.py:247-283)."""
     if guess == "learned" and net is None:
         from .train_guess import load
         net = load()
     workers = workers or max(1, min(16, (os.cpu_count() or 2) - 1))
     from .shard import shard_indices
     chunks = [(seed, s, min(batch, n_total - s), max_heavy) for s in shard_indices(n_total, batch, rank, world)]
+    skipped = 0
+    if resume:
+        done_idx = np.array(sorted(done_indices(out, fmt, seed)), np.int64)
+        kept = []
+        for c in chunks:
+            lo, hi = np.searchsorted(done_idx, [c[1], c[1] + c[2]])
+            skipped += int(hi - lo)
+            if hi - lo < c[2]:                    # chunks fully written are not generated again
+                kept.append(c + (tuple(int(i) for i in done_idx[lo:hi]),))
+        chunks = kept
     ctx = mp.get_context("spawn")
     pool = ctx.Pool(workers, initializer=_low_priority)
     ready = queue.Queue(maxsize=2)        # generated batches waiting for the GPU
     done = queue.Queue(maxsize=4)         # finished batches waiting for the writer
-    writer = RowWriter(out, fmt)
+    writer = RowWriter(out, fmt, append=resume)
     stats = {"iterations": [], "converged": 0, "batches": 0, "gpu_s": 0.0}
     err = []
 
     def submit(c):
-        # one batch split over every worker
-        seed_, start, n, mh = c
+        # one batch split over every worker (with the indices each piece skips, if resuming)
+        seed_, start, n, mh = c[:4]
+        skip = c[4] if len(c) > 4 else ()
         step = max(1, -(-n // workers))
-        return [pool.apply_async(prepare_chunk, ((seed_, s0, min(step, start + n - s0), mh),))
+        return [pool.apply_async(prepare_chunk, ((seed_, s0, min(step, start + n - s0), mh,
+                                                  tuple(i for i in skip if s0 <= i < s0 + step)),))
                 for s0 in range(start, start + n, step)]
 
     def produce():
@@ -249,7 +299,7 @@ def run_stream(n_total, batch=4096, seed=0, level=0, precision="mixed", guess="l
             "p50_iterations": float(np.percentile(its_c, 50)) if len(its_c) else None,
             "p99_iterations": float(np.percentile(its_c, 99)) if len(its_c) else None,
             "mean_iterations": float(its_c.mean()) if len(its_c) else None,
-            "workers": workers, "out": out, "format": fmt}
+            "workers": workers, "out": out, "format": fmt, "skipped_already_written": skipped}
 
 
 def main(argv=None):
@@ -264,10 +314,11 @@ def main(argv=None):
     ap.add_argument("--format", default=None, choices=["parquet", "csv"])
     ap.add_argument("--workers", type=int, default=None)
     ap.add_argument("--gradient", action="store_true", help="also write each molecule's nuclear gradient")
+    ap.add_argument("--resume", action="store_true", help="skip the molecules whose rows --out already holds")
     a = ap.parse_args(argv)
     fmt = a.format or ("csv" if a.out and a.out.endswith((".csv", ".csv.gz", ".gz")) else "parquet")
     r = run_stream(a.n, batch=a.batch, seed=a.seed, level=a.level, precision=a.precision, guess=a.guess,
-                   out=a.out, fmt=fmt, workers=a.workers, gradient=a.gradient)
+                   out=a.out, fmt=fmt, workers=a.workers, gradient=a.gradient, resume=a.resume)
     print(json.dumps(r))
     return r
 

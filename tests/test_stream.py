@@ -211,3 +211,36 @@ def test_packed_chunk_round_trip():
         assert (m.symbols, m.natm, m.nbas, m.nao, m.nelectron, m.basis, m.charge) == \
             (r.symbols, r.natm, r.nbas, r.nao, r.nelectron, r.basis, r.charge)
         assert m.energy_nuc() == r.energy_nuc() and st == static_columns(i, r, args[0])
+
+
+def _stub_run_batches(batches, **kw):
+    for mols in batches:
+        n = len(mols)
+        mo = np.zeros((n, 72))
+        mo[:, :2] = [-0.5, 0.1]
+        yield mols, {"energy": np.full(n, -40.0), "iterations": np.full(n, 6, np.int32),
+                     "converged": np.ones(n, bool), "mo_energy": mo, "last5": np.full((n, 5), -40.0),
+                     "diis_err": np.zeros(n), "its_run": 6, "host_ms": {"engine": 0.0, "prepare": 0.0, "scf": 0.0}}
+
+
+@pytest.mark.parametrize("fmt", ["parquet", "csv"])
+def test_stream_resume_skips_written_molecules(tmp_path, monkeypatch, fmt):
+    """the engine stubbed out: a stream stopped after 7 molecules and resumed to 12 writes every
+    molecule once (dft.py:247-283, -resume)"""
+    import pandas as pd
+    from b200dft import stream
+    monkeypatch.setattr(stream, "run_batches", _stub_run_batches)
+    path = str(tmp_path / ("rows.parquet" if fmt == "parquet" else "rows.csv.gz"))
+    kw = dict(batch=5, seed=3, guess="minao", out=path, fmt=fmt, workers=2)
+    r1 = stream.run_stream(7, **kw)
+    assert r1["molecules"] == 7 and r1["skipped_already_written"] == 0
+    r2 = stream.run_stream(12, resume=True, **kw)
+    assert r2["molecules"] == 5 and r2["skipped_already_written"] == 7
+    if fmt == "parquet":
+        smiles = pd.read_parquet(path)["smile"].tolist()
+    else:
+        smiles = pd.read_csv(path, compression="gzip")["smile"].tolist()
+    assert sorted(int(s.split(":")[2]) for s in smiles) == list(range(12))
+    assert stream.done_indices(path, fmt, 3) == set(range(12)) and stream.done_indices(path, fmt, 4) == set()
+    r3 = stream.run_stream(12, resume=True, **kw)            # nothing left to do
+    assert r3["molecules"] == 0 and r3["skipped_already_written"] == 12
