@@ -244,3 +244,26 @@ def test_stream_resume_skips_written_molecules(tmp_path, monkeypatch, fmt):
     assert stream.done_indices(path, fmt, 3) == set(range(12)) and stream.done_indices(path, fmt, 4) == set()
     r3 = stream.run_stream(12, resume=True, **kw)            # nothing left to do
     assert r3["molecules"] == 0 and r3["skipped_already_written"] == 12
+
+
+@pytest.mark.gpu
+def test_stream_force_labels_match_engine(tmp_path):
+    """force labels (run_stream(gradient=True)): each row's gradient equals the batched engine's
+    gradient of the same molecule (float64 SCF, one batch of the same molecules)"""
+    pq = pytest.importorskip("pyarrow.parquet")
+    from b200dft.engine import RKSEngine
+    path = str(tmp_path / "f.parquet")
+    r = run_stream(12, batch=6, seed=5, guess="minao", precision="fp64", out=path, workers=2, max_heavy=4,
+                   gradient=True)
+    assert r["molecules"] == 12 and r["converged"] == 12
+    t = pq.read_table(path).to_pydict()
+    mols = [m for _, _, m in stream_chunk((5, 0, 12, 4))]
+    eng = RKSEngine(mols, level=0, precision="fp64", guess="minao")
+    eng.run_converged()
+    g = eng.gradient().cpu().numpy()
+    eng.close()
+    a0 = 0
+    for k, m in enumerate(mols):
+        assert len(t["gradient"][k]) == 3 * m.natm
+        np.testing.assert_allclose(np.array(t["gradient"][k]).reshape(-1, 3), g[a0:a0 + m.natm], atol=1e-6, rtol=0)
+        a0 += m.natm
