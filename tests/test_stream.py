@@ -249,7 +249,7 @@ def test_stream_resume_skips_written_molecules(tmp_path, monkeypatch, fmt):
 @pytest.mark.gpu
 def test_stream_force_labels_match_engine(tmp_path):
     """force labels (run_stream(gradient=True)): each row's gradient equals the batched engine's
-    gradient of the same molecule (float64 SCF, one batch of the same molecules)"""
+    gradient of the same molecule (float64 SCF, the same two batches run directly)"""
     pq = pytest.importorskip("pyarrow.parquet")
     from b200dft.engine import RKSEngine
     path = str(tmp_path / "f.parquet")
@@ -257,11 +257,15 @@ def test_stream_force_labels_match_engine(tmp_path):
                    gradient=True)
     assert r["molecules"] == 12 and r["converged"] == 12
     t = pq.read_table(path).to_pydict()
-    mols = [m for _, _, m in stream_chunk((5, 0, 12, 4))]
-    eng = RKSEngine(mols, level=0, precision="fp64", guess="minao")
-    eng.run_converged()
-    g = eng.gradient().cpu().numpy()
-    eng.close()
+    mols, gs = [], []
+    for start in (0, 6):                      # the stream's two batches, run directly
+        mb = [m for _, _, m in stream_chunk((5, start, 6, 4))]
+        eng = RKSEngine(mb, level=0, precision="fp64", guess="minao")
+        eng.run_converged()
+        gs.append(eng.gradient().cpu().numpy())
+        eng.close()
+        mols += mb
+    g = np.concatenate(gs)
     a0 = 0
     for k, m in enumerate(mols):
         assert len(t["gradient"][k]) == 3 * m.natm
