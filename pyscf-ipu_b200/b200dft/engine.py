@@ -417,15 +417,6 @@ class RKSEngine:
         out["C"] = self.C.cpu().numpy()
         return out
 
-    def _capture(self, use_diis):
-        g = torch.cuda.CUDAGraph()
-        s = torch.cuda.Stream()
-        s.wait_stream(torch.cuda.current_stream())
-        with torch.cuda.stream(s):
-            self.step(use_diis)                       # warm-up launch outside capture
-        torch.cuda.current_stream().wait_stream(s)
-        return g
-
     def run_converged(self, max_its=40, e_tol=1e-6, diis_tol=1e-4, use_diis=True, graph=True,
                       check_every=1, fallback=True, rise=3.0, fallback_window=5, tail=0.25):
         """Iterate until each molecule's |E_i - E_{i-1}| < e_tol and DIIS error < diis_tol, then

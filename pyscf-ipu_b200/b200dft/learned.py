@@ -172,21 +172,6 @@ class GuessNet:
         t = self.grads if grad else self.params
         return t[o:o + int(np.prod(s))].view(*s)
 
-    def load_numpy(self, p):
-        self.params.copy_(torch.from_numpy(np.concatenate([np.asarray(p[n], np.float32).reshape(-1)
-                                                           for n, _ in self.shapes])).to(self.device))
-
-    def state_dict(self):
-        return {"params": self.params.cpu().numpy(), "m": self.m.cpu().numpy(), "v": self.v.cpu().numpy(),
-                "step": self.step_count}
-
-    def load_state_dict(self, d):
-        self.params.copy_(torch.from_numpy(d["params"]).to(self.device))
-        if "m" in d:
-            self.m.copy_(torch.from_numpy(d["m"]).to(self.device))
-            self.v.copy_(torch.from_numpy(d["v"]).to(self.device))
-            self.step_count = int(d.get("step", 0))
-
     # ---- primitives ------------------------------------------------------------------------
     def _mm(self, X, W, bias=None, out=None, beta=0.0):
         """out = X @ W (+ bias), X (M,K) row-major, W (K,N) row-major"""
