@@ -1,10 +1,25 @@
-// Shell-quartet ERI evaluation: one thread computes every component (i j | k l) of one bra
-// shell pair IJ against one ket shell pair KL of a fixed angular class.  Same formulation as
-// eri_math.cuh (Hermite/derivative form, d_c f_n = X_c f_{n+1}); the primitive-quartet
+// Two-electron integrals (ij|kl) for s/p Gaussians.
+//
+// Formulation (this project's own, from the McMurchie-Davidson Hermite expansion):
+// every s/p bra factor (r-A)_a = (r-P)_a + PA_a, and (r-P)_a exp(-zeta|r-P|^2) =
+// (1/2zeta) d/dP_a exp(...), so a primitive bra pair is a short polynomial in
+// derivatives with respect to P:
+//   E0 + Ea d_alpha + Eb d_beta + Eab d_alpha d_beta
+//   (E0 = sa sb + [a.b] u, Ea = sb u, Eb = sa u, Eab = u^2, u = 1/(2 zeta),
+//    sa = PA.alpha or 1 for s, sb = PB.beta or 1 for s);
+// the ket likewise with u -> v = 1/(2 eta), derivatives taken w.r.t. Q = -X.
+// Derivatives of the base integral f_0(X) = pref F_0(rho |X|^2) follow from
+// d_c f_n = X_c f_{n+1}, f_n = pref (-2 rho)^n F_n(rho X^2), which gives closed forms for
+// every bra/ket combination (the f[n] and g terms below).  The reference computes the same
+// integrals by Rys quadrature (int2e_sph.cpp:1785-1892, 2452-2719); results agree to
+// rounding.
+//
+// Shell-quartet evaluation: one thread computes every component (i j | k l) of one bra shell
+// pair IJ against one ket shell pair KL of a fixed angular class; the primitive-quartet
 // quantities (Boys values, X = P - Q, prefactor) are computed once per primitive quartet and
-// shared by all components, instead of once per bra AO pair.
+// shared by all components.
 #pragma once
-#include "eri_math.cuh"
+#include "boys.cuh"
 #include "plan_host.hpp"
 
 // CI < 0: all bra i components in this thread; CI >= 0: only component CI (float64 form

@@ -1,8 +1,7 @@
-// Test-only host build of the device math (ERI row items, Boys function, B3LYP point
-// functional).  It runs the exact __host__ __device__ code the kernels run, on the CPU, so
+// Test-only host build of the device math (ERI shell quartets, Boys function, B3LYP point
+// functional, gradient terms).  It runs the exact __host__ __device__ code the kernels run, on the CPU, so
 // the CPU test suite can check the kernel arithmetic against the oracle without a GPU.
 // It is never loaded by the product path (libb200dft.so has no CPU fallback).
-#include "eri_row.cuh"
 #include "eri_sq.cuh"
 #include "grad_math.cuh"
 #include "xc_math.cuh"
