@@ -80,10 +80,6 @@ k_nn_gemm(int M, int N, int K, const float *__restrict__ A, long long sai, long 
 #define TC_BN 128
 #define TC_BK 32
 #define TC_LD (TC_BK + 8)
-__device__ __forceinline__ unsigned b2_pack_bf16(float lo, float hi) {
-  const __nv_bfloat16 a = __float2bfloat16_rn(lo), b = __float2bfloat16_rn(hi);
-  return (unsigned)__bfloat16_as_ushort(a) | ((unsigned)__bfloat16_as_ushort(b) << 16);
-}
 
 __global__ void __launch_bounds__(256)
 k_nn_gemm_tc(int M, int N, int K, const float *__restrict__ A, long long sai, long long sak,

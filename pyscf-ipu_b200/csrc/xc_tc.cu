@@ -103,16 +103,6 @@ __device__ __forceinline__ bool b2_mbar_wait(uint32_t a, uint32_t parity) {
   }
   return false;
 }
-__device__ __forceinline__ void b2_tmem_ld8(uint32_t ta, float *v) {
-  uint32_t r[8];
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
-                 "=r"(r[6]), "=r"(r[7])
-               : "r"(ta));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(r[i]);
-}
 __device__ __forceinline__ void b2_tmem_st4(uint32_t ta, float a, float b, float c, float d) {
   asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1,%2,%3,%4};"
                :: "r"(ta), "r"(__float_as_uint(a)), "r"(__float_as_uint(b)),
@@ -125,10 +115,6 @@ __device__ __forceinline__ float b2_ex2(float x) {     // 2^x (approximate; AO v
 }
 __device__ __forceinline__ void b2_tmem_wait_st() {
   asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
-}
-__device__ __forceinline__ void b2_split(float x, float &hi, float &lo) {
-  hi = __uint_as_float(__float_as_uint(x) & 0xFFFFE000u);
-  lo = x - hi;
 }
 __device__ __forceinline__ void b2_st4(float *p, float a, float b, float c, float d) {
   *reinterpret_cast<float4 *>(p) = make_float4(a, b, c, d);
