@@ -434,6 +434,9 @@ def main():
         v, dt, _ = cpu_baseline(atoms, a.level, oeri.ref_available())
         cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "reference" if oeri.ref_available() else "port",
                "sample": f"first {a.cpu_sample} molecules of the batch, 20 SCF iterations, FP64, 1 core ({dt:.1f}s)"}
+        from b200dft.mole import methane
+        _, dt1, _ = cpu_baseline([methane()], a.level, oeri.ref_available())
+        cpu["ch4_s_per_molecule"] = dt1          # the CPU-runnable single-molecule case, same path
 
     # e2e through the public batch API (b200dft.engine.run_batches): every step builds a plan
     # from the host libcint arrays (tables staged in pinned host memory and copied to the
