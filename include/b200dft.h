@@ -208,14 +208,18 @@ int b2_grad(b2_plan_t plan, int parts, double hyb, const double *C, const double
 int b2_int2e_sph_s8(const int *atm, int natm, const int *bas, int nbas, const double *env,
                     int n_env, int precision, void *eri_out, void *stream);
 
-/* Allocation-free variant of b2_int2e_sph_s8 (no counterpart in the reference).  For callers
- * that cannot allocate device memory -- work being captured into a CUDA graph, processes whose
- * device memory belongs to another allocator or a fixed-budget pool, loops that must not block
- * in an allocator.  Its tables live in a 2.5 MiB static device array that every GPU loading the
- * library keeps until exit.  Limits: nbas <= 48 shells, nao <= 70 (B2_ERR_SIZE beyond).  All
- * calls share that array, so calls that overlap on the GPU (other streams, other host threads)
- * race; calls on one stream are ordered.  The first call on a device must be made with that
- * device current and, if graph capture is used, before capture begins. */
+/* Allocation-free single-molecule ERI entry (no counterpart in the reference).  For callers
+ * that must not call cudaMalloc: processes whose device memory is handed out by another
+ * allocator or a fixed-budget pool, and loops with a latency budget (cudaMalloc/cudaFree can
+ * block and synchronise the device).  Same inputs and s8 output as b2_int2e_sph_s8, but the
+ * tables live in a 2.5 MiB static device array that every GPU loading the library keeps until
+ * exit.  Limits: nbas <= 48 shells, nao <= 70 (B2_ERR_SIZE beyond).  Unlike b2_int2e_sph_s8 it
+ * does not synchronise: the output is ready, and kernel errors show, only after the caller
+ * synchronises `stream`.  All calls share the static array and a static host staging buffer:
+ * calls from several host threads must be serialised by the caller, and calls whose work
+ * overlaps on the GPU (different streams) race; calls on one stream are ordered.  The first
+ * call on a device looks up the array's address with that device current; make it before any
+ * stream capture. */
 int b2_int2e_sph_s8_noalloc(const int *atm, int natm, const int *bas, int nbas, const double *env,
                             int n_env, int precision, void *eri_out, void *stream);
 

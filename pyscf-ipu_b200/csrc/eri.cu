@@ -405,18 +405,22 @@ int b2_launch_eri_s8(B2PlanDev &P, int precision, void *out, cudaStream_t st) {
 // ============================================================================================
 // Allocation-free single-molecule ERI entry (b2_int2e_sph_s8_noalloc).
 //
-// For callers that cannot allocate device memory: code running while a CUDA stream is being
-// captured into a graph (allocation is not a capturable operation), processes whose device
-// memory is entirely owned by another allocator or memory pool with a fixed budget, and
-// latency-critical loops that must not block in the allocator.  The per-molecule tables the
-// ERI kernels read (molecule descriptor, shell-pair primitive data, class lists, work list,
-// Boys table) live in one file-scope __device__ array of B2_NOALLOC_BYTES (2.5 MiB) that every
-// GPU loading this library keeps until the process exits; host staging uses a static buffer of
-// the same size.  Limits: nbas <= 48 shells, nao <= 70, s/p shells with <= 3 primitives.
-// The s8 output is written completely, so no part of the array has to start at zero.  All calls
-// share the array: calls whose work overlaps on the GPU (different streams, or different host
-// threads) race; calls on one stream are ordered.  The first call on a device looks up the
-// array's device address (cudaGetSymbolAddress) with that device current.
+// For callers that must not call cudaMalloc: processes whose device memory is handed out by
+// another allocator or a pool with a fixed budget (a cudaMalloc there would fail or take memory
+// the pool has promised elsewhere), and loops with a latency budget, where cudaMalloc/cudaFree
+// can block and synchronise the device.  The per-molecule tables the ERI kernels read (molecule
+// descriptor, shell-pair primitive data, class lists, work list, Boys table) live in one
+// file-scope __device__ array of B2_NOALLOC_BYTES (2.5 MiB) that every GPU loading this library
+// keeps until the process exits; the host side fills a static buffer of the same size and copies
+// it with one cudaMemcpyAsync (pageable source: the copy has left the buffer when the call
+// returns).  Limits: nbas <= 48 shells, nao <= 70, s/p shells with <= 3 primitives.  The s8
+// output is written completely, so no part of the array has to start at zero.
+// The call is asynchronous on `stream`: the output is ready, and kernel faults are reported,
+// only once the caller synchronises that stream.  All calls share the device array and the
+// host staging buffer: calls from several host threads must be serialised by the caller, and
+// calls whose work overlaps on the GPU (different streams) race; calls on one stream are
+// ordered.  The first call on a device looks up the array's device address
+// (cudaGetSymbolAddress) with that device current; make it before any stream capture.
 #define B2_NOALLOC_MAXBAS 48
 #define B2_NOALLOC_MAXSP (B2_NOALLOC_MAXBAS * (B2_NOALLOC_MAXBAS + 1) / 2)
 #define B2_NOALLOC_MAXTASK (B2_NOALLOC_MAXSP * 42)
@@ -448,13 +452,6 @@ extern "C" int b2_int2e_sph_s8_noalloc(const int *atm, int natm, const int *bas,
   if (!atm || !bas || !env || !eri_out || natm <= 0 || nbas <= 0 || n_env <= 0) return B2_ERR_ARG;
   if (precision != 64 && precision != 32) return B2_ERR_ARG;
   if (nbas > B2_NOALLOC_MAXBAS) return B2_ERR_SIZE;
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return B2_ERR_CUDA;
-  if (!g_b2_noalloc_dev[dev]) {
-    void *p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_b2_noalloc_scratch) != cudaSuccess || !p) return B2_ERR_CUDA;
-    g_b2_noalloc_dev[dev] = (unsigned char *)p;
-  }
   unsigned char *H = g_b2_noalloc_stage;
   // ---- host tables in the static staging buffer (same layout as the device array) ----
   const size_t o_mol = 0;
@@ -475,7 +472,8 @@ extern "C" int b2_int2e_sph_s8_noalloc(const int *atm, int natm, const int *bas,
     if (l > B2_MAXL || np < 1 || np > B2_MAXPRIM || b[B2_NCTR_OF] != 1) return B2_ERR_UNSUPPORTED;
     if (ia < 0 || ia >= natm) return B2_ERR_ARG;
     const int pc = atm[ia * B2_ATM_SLOTS + B2_PTR_COORD];
-    if (pc < 0 || pc + 3 > n_env || b[B2_PTR_EXP] + np > n_env || b[B2_PTR_COEFF] + np > n_env)
+    if (pc < 0 || pc + 3 > n_env || b[B2_PTR_EXP] < 0 || b[B2_PTR_COEFF] < 0 ||
+        b[B2_PTR_EXP] + np > n_env || b[B2_PTR_COEFF] + np > n_env)
       return B2_ERR_ARG;
     memset(&S[s], 0, sizeof(B2Shell));
     for (int d = 0; d < 3; ++d) S[s].R[d] = env[pc + d];
@@ -546,6 +544,14 @@ extern "C" int b2_int2e_sph_s8_noalloc(const int *atm, int natm, const int *bas,
     for (int i = 0; i < B2_BOYS_NT * B2_BOYS_NM; ++i) bf[i] = (float)bd[i];   // in place, ascending
   }
   // ---- stage to the device array and launch (no device allocation anywhere) ----
+  // arguments are all checked above, before any CUDA call; first call on a device: set-up
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return B2_ERR_CUDA;
+  if (!g_b2_noalloc_dev[dev]) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_b2_noalloc_scratch) != cudaSuccess || !p) return B2_ERR_CUDA;
+    g_b2_noalloc_dev[dev] = (unsigned char *)p;
+  }
   unsigned char *Dv = g_b2_noalloc_dev[dev];
   cudaStream_t st = (cudaStream_t)stream;
   if (cudaMemcpyAsync(Dv, H, total, cudaMemcpyHostToDevice, st) != cudaSuccess) return B2_ERR_CUDA;

@@ -38,3 +38,26 @@ def test_no_cpu_fallback():
     from b200dft._lib import B200DFTError
     with pytest.raises(B200DFTError):
         RKSEngine([Mole(methane())])
+
+
+def test_noalloc_rejects_bad_arguments_without_a_gpu():
+    # b2_int2e_sph_s8_noalloc checks its host arguments before any CUDA call: a negative or
+    # out-of-range exponent / coefficient offset is B2_ERR_ARG, too many shells B2_ERR_SIZE
+    import numpy as np
+    from b200dft._lib import lib, ptr
+    from b200dft.mole import Mole, methane
+    m = Mole(methane())
+    env = np.ascontiguousarray(m._env)
+    out = ctypes.c_void_p(16)                 # never dereferenced: every case fails its checks first
+    for slot, value in ((5, -1), (6, -3), (5, len(env))):        # PTR_EXP, PTR_COEFF
+        bas = np.array(m._bas, np.int32)
+        bas[0, slot] = value
+        atm = np.ascontiguousarray(m._atm, np.int32)
+        rc = lib().b2_int2e_sph_s8_noalloc(ptr(atm), m.natm, ptr(bas), m.nbas, ptr(env), len(env), 64,
+                                           out, None)
+        assert rc == -1, (slot, value, rc)
+    big = Mole("; ".join(f"H {x * 1.5} 0 0" for x in range(50)))
+    rc = lib().b2_int2e_sph_s8_noalloc(ptr(np.ascontiguousarray(big._atm, np.int32)), big.natm,
+                                       ptr(np.ascontiguousarray(big._bas, np.int32)), big.nbas,
+                                       ptr(np.ascontiguousarray(big._env)), len(big._env), 64, out, None)
+    assert rc == -4

@@ -1,8 +1,9 @@
 """The allocation-free ERI entry point (b2_int2e_sph_s8_noalloc) against b2_int2e_sph_s8.
 
-Callers that cannot allocate device memory (graph capture, memory owned by another
-allocator, allocation-free loops) use the no-alloc entry; it must give the same s8 list as the
-allocating entry, and keep doing so on consecutive calls that reuse its static device array.
+Callers that must not call cudaMalloc (device memory owned by another allocator or a
+fixed-budget pool, loops where an allocation could block or synchronise the device) use the
+no-alloc entry; it must give the same s8 list as the allocating entry, and keep doing so on
+consecutive calls that reuse its static device array.
 Collected last so that a failure here does not hide the rest of the GPU suite.
 """
 import numpy as np
