@@ -38,11 +38,15 @@ def _peaks():
     return 6650.0, "fallback"
 
 
-def _tensor_peak():
+def _tensor_peak(sustained=True):
+    """bf16 dense peak: the sustained figure for a kernel timed inside a long SCF step"""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
-        return json.load(open(p)).get("bf16_tflops", 1590.0), "measured"
-    return 1590.0, "fallback"
+        d = json.load(open(p))
+        if sustained and "bf16_tflops_sustained" in d:
+            return d["bf16_tflops_sustained"], "measured sustained"
+        return d.get("bf16_tflops", 1590.0), "measured burst"
+    return (1400.0, "fallback sustained") if sustained else (1590.0, "fallback burst")
 
 
 def quartet_counts(mols):
@@ -58,44 +62,67 @@ def quartet_counts(mols):
     return quartets, prim
 
 
-def kernel_figures(eng, precision):
-    """Throughput of the ERI and XC entry points on the resident batch (CUDA events around
-    repeated calls, after one warm-up call): shell quartets/s and primitive quartets/s of the s8
-    ERI generation (b2_eri_s8; float32 SIMT, no measured peak to divide by) and the XC grid
-    products' algorithmic TFLOP/s (b2_xc_direct; 4 G N^2 per molecule: rho and V_xc products)."""
+def _timed(fn, n):
+    """mean CUDA-event time (ms) of n calls on the current stream, after one warm-up call"""
     import torch
+    fn()
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(n):
+        fn()
+    t1.record()
+    torch.cuda.synchronize()
+    return t0.elapsed_time(t1) / n
+
+
+def kernel_rooflines(eng, precision):
+    """Roofline figures of the three kernel families on the resident batch, each timed with
+    CUDA events around repeated calls of the entry the SCF uses (after the timed region, same
+    batch and data):
+      * XC (k_xc_tc, tensor bound): algorithmic flops 4 G N^2 per molecule (the rho and V_xc
+        contractions, N = nao unpadded) against the measured sustained bf16 dense peak; the
+        operands are split tf32 (nominal tf32 rate = half the bf16 rate).
+      * J/K (k_symv, HBM bound): algorithmic bytes n4 x 4 B per molecule (the s8 list read once,
+        D/J/K on chip) against the measured HBM copy rate.
+      * ERI (k_eri_*, float32 SIMT): shell and primitive quartets per second.
+    Returns the list, dominant kernel (largest device-time share) first."""
     from b200dft._lib import lib, check, ptr, stream_handle
     P = eng.plan
-
-    def timed(fn, n):
-        fn()
-        torch.cuda.synchronize()
-        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        t0.record()
-        for _ in range(n):
-            fn()
-        t1.record()
-        torch.cuda.synchronize()
-        return t0.elapsed_time(t1) / n
-
-    quartets, prim = quartet_counts(eng.mols)
-    prec = 64 if precision == "fp64" else 32
-    eri_ms = timed(lambda: check(lib().b2_eri_s8(P.h, prec, ptr(eng.eri), stream_handle()), "b2_eri_s8"), 3)
+    hbm, hbm_kind = _peaks()
+    tpk, tkind = _tensor_peak(sustained=True)
+    rbytes = 4 if precision == "mixed" else 8
+    out = []
     G = np.diff(P.grid_off).astype(np.float64)
     N = P.nao.astype(np.float64)
     flops = float((4.0 * G * N * N).sum())
-    xc_ms = timed(lambda: eng.xc(active=None), 5)
+    xc_ms = _timed(lambda: eng.xc(active=None), 5)
     tf = flops / (xc_ms / 1e3) / 1e12
-    peak, kind = _tensor_peak()
-    return {
-        "eri": {"entry": "b2_eri_s8", "ms_per_call": eri_ms, "shell_quartets": quartets,
-                "primitive_quartets_unscreened": prim, "shell_quartets_per_s": quartets / (eri_ms / 1e3),
-                "primitive_quartets_per_s": prim / (eri_ms / 1e3), "bound": "float32 SIMT compute"},
-        "xc": {"entry": "b2_xc_direct", "ms_per_call": xc_ms, "algorithmic_flops": flops, "tflops": tf,
-               "peak_tflops": peak, "peak_kind": f"{kind} bf16 dense", "frac": tf / peak,
-               "note": "tf32 operands (nominal tf32 peak is half the bf16 peak); AO values are generated on "
-                       "chip, so the kernel also spends CUDA-core time per point"},
-    }
+    out.append({"kernel": "k_xc_tc" if precision == "mixed" else "k_xc_direct", "bound": "tensor",
+                "achieved": tf, "peak": tpk, "unit": "TFLOP/s", "frac": tf / tpk, "traffic": None,
+                "peak_kind": f"{tkind} bf16 dense (of measured)", "algorithmic_flops_per_launch": flops,
+                "ms_per_launch": xc_ms, "operands": "split tf32, fp32 accumulate"})
+    eng.D.copy_(eng.D0)
+    jk_ms = _timed(lambda: eng.jk(active=None), 10)
+    n4 = float(sum(int(n) * (int(n) + 1) // 2 * (int(n) * (int(n) + 1) // 2 + 1) // 2 for n in P.nao))
+    jk_bytes = n4 * rbytes
+    gbs = jk_bytes / (jk_ms / 1e3) / 1e9
+    read = (2 if eng.jk_impl == "pairs" else 1) * P.n_eri * rbytes
+    # DRAM bytes per launch: ncu capture of k_symv on the 256-molecule batch (868.8 MB read +
+    # 6.4 MB written for 860.7 MB of float32 list entries in both lists), scaled by list size
+    traffic = read * (875.2 / 860.7) if (precision == "mixed" and eng.jk_impl == "pairs") else None
+    out.append({"kernel": "k_symv" if eng.jk_impl == "pairs" else "k_jk_s8", "bound": "hbm", "achieved": gbs,
+                "peak": hbm, "unit": "GB/s", "frac": gbs / hbm, "traffic": traffic,
+                "peak_kind": f"{hbm_kind} HBM copy", "algorithmic_bytes_per_launch": jk_bytes,
+                "bytes_read_per_launch": read, "ms_per_launch": jk_ms})
+    quartets, prim = quartet_counts(eng.mols)
+    prec = 64 if precision == "fp64" else 32
+    eri_ms = _timed(lambda: check(lib().b2_eri_s8(P.h, prec, ptr(eng.eri), stream_handle()), "b2_eri_s8"), 3)
+    out.append({"kernel": "k_eri_*", "bound": "fp32 simt", "ms_per_launch": eri_ms,
+                "shell_quartets_per_s": quartets / (eri_ms / 1e3),
+                "primitive_quartets_per_s": prim / (eri_ms / 1e3), "shell_quartets": quartets,
+                "primitive_quartets_unscreened": prim})
+    return out
 
 
 class Clocks:
@@ -214,7 +241,8 @@ def run_reference(a):
                 vals.append(v)
                 t_all += dt
     finally:
-        pool.terminate()
+        pool.close()                     # workers exit normally (their loaded libraries stay visible)
+        pool.join()
     value = float(np.mean(vals))
     kind = "reference" if use_ref else "port"
     sample = (f"{per_step} molecules per step of the batched distribution, 20 SCF iterations, level-{a.level} "
@@ -271,7 +299,7 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--guess", default="learned", choices=["learned", "minao"])
     ap.add_argument("--plain-sample", type=int, default=32)
-    ap.add_argument("--cpu-sample", type=int, default=8)
+    ap.add_argument("--cpu-sample", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-mode", action="store_true", help="timed steps only (for ncu captures)")
     ap.add_argument("--grad", type=int, default=0,
@@ -289,6 +317,10 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != a.gpus:
+        if "WORLD_SIZE" in os.environ:
+            sys.exit(f"bench.py: --gpus {a.gpus} but WORLD_SIZE={world}")
+        return spawn_ranks(a.gpus)               # one process per GPU, as torchrun would start them
     torch.cuda.set_device(local)
     if world > 1:
         from datetime import timedelta
@@ -361,45 +393,15 @@ def main():
     value = shard.aggregate_rate(a.nmol, world, ms / 1000.0)
     conv = res["converged"].cpu().numpy()
     iters = res["iterations"].cpu().numpy()
+    res["D"] = eng.D.clone()                 # converged densities of the timed batch (parity)
 
-    # roofline of the ERI kernel's companion: the J/K kernel streams the s8 list once per call
-    P = eng.plan
-    hbm, peak_kind = _peaks()
-    rbytes = 4 if a.precision == "mixed" else 8
-    eng.D.copy_(eng.D0)
-    jk_ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-    for _ in range(3):
-        eng.jk(active=None)
-    torch.cuda.synchronize()
-    njk = 10
-    jk_ev[0].record()
-    for _ in range(njk):
-        eng.jk(active=None)
-    jk_ev[1].record()
-    torch.cuda.synchronize()
-    jk_ms = jk_ev[0].elapsed_time(jk_ev[1]) / njk
-    # J/K reads the s8 list and the exchange list (same size) once per call
-    nlists = 2 if eng.jk_impl == "pairs" else 1
-    jk_bytes = nlists * P.n_eri * rbytes
-    achieved = jk_bytes / (jk_ms / 1000.0) / 1e9
-    # DRAM traffic per launch: ncu capture of the same kernel on the 256-molecule batch
-    # (k_symv: 868.8 MB read + 6.4 MB written for 860.7 MB of float32 list entries),
-    # scaled to this launch by the number of entries processed (traffic grows with the lists)
-    traffic = jk_bytes * (875.2 / 860.7) if (a.precision == "mixed" and nlists == 2) else None
-    roofline = {"kernel": "k_symv" if nlists == 2 else "k_jk_s8", "bound": "hbm", "achieved": achieved,
-                "peak": hbm, "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
-                "traffic_source": "ncu 256-molecule capture scaled by list size",
-                "algorithmic_bytes_per_launch": jk_bytes, "ms_per_launch": jk_ms}
-
-    # per-kernel figures beside the roofline; a failure here is recorded in the line, it does
-    # not void it
-    kernels = {}
-    if not a.profile_mode:
-        try:
-            kernels = kernel_figures(eng, a.precision)
-        except Exception as e:  # noqa: BLE001
-            kernels = {"error": f"{type(e).__name__}: {e}"}
-    kernels["jk"] = {"entry": "b2_jk_pairs", "ms_per_call": jk_ms, "gbs": achieved, "frac": achieved / hbm}
+    # ---- roofline figures of the kernel families (dominant first) on the resident batch
+    rooflines = []
+    try:
+        rooflines = kernel_rooflines(eng, a.precision)
+    except Exception as e:  # noqa: BLE001  (recorded in the line, it does not void it)
+        rooflines = [{"error": f"{type(e).__name__}: {e}"}]
+    roofline = rooflines[0]
 
     grad = None
     if a.grad > 0 and rank == 0:
@@ -408,41 +410,61 @@ def main():
     if a.profile_mode:
         a.plain_sample = 0
         a.no_cpu = True
-    # plain FP64 per-molecule GPU path on a sample (same convergence rule, minao guess)
+    # ---- parity of every molecule of the timed batch against the plain FP64 path
+    parity = None
+    if rank == 0 and not a.profile_mode:
+        parity = batch_parity(eng, mols, a, res)
+    learned = None
+    if rank == 0 and not a.profile_mode and a.guess == "learned":
+        learned = learned_guess_criterion(mols, a, net)
+    cfg2 = None
+    if rank == 0 and not a.profile_mode:
+        try:
+            cfg2 = config2_report()
+        except Exception as e:  # noqa: BLE001
+            cfg2 = {"error": f"{type(e).__name__}: {e}"}
+
+    # ---- plain FP64 per-molecule GPU path on a sample (same convergence rule, minao guess):
+    # wall clock per molecule (plan, engine, eager SCF, close) and its device time
     plain = None
     if rank == 0 and a.plain_sample > 0:
         sample = mols[:a.plain_sample]
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         plainE = []
+        dev_ms = 0.0
         for m in sample:
             e1 = RKSEngine([m], level=a.level, precision="fp64")
+            s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s0.record()
             r1 = e1.run_converged(graph=False)
+            s1.record()
             plainE.append(float(r1["energy"][0]))
             e1.close()
+            s1.synchronize()
+            dev_ms += s0.elapsed_time(s1)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         dE = np.abs(np.array(plainE) - res["energy"].cpu().numpy()[:a.plain_sample])
         plain = {"value": len(sample) / dt, "unit": UNIT, "sample": len(sample),
-                 "max_abs_dE_batched_vs_plain_Ha": float(dE.max())}
+                 "device_ms_per_molecule": dev_ms / len(sample), "wall_ms_per_molecule": 1e3 * dt / len(sample),
+                 "max_abs_dE_batched_vs_plain_Ha": float(dE.max()),
+                 "timing": "wall clock over the sample (plan + engine + eager SCF + close per molecule); "
+                           "device time = CUDA events around each molecule's SCF"}
 
+    # ---- CPU baseline: the reference's compiled int2e_sph + the FP64 port of its SCF on a
+    # bounded sample of the batch, on a pool of the host's cores; its energies also check the
+    # GPU results of the same molecules (FP64 oracle subset)
     cpu = None
     if rank == 0 and not a.no_cpu and a.cpu_sample > 0:
-        from oracle import eri as oeri
-        from b200dft.molgen import config3_batch
-        atoms = config3_batch(a.nmol, seed=a.seed)[:a.cpu_sample]
-        v, dt, _ = cpu_baseline(atoms, a.level, oeri.ref_available())
-        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": "reference" if oeri.ref_available() else "port",
-               "sample": f"first {a.cpu_sample} molecules of the batch, 20 SCF iterations, FP64, 1 core ({dt:.1f}s)"}
-        from b200dft.mole import methane
-        _, dt1, _ = cpu_baseline([methane()], a.level, oeri.ref_available())
-        cpu["ch4_s_per_molecule"] = dt1          # the CPU-runnable single-molecule case, same path
+        cpu = cpu_leg(a, res, parity)
 
-    # e2e through the public batch API (b200dft.engine.run_batches): every step builds a plan
-    # from the host libcint arrays (tables staged in pinned host memory and copied to the
-    # device), runs the batch to convergence and copies its results to host memory; the next
-    # step's plan is built on a worker thread while the GPU runs the current batch.  The
-    # device-timed engine is released first, so the batches reuse its memory.
+    # ---- e2e through the public batch API (b200dft.engine.run_batches): every step builds a
+    # plan from the host libcint arrays of the batch's molecules (tables staged in pinned host
+    # memory and copied to the device), runs the batch to convergence and copies its results to
+    # host memory; the next step's plan is built on a worker thread while the GPU runs the
+    # current batch.  The steps reuse the same 4096 host Mole objects (their libcint arrays are
+    # built once, before timing).  The device-timed engine is released first.
     eng.close()
     del eng
     e2e = None
@@ -472,12 +494,16 @@ def main():
         gc_pauses = [round(1e3 * (b[1] - a_[1]), 1) for a_, b in zip(gcl[0::2], gcl[1::2]) if a_[2] == 2]
         barrier()
         dt = max_over_ranks(dt * 1000.0) / 1000.0
+        steps_ms = [round(1e3 * (b - a_), 1) for a_, b in zip(marks[:-1], marks[1:])]
         e2e = {"value": shard.aggregate_rate(a.nmol, world, dt / ke), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d // ke), "d2h_bytes_per_step": int(d2h // ke),
                "steps": ke, "timing": "wall clock over the steps, max over ranks",
-               "step_ms": [round(1e3 * (b - a_), 1) for a_, b in zip(marks[:-1], marks[1:])],
-               "step_host_ms": host, "gc_gen2_pauses_ms": gc_pauses,
-               "api": "b200dft.engine.run_batches (plan of the next batch prefetched on a worker thread)"}
+               "step_ms_min_max": [min(steps_ms), max(steps_ms)],
+               "api": "b200dft.engine.run_batches (plan of the next batch prefetched on a worker thread)",
+               "inputs": "the same 4096 host Mole objects (libcint arrays built before timing) every step"}
+        # per-step detail goes to stderr, keeping the JSON line short
+        print(json.dumps({"e2e_step_ms": steps_ms, "e2e_step_host_ms": host, "gc_gen2_pauses_ms": gc_pauses}),
+              file=sys.stderr)
 
     if rank == 0:
         out = {
@@ -486,22 +512,163 @@ def main():
             "vs_baseline": None, "dtype": "f32+f64" if a.precision == "mixed" else "f64", "data": "synthetic",
             "config": {"workload": "batched uneven STO-3G B3LYP molecules (1-9 heavy atoms C/N/O/F 0.7/0.1/0.15/0.05), level-0 grid",
                        "nmol_per_gpu": a.nmol, "precision": a.precision, "guess": a.guess,
-                       "l2": "inputs (s8 ERIs, AO values) larger than L2 between iterations",
+                       "l2": "inputs (s8 ERIs, grid) larger than L2 between iterations",
                        "convergence": "|dE|<1e-6 Ha and DIIS err<1e-4, retire converged"},
-            "roofline": roofline, "kernels": kernels, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-            "gpu_launches": gpu_launches,
-            "phases_ms_per_step": {k: v / a.steps for k, v in phase.items()},
+            "roofline": roofline, "rooflines": rooflines[1:], "parity": parity, "cpu_baseline": cpu,
+            "e2e": e2e, "clocks": clocks, "gpu_launches": gpu_launches,
+            "phases_ms_per_step": {k: round(v / a.steps, 3) for k, v in phase.items()},
             "scf": {"converged": int(conv.sum()), "of": int(len(conv)),
                     "fallbacks_to_minao": int(res["fell_back"].sum().item()), "mean_its": float(iters[conv].mean()) if conv.any() else None,
                     "p50_its": float(np.percentile(iters[conv], 50)) if conv.any() else None,
                     "p99_its": float(np.percentile(iters[conv], 99)) if conv.any() else None},
-            "plain_fp64_per_molecule": plain,
+            "plain_fp64_per_molecule": plain, "learned_guess": learned, "config2": cfg2,
         }
         if grad is not None:
             out["gradient"] = grad
         print(json.dumps(out))
     if world > 1:
         dist.destroy_process_group()
+
+
+def spawn_ranks(n):
+    """``--gpus N`` without a launcher: start N ranks of this script through
+    torch.distributed.run on this node (127.0.0.1) and return its exit status"""
+    import socket
+    with socket.socket() as so:
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + sys.argv[1:]
+    rc = subprocess.call(cmd)
+    if rc:
+        sys.exit(rc)
+
+
+def batch_parity(eng, mols, a, res):
+    """Every molecule of the timed batch against the plain FP64 path: the same molecules through
+    the float64 engine (float64 ERIs, J/K and grid path, MINAO guess, same convergence rule;
+    the float64 path matches the FP64 oracle per iteration within 1e-6 Ha in the GPU tests).
+    Reports max |dE| and the count above 1e-4 Ha, max |dD| between the converged densities,
+    and max |dERI| between the float32 and float64 s8 lists."""
+    import torch
+    from b200dft.engine import RKSEngine
+    t0 = time.perf_counter()
+    e64 = RKSEngine(mols, level=a.level, precision="fp64", guess="minao")   # own plan, same layout
+    try:
+        r64 = e64.run_converged()
+        E32 = res["energy"].cpu().numpy()
+        E64 = r64["energy"].cpu().numpy()
+        c32 = res["converged"].cpu().numpy()
+        c64 = r64["converged"].cpu().numpy()
+        dE = np.abs(E32 - E64)
+        dD = float((res["D"] - e64.D).abs().max().item())
+        dERI = 0.0
+        n = eng.eri.numel()
+        step = 1 << 28
+        for o in range(0, n, step):
+            dERI = max(dERI, float((eng.eri[o:o + step].double() - e64.eri[o:o + step]).abs().max().item()))
+        torch.cuda.synchronize()
+        return {"n": int(len(mols)), "reference": "plain FP64 GPU path (float64 ERIs/J/K/grid, MINAO guess), "
+                                                 "same convergence rule",
+                "max_abs_dE_Ha": float(dE.max()), "n_over_1e-4": int((dE > 1e-4).sum()),
+                "mean_abs_dE_Ha": float(dE.mean()), "converged_mixed": int(c32.sum()), "converged_fp64": int(c64.sum()),
+                "max_abs_dD": dD, "max_abs_dERI": dERI, "seconds": round(time.perf_counter() - t0, 2)}
+    finally:
+        e64.close()
+
+
+def learned_guess_criterion(mols, a, net):
+    """The learned guess's own figure: SCF iterations to DIIS error < 1e-6 (and |dE| < 1e-6 Ha)
+    from the network's density vs from the MINAO-style guess, same batch, same engine."""
+    from b200dft.engine import RKSEngine
+    out = {"criterion": "DIIS error < 1e-6 and |dE| < 1e-6 Ha", "n": len(mols)}
+    for guess in ("learned", "minao"):
+        eng = RKSEngine(mols, level=a.level, precision=a.precision, guess=guess, net=net)
+        try:
+            r = eng.run_converged(diis_tol=1e-6, max_its=60, fallback=(guess == "learned"))
+            it = r["iterations"].cpu().numpy()
+            c = r["converged"].cpu().numpy()
+            out[guess] = {"converged": int(c.sum()), "mean_its": float(it[c].mean()) if c.any() else None,
+                          "p50_its": float(np.percentile(it[c], 50)) if c.any() else None,
+                          "p99_its": float(np.percentile(it[c], 99)) if c.any() else None}
+        finally:
+            eng.close()
+    if out["learned"]["mean_its"] and out["minao"]["mean_its"]:
+        out["its_saved_per_molecule"] = out["minao"]["mean_its"] - out["learned"]["mean_its"]
+    return out
+
+
+def config2_report():
+    """The single-molecule configuration at the size cap: the seeded 9-heavy-atom C/N/O tree on
+    the level-3 grid, per precision: max |dERI| of the float32 list against the float64 list,
+    max |dJ| / |dK| of the mixed J/K against the float64 J/K at the FP64 oracle's converged
+    density, and |dE| of each form's 20-iteration energies against the FP64 oracle trajectory
+    (committed fixture tests/golden/scf_oracle_config2_level3.npz)."""
+    import torch
+    from b200dft.engine import RKSEngine
+    from b200dft.molgen import config2_molecule
+    from b200dft.mole import Mole
+    g = np.load(os.path.join(ROOT, "tests", "golden", "scf_oracle_config2_level3.npz"))
+    m = Mole(config2_molecule(0))
+    out = {"molecule": "config2_molecule(seed 0)", "nao": int(m.nao), "level": 3}
+    engs = {}
+    try:
+        for prec in ("fp64", "mixed"):
+            e = RKSEngine([m], level=3, precision=prec, guess="minao")
+            engs[prec] = e
+            t0 = time.perf_counter()
+            r = e.run(its=20, log=False)
+            out[prec] = {"max_abs_dE_per_iteration_Ha": float(np.abs(r["energies"][:, 0, 0] - g["energies"][:, 0]).max()),
+                         "final_abs_dE_Ha": float(abs(r["energies"][-1, 0, 0] - g["energies"][-1, 0])),
+                         "seconds": round(time.perf_counter() - t0, 2)}
+        P = engs["fp64"].plan
+        out["n_points"] = int(P.n_points)
+        n4 = int(m.nao * (m.nao + 1) // 2 * (m.nao * (m.nao + 1) // 2 + 1) // 2)
+        o = int(P.eri_off[0])
+        out["mixed"]["max_abs_dERI"] = float((engs["mixed"].eri[o:o + n4].double() - engs["fp64"].eri[o:o + n4])
+                                             .abs().max().item())
+        Dref = torch.from_numpy(P.pack([g["D"]])).to(engs["fp64"].D.device)
+        for e in engs.values():
+            e.jk(D=Dref)
+        nn = m.nao * m.nao
+        out["mixed"]["max_abs_dJ"] = float((engs["mixed"].J[:nn] - engs["fp64"].J[:nn]).abs().max().item())
+        out["mixed"]["max_abs_dK"] = float((engs["mixed"].K[:nn] - engs["fp64"].K[:nn]).abs().max().item())
+        torch.cuda.synchronize()
+    finally:
+        for e in engs.values():
+            e.close()
+    return out
+
+
+def cpu_leg(a, res, parity):
+    """CPU baseline on a bounded sample of the batch (the first ``cpu_sample`` molecules): the
+    reference's compiled int2e_sph (oracle/_ref) + the FP64 port of its SCF, 20 iterations, on
+    spawned workers over the host's cores; the same energies check the GPU batch on those
+    molecules.  Also the CH4 single-molecule time on one core (warm, second call)."""
+    from oracle import eri as oeri
+    from b200dft.molgen import config3_batch
+    from b200dft.mole import methane
+    use_ref = oeri.ref_available()
+    procs = min(os.cpu_count() or 1, a.cpu_sample)
+    atoms = config3_batch(a.nmol, seed=a.seed)[:a.cpu_sample]
+    pool = _cpu_pool(procs, a.level, use_ref)
+    try:
+        v, dt, es = cpu_baseline(atoms, a.level, use_ref, pool)
+    finally:
+        pool.close()
+        pool.join()
+    Eg = res["energy"].cpu().numpy()[:len(es)]
+    dE = np.abs(np.asarray(es) - Eg)
+    cpu = {"value": v, "unit": UNIT, "cores": procs, "kind": "reference" if use_ref else "port",
+           "sample": f"first {len(atoms)} molecules of the batch, 20 SCF iterations, FP64, {procs} worker "
+                     f"processes with one BLAS thread each ({dt:.1f}s)"}
+    if parity is not None:
+        parity["oracle_subset"] = {"n": len(es), "max_abs_dE_Ha": float(dE.max()),
+                                   "vs": "batched mixed path, converged; oracle: 20 fixed iterations"}
+    cpu_baseline([methane()], a.level, use_ref)
+    _, dt1, _ = cpu_baseline([methane()], a.level, use_ref)
+    cpu["ch4_s_per_molecule"] = dt1
+    return cpu
 
 
 if __name__ == "__main__":

@@ -84,6 +84,6 @@ def build(src_root, quiet=False):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--src", default="/root/reference")
+    ap.add_argument("--src", default=os.environ.get("PYSCF_IPU_REFERENCE", "/root/reference"))
     a = ap.parse_args()
     build(a.src)
