@@ -95,6 +95,7 @@ static int b2_upload(T **dst, const std::vector<T> &src, B2Upload *u = nullptr) 
 static void b2_subset_free(B2PlanDev *P) {
   b2_dfree(P->sub.mol_map); b2_dfree(P->sub.jk_off); b2_dfree(P->sub.x32); b2_dfree(P->sub.x64);
   b2_dfree(P->sub.xtc); b2_dfree(P->sub.sv_off); b2_dfree(P->sub.bkt_map);
+  b2_dfree(P->sub.xq_items);
   P->sub = B2SubsetDev();
 }
 
@@ -333,7 +334,7 @@ int b2_plan_set_subset(void *plan, const int *mols, int n) {
   P->sub.sv_n = so[n];
   std::vector<int> bmap;
   b2_buckets(P, map, bmap, P->sub.bkt_off_h);
-  if ((rc = b2_upload(&P->sub.bkt_map, bmap))) {
+  if ((rc = b2_upload(&P->sub.bkt_map, bmap)) || (rc = b2_xq_build(*P, map, &P->sub.xq_items, P->sub.xq_off_h))) {
     b2_subset_free(P);
     return rc;
   }

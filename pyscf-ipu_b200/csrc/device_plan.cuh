@@ -16,6 +16,9 @@ struct B2GridDev {             // grid layout registered with b2_grid_set
   double *tmpl = nullptr;      // atomic grid templates (x, y, z, w)
   long long *tmpl_off = nullptr, *atom_pt_off = nullptr;
   std::vector<long long> grid_off_h, ao_off_h, xblk32_h, xblk64_h, xblk_tc_h;
+  void *xq_items = nullptr;                         // per-bucket XC work items (molecule, tile)
+  std::vector<long long> xq_off_h;                  // B2_NBKT + 1 bucket starts in xq_items
+  int *xq_queue = nullptr;                          // B2_NBKT work-queue counters
 };
 
 #define B2_NBKT 5              // orbital buckets nao <= 16, 32, 48, 64, more
@@ -27,6 +30,8 @@ struct B2SubsetDev {           // compacted work tables for a subset of the batc
   std::vector<int> bkt_off_h;  // B2_NBKT + 1
   long long *jk_off = nullptr, *x32 = nullptr, *x64 = nullptr, *xtc = nullptr, *sv_off = nullptr;
   long long jk_n = 0, n_x32 = 0, n_x64 = 0, n_xtc = 0, sv_n = 0;
+  void *xq_items = nullptr;    // per-bucket XC work items of the subset
+  std::vector<long long> xq_off_h;
 };
 
 struct B2PlanDev {
@@ -84,3 +89,6 @@ int b2_jk_status_read(int reset);     // error flag of the J/K product kernel (-
 int b2_launch_jk_s8(const B2PlanDev &P, int precision, const int *active, const void *eri,
                     const double *D, double *J, double *K, cudaStream_t st);
 int b2_zero_active(const B2PlanDev &P, const int *active, double *A, double *B, cudaStream_t st);
+// per-bucket work items of the tensor-core XC kernel for `mols` (device array in *items,
+// bucket starts in off), P.g.tpc_tc tiles per item
+int b2_xq_build(const B2PlanDev &P, const std::vector<int> &mols, void **items, std::vector<long long> &off);

@@ -277,6 +277,11 @@ int b2_grid_setup(B2PlanDev &P, const long long *grid_off_host) {
   B2_CUDA_TRY(cudaMemcpy(P.g.xblk64, x64.data(), nb, cudaMemcpyHostToDevice));
   B2_CUDA_TRY(cudaMemcpy(P.g.xblk_tc, xtc.data(), nb, cudaMemcpyHostToDevice));
   B2_CUDA_TRY(cudaMemcpy(P.g.ao_off, aoff.data(), nb, cudaMemcpyHostToDevice));
+  std::vector<int> all(nmol);
+  for (int m = 0; m < nmol; ++m) all[m] = m;
+  int rc = b2_xq_build(P, all, &P.g.xq_items, P.g.xq_off_h);
+  if (rc) return rc;
+  B2_CUDA_TRY(b2_dmalloc_t(&P.g.xq_queue, sizeof(int) * B2_NBKT));
   return B2_OK;
 }
 
@@ -292,7 +297,9 @@ int b2_xc_set_tpc(B2PlanDev &P, int tpc) {
   P.g.xblk_tc = d;
   P.g.xblk_tc_h = xtc;
   P.g.n_xblk_tc = xtc[P.h.nmol];
-  return B2_OK;
+  std::vector<int> all(P.h.nmol);
+  for (int m = 0; m < P.h.nmol; ++m) all[m] = m;
+  return b2_xq_build(P, all, &P.g.xq_items, P.g.xq_off_h);
 }
 
 void b2_grid_free(B2PlanDev &P) {
@@ -300,6 +307,7 @@ void b2_grid_free(B2PlanDev &P) {
   b2_dfree(P.g.xblk_tc);
   b2_dfree(P.g.ao_off);
   b2_dfree(P.g.tmpl); b2_dfree(P.g.tmpl_off); b2_dfree(P.g.atom_pt_off);
+  b2_dfree(P.g.xq_items); b2_dfree(P.g.xq_queue);
   P.g = B2GridDev();
 }
 

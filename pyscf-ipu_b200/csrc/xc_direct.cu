@@ -281,6 +281,8 @@ int b2_launch_xc_direct(const B2PlanDev &P, int precision, const int *active, co
     return b2_xcd_impl<double, 32>(P, active, coords, w, D, V, exc, sub ? P.sub.x64 : P.g.xblk64,
                                    sub ? P.sub.n_x64 : P.g.n_xblk64, P.g.tpc64, st);
   if (precision == 32 && P.xc_impl == 0)
+    return b2_launch_xc_tq(P, active, coords, w, D, V, exc, st);
+  if (precision == 32 && P.xc_impl == 2)
     return b2_launch_xc_tc(P, active, coords, w, D, V, exc, st);
   if (precision == 32)
     return b2_xcd_impl<float, 64>(P, active, coords, w, D, V, exc, sub ? P.sub.x32 : P.g.xblk32,

@@ -38,6 +38,7 @@
 // (read with b2_xc_tc_status), waits (bounded) for its issued MMAs, frees its TMEM and
 // returns.
 #include "device_plan.cuh"
+#include "devmem.cuh"
 #include "xc_math.cuh"
 #include "xc.cuh"
 #include <cstdint>
@@ -560,6 +561,525 @@ int b2_launch_xc_tc(const B2PlanDev &P, const int *active, const double *coords,
   return b2_sym_v(P, active, V, st);
 }
 
+// ============================================================================================
+// Per-bucket persistent form (default).  Same products, precision and result as k_xc_tc, with
+// these differences:
+//   * one launch per orbital bucket (NB = 16 Q), shared memory and tensor memory sized for that
+//     bucket (Q <= 2: two CTAs per SM);
+//   * persistent CTAs pull work items (molecule, block of tiles) from a device queue (one
+//     atomic counter per bucket, cleared before the launch) until it is empty; an item of an
+//     inactive molecule is skipped;
+//   * AO gradients are not stored: per orbital the radial factors ga = sum c e^{-a r^2} and
+//     gb = sum -2 a c e^{-a r^2} go to tensor memory (two columns per orbital) and the rho
+//     gradient and Y use them with the shell's displacement d = r - R:
+//       s:   AO = ga,      grad AO = gb d
+//       p_k: AO = d_k ga,  grad AO = ga e_k + d_k gb d
+//     so rho_c = sum_n X_n grad_c AO_n and Y_n = AO_n rt0 + grad AO_n . rt take a few FMAs per
+//     orbital, with one exponential evaluation per shell and tile (consecutive shells with the
+//     same centre and exponents, the 2s/2p pair of STO-3G, share them);
+//   * the AO0^T tile holds NB rows: the M = 64 product's rows >= NB read whatever follows
+//     (the next point chunk, or a pad), which only reaches accumulator rows >= NB, never read;
+//   * 4 CTA barriers per tile (was 6): the tensor-memory stores of the radial factors and the
+//     shell exponentials run before the wait on the previous tile's V product.
+// Tensor memory columns: X [0, NB), ga [NB, 2NB), gb [2NB, 3NB), V [3NB, 4NB) (+ [4NB, 5NB)
+// for NB > 64).
+struct __align__(8) B2XtItem { int m, t0; };
+
+// pad after each T tile: the M = 64 product reads (64 - NB) / 8 row groups past a chunk
+template <int Q> __host__ __device__ constexpr int b2_xq_pad() { return 16 * Q < 64 ? 256 : 0; }
+template <int Q>
+__host__ __device__ constexpr int b2_xq_dyn_floats() {   // D, N / Y^T and T tiles, T pads
+  return 2 * (16 * Q) * (16 * Q) + 4 * (32 * b2_lt(16 * Q)) / 4 + 2 * b2_xq_pad<Q>();
+}
+template <int Q> __host__ __device__ constexpr uint32_t b2_xq_tmem_cols() {
+  return (16 * Q > 64 ? 5 : 4) * 16 * Q <= 64 ? 64 : (16 * Q > 64 ? 5 : 4) * 16 * Q <= 128 ? 128
+         : (16 * Q > 64 ? 5 : 4) * 16 * Q <= 256 ? 256 : 512;
+}
+
+template <int Q>
+__global__ void __launch_bounds__(B2_XT_NT, Q <= 2 ? 2 : 1)
+k_xc_tq(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
+        const B2XtItem *__restrict__ items, int n_items, int *__restrict__ queue,
+        const long long *__restrict__ grid_off, int tpc, const int *__restrict__ active,
+        const double *__restrict__ coords, const double *__restrict__ w, const double *__restrict__ D,
+        double *__restrict__ V, double *__restrict__ exc) {
+  constexpr int NB = 16 * Q;
+  constexpr int R1 = (32 * b2_lt(NB)) / 4;          // floats of one N / Y^T / T tile
+  constexpr uint32_t NCOL = b2_xq_tmem_cols<Q>();
+  constexpr uint32_t colX = 0, colGA = NB, colGB = 2 * NB, colV = 3 * NB, colV2 = 4 * NB;
+  extern __shared__ __align__(128) float smem_f[];
+  __shared__ B2XtOrb sOrb[NB];
+  __shared__ double sR[B2_XT_MAXSH][3];
+  __shared__ float sRed[16 * B2_XT_PT];
+  // NB = 80 leaves no room for a separate B3LYP exchange buffer: it reuses sRed (one more barrier)
+  constexpr bool kAlias = Q >= 5;
+  __shared__ float sFnArr[kAlias ? 1 : 9 * B2_XT_PT];
+  float *sFn = kAlias ? sRed : sFnArr;
+  __shared__ double red[16];
+  __shared__ __align__(8) unsigned long long sBar[2];
+  __shared__ uint32_t sTmem;
+  __shared__ int sItem, sAbort;
+  constexpr int PAD = b2_xq_pad<Q>();
+  float *sDh = smem_f, *sDl = sDh + NB * NB, *sAh = sDl + NB * NB, *sAl = sAh + R1;
+  float *sTh = sAl + R1, *sTl = sTh + R1 + PAD;     // each T tile followed by its pad
+  float *sYh = sAh, *sYl = sAl;                     // Y^T tiles reuse the N tiles
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int q4 = warp & 3, qq = warp >> 2, p = 32 * q4 + lane;
+  const int nq0 = qq * 4 * Q;                       // first orbital of this thread's quarter
+
+  if (tid == 0) {
+    sAbort = 0;
+    b2_mbar_init(b2_su32(&sBar[0]), 1);
+    b2_mbar_init(b2_su32(&sBar[1]), 1);
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                 :: "r"(b2_su32(&sTmem)), "r"(NCOL) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  // T tiles' pads: finite values (they only feed accumulator rows that are never read)
+  for (int e = tid; e < PAD; e += B2_XT_NT) { sTh[R1 + e] = 0.f; sTl[R1 + e] = 0.f; }
+  b2_fence_before();
+  __syncthreads();
+  b2_fence_after();
+  const uint32_t tbase = sTmem;
+  const uint32_t tl = tbase + ((uint32_t)(32 * q4) << 16);     // this warp's lane quarter
+  const uint32_t mbar1 = b2_su32(&sBar[0]), mbar2 = b2_su32(&sBar[1]);
+  const uint32_t id1 = b2_idesc_tf32(128, NB, 0, 0);            // X = AO0 D
+  const uint32_t id2 = b2_idesc_tf32(64, NB, 0, 0);             // V = AO0^T Y
+  uint32_t ph1 = 0, ph2 = 0;
+  bool g2_pending = false, x_pending = false;      // an issued product not yet seen complete
+
+  for (;;) {
+    __syncthreads();                                // every thread is done with the last item
+    if (tid == 0) sItem = atomicAdd(queue, 1);
+    __syncthreads();
+    const int it = sItem;
+    if (it >= n_items || sAbort) break;
+    const B2XtItem item = items[it];
+    const int m = item.m;
+    if (active && !active[m]) continue;             // uniform: every thread read the same item
+    const B2MolDev md = mols[m];
+    const int N = md.nao;
+    const long long G = grid_off[m + 1] - grid_off[m];
+    const double *cm = coords + 3 * grid_off[m];
+    const double *wm = w + grid_off[m];
+    // the previous item's V product may still read the T / Y^T tiles, and its V flush already
+    // waited for it; here: orbital table, shell centres, D split into TF32 pieces
+    for (int s = tid; s < md.nbas; s += B2_XT_NT) {
+      const B2Shell &S = shells[md.sh_off + s];
+      sR[s][0] = S.R[0];
+      sR[s][1] = S.R[1];
+      sR[s][2] = S.R[2];
+      const int nc = S.l == 0 ? 1 : 3;
+      bool same = false;                            // same centre and exponents as shell s-1
+      if (s > 0) {
+        const B2Shell &P0 = shells[md.sh_off + s - 1];
+        same = P0.atom == S.atom && P0.nprim == S.nprim;
+        for (int k = 0; k < S.nprim && same; ++k) same = P0.exp[k] == S.exp[k];
+      }
+      for (int c = 0; c < nc; ++c) {
+        B2XtOrb o;
+        for (int k = 0; k < 3; ++k) {
+          const bool has = k < S.nprim;
+          o.e2[k] = has ? (float)(S.exp[k] * 1.4426950408889634) : 0.f;
+          o.c[k] = has ? (float)S.coef[k] : 0.f;
+          o.m2a[k] = has ? (float)(-2.0 * S.exp[k]) : 0.f;
+        }
+        o.s = (float)s;
+        o.comp = S.l == 0 ? -1.f : (float)c;
+        o.pad = same ? 1.f : 0.f;
+        sOrb[S.ao0 + c] = o;
+      }
+    }
+    for (int e = tid; e < NB * NB; e += B2_XT_NT) {
+      const int r = e / NB, k = e - r * NB;
+      const float v = (r < N && k < N) ? (float)D[md.mat_off + (long long)r * N + k] : 0.f;
+      float d1, d2, t;
+      b2_split_rn(v, d1, t);
+      d2 = __uint_as_float((__float_as_uint(t) + 0x1000u) & 0xFFFFE000u);
+      const int idx = (((k >> 2) * (NB / 8) + (r >> 3)) * 8 + (r & 7)) * 4 + (k & 3);
+      sDh[idx] = d1;
+      sDl[idx] = d2;
+    }
+    // (the D tiles are read only by the X product, issued after the first tile's barrier)
+    double e_part = 0.0;
+    bool first = true;
+    for (int tt = 0; tt < tpc; ++tt) {
+      const long long g0 = ((long long)item.t0 + tt) * B2_XT_PT;
+      if (g0 >= G) break;
+      const int np = (int)min((long long)B2_XT_PT, G - g0);
+      const bool valid = p < np;
+      double px = 0, py = 0, pz = 0, wd = 0;
+      if (valid) {
+        px = cm[3 * (g0 + p)];
+        py = cm[3 * (g0 + p) + 1];
+        pz = cm[3 * (g0 + p) + 2];
+        wd = wm[g0 + p];
+      }
+      const float wp = (float)wd;
+      // ---- radial factors per orbital (tensor memory) and AO values (registers)
+      float a0[4 * Q];
+      {
+        int s_prev = -1;
+        float ev0 = 0, ev1 = 0, ev2 = 0, dx = 0, dy = 0, dz = 0, ga = 0, gb = 0;
+#pragma unroll
+        for (int j4 = 0; j4 < Q; ++j4) {
+          float g4a[4], g4b[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int n = nq0 + 4 * j4 + u;
+            float av = 0.f, gav = 0.f, gbv = 0.f;
+            if (n < N && valid) {
+              const float4 o0 = reinterpret_cast<const float4 *>(sOrb)[3 * n];
+              const float4 o1 = reinterpret_cast<const float4 *>(sOrb)[3 * n + 1];
+              const int sh = (int)o0.w;
+              if (sh != s_prev) {        // same for every lane of the warp
+                const float4 o2 = reinterpret_cast<const float4 *>(sOrb)[3 * n + 2];
+                if (!(o2.w != 0.f && sh == s_prev + 1 && s_prev >= 0)) {
+                  dx = (float)(px - sR[sh][0]);
+                  dy = (float)(py - sR[sh][1]);
+                  dz = (float)(pz - sR[sh][2]);
+                  const float r2 = dx * dx + dy * dy + dz * dz;
+                  ev0 = b2_ex2(-o0.x * r2);
+                  ev1 = b2_ex2(-o0.y * r2);
+                  ev2 = b2_ex2(-o0.z * r2);
+                }
+                s_prev = sh;
+                ga = o1.x * ev0 + o1.y * ev1 + o1.z * ev2;
+                gb = o2.x * o1.x * ev0 + o2.y * o1.y * ev1 + o2.z * o1.z * ev2;
+              }
+              const float comp = o1.w;
+              gav = ga;
+              gbv = gb;
+              av = comp < 0.f ? ga : (comp == 0.f ? dx : (comp == 1.f ? dy : dz)) * ga;
+            }
+            a0[4 * j4 + u] = av;
+            g4a[u] = gav;
+            g4b[u] = gbv;
+          }
+          b2_tmem_st4(tl + colGA + nq0 + 4 * j4, g4a[0], g4a[1], g4a[2], g4a[3]);
+          b2_tmem_st4(tl + colGB + nq0 + 4 * j4, g4b[0], g4b[1], g4b[2], g4b[3]);
+        }
+      }
+      // the previous tile's V product reads the T / Y^T tiles: wait before overwriting them
+      if (g2_pending) {
+        if (b2_mbar_wait(mbar2, ph2)) { ph2 ^= 1; g2_pending = false; }
+        else { atomicExch(&g_b2_xt_err, 2); sAbort = 1; }
+      }
+#pragma unroll
+      for (int j4 = 0; j4 < Q; ++j4) {
+        const int n0 = nq0 + 4 * j4;
+        float hi[4], lo[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) b2_split_rn(a0[4 * j4 + u], hi[u], lo[u]);
+        b2_st4(sAh + b2_tile_idx(p, n0), hi[0], hi[1], hi[2], hi[3]);
+        b2_st4(sAl + b2_tile_idx(p, n0), lo[0], lo[1], lo[2], lo[3]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {               // T tile: one float per orbital (conflict-free)
+          const int ti = b2_tt_idx(NB, n0 + u, p >> 2) + (p & 3);
+          sTh[ti] = hi[u];
+          sTl[ti] = lo[u];
+        }
+      }
+      b2_tmem_wait_st();
+      b2_fence_async_smem();
+      b2_fence_before();
+      __syncthreads();                                              // [1]
+      if (sAbort) break;
+      x_pending = true;
+      // ---- X = AO0 D = (A_h + A_l)(D_1 + D_2): three TF32 products per K step
+      if (tid == 0) {
+        b2_fence_after();
+        const uint32_t aH = b2_su32(sAh), aL = b2_su32(sAl), dH = b2_su32(sDh), dL = b2_su32(sDl);
+        constexpr uint32_t LBO_A = 2048, SBO_A = 128, LBO_D = (NB / 8) * 128, SBO_D = 128;
+#pragma unroll 1
+        for (int s = 0; s < NB / 8; ++s) {
+          const uint64_t ah = b2_sdesc(aH + s * 2 * LBO_A, LBO_A, SBO_A);
+          const uint64_t al = b2_sdesc(aL + s * 2 * LBO_A, LBO_A, SBO_A);
+          const uint64_t bh = b2_sdesc(dH + s * 2 * LBO_D, LBO_D, SBO_D);
+          const uint64_t bl = b2_sdesc(dL + s * 2 * LBO_D, LBO_D, SBO_D);
+          b2_mma_tf32(tbase + colX, al, bh, id1, s > 0 ? 1u : 0u);
+          b2_mma_tf32(tbase + colX, ah, bl, id1, 1u);
+          b2_mma_tf32(tbase + colX, ah, bh, id1, 1u);
+        }
+        b2_mma_commit(mbar1);
+      }
+      // ---- rho partials over this thread's orbitals: radial factors first (no MMA wait)
+      uint32_t ra[4 * Q], rb[4 * Q], xr[4 * Q];
+#pragma unroll
+      for (int j4 = 0; j4 < Q; ++j4) {
+        b2_tmem_ld4(tl + colGA + nq0 + 4 * j4, ra + 4 * j4);
+        b2_tmem_ld4(tl + colGB + nq0 + 4 * j4, rb + 4 * j4);
+      }
+      if (b2_mbar_wait(mbar1, ph1)) { ph1 ^= 1; x_pending = false; }
+      else { atomicExch(&g_b2_xt_err, 1); sAbort = 1; }
+      b2_fence_after();
+#pragma unroll
+      for (int j4 = 0; j4 < Q; ++j4) b2_tmem_ld4(tl + colX + nq0 + 4 * j4, xr + 4 * j4);
+      b2_tmem_wait_ld();
+      float r0 = 0.f, r1 = 0.f, r2 = 0.f, r3 = 0.f;
+      {
+        int s_prev = -1;
+        float dx = 0, dy = 0, dz = 0;
+#pragma unroll
+        for (int k = 0; k < 4 * Q; ++k) {
+          const int n = nq0 + k;
+          if (n < N) {
+            const float4 o0 = reinterpret_cast<const float4 *>(sOrb)[3 * n];
+            const float comp = reinterpret_cast<const float4 *>(sOrb)[3 * n + 1].w;
+            const int sh = (int)o0.w;
+            if (sh != s_prev) {
+              s_prev = sh;
+              dx = (float)(px - sR[sh][0]);
+              dy = (float)(py - sR[sh][1]);
+              dz = (float)(pz - sR[sh][2]);
+            }
+            const float xv = __uint_as_float(xr[k]), ga = __uint_as_float(ra[k]), gb = __uint_as_float(rb[k]);
+            const float dk = comp < 0.f ? 1.f : (comp == 0.f ? dx : (comp == 1.f ? dy : dz));
+            const float t = xv * dk * gb;
+            r0 += xv * dk * ga;
+            r1 += t * dx;
+            r2 += t * dy;
+            r3 += t * dz;
+            const float xg = comp < 0.f ? 0.f : xv * ga;
+            r1 += comp == 0.f ? xg : 0.f;
+            r2 += comp == 1.f ? xg : 0.f;
+            r3 += comp == 2.f ? xg : 0.f;
+          }
+        }
+      }
+      sRed[(qq * 4 + 0) * B2_XT_PT + p] = r0;
+      sRed[(qq * 4 + 1) * B2_XT_PT + p] = r1;
+      sRed[(qq * 4 + 2) * B2_XT_PT + p] = r2;
+      sRed[(qq * 4 + 3) * B2_XT_PT + p] = r3;
+      b2_fence_before();
+      __syncthreads();                                              // [2]
+      if (sAbort) break;
+      float rho[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        rho[c] = ((sRed[c * B2_XT_PT + p] + sRed[(4 + c) * B2_XT_PT + p]) + sRed[(8 + c) * B2_XT_PT + p]) +
+                 sRed[(12 + c) * B2_XT_PT + p];
+      if (kAlias) __syncthreads();                                  // sFn overwrites sRed
+      // ---- B3LYP in three parts: Slater + B88 (qq 0), VWN (qq 1), LYP (qq 2)
+      if (qq < 3) {
+        const B2XcPoint<float> o = qq == 0 ? b2_b3lyp_x<float>(rho[0], rho[1], rho[2], rho[3])
+                                   : qq == 1 ? b2_b3lyp_vwn<float>(rho[0], rho[1], rho[2], rho[3])
+                                             : b2_b3lyp_lyp<float>(rho[0], rho[1], rho[2], rho[3]);
+        sFn[(qq * 3 + 0) * B2_XT_PT + p] = o.exc;
+        sFn[(qq * 3 + 1) * B2_XT_PT + p] = o.vrho;
+        sFn[(qq * 3 + 2) * B2_XT_PT + p] = o.vgamma;
+      }
+      __syncthreads();                                              // [3]
+      const float ex = sFn[0 * B2_XT_PT + p] + (sFn[3 * B2_XT_PT + p] + sFn[6 * B2_XT_PT + p]);
+      const float vrho = sFn[1 * B2_XT_PT + p] + (sFn[4 * B2_XT_PT + p] + sFn[7 * B2_XT_PT + p]);
+      const float vg = sFn[2 * B2_XT_PT + p] + (sFn[5 * B2_XT_PT + p] + sFn[8 * B2_XT_PT + p]);
+      if (qq == 0 && valid) e_part += (double)rho[0] * wd * (double)ex;
+      const float rt0 = vrho * 0.5f * wp, f4 = 4.f * vg * wp;
+      const float rt1 = f4 * rho[1], rt2 = f4 * rho[2], rt3 = f4 * rho[3];
+      // ---- Y_n = AO_n rt0 + grad AO_n . rt -> Y^T tiles (the X product has finished reading
+      //      the N tiles they overwrite)
+      {
+        int s_prev = -1;
+        float dx = 0, dy = 0, dz = 0, dr = 0;
+#pragma unroll
+        for (int j4 = 0; j4 < Q; ++j4) {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int k = 4 * j4 + u, n = nq0 + k;
+            float y = 0.f;
+            if (n < N) {
+              const float4 o0 = reinterpret_cast<const float4 *>(sOrb)[3 * n];
+              const float comp = reinterpret_cast<const float4 *>(sOrb)[3 * n + 1].w;
+              const int sh = (int)o0.w;
+              if (sh != s_prev) {
+                s_prev = sh;
+                dx = (float)(px - sR[sh][0]);
+                dy = (float)(py - sR[sh][1]);
+                dz = (float)(pz - sR[sh][2]);
+                dr = dx * rt1 + dy * rt2 + dz * rt3;
+              }
+              const float ga = __uint_as_float(ra[k]), gb = __uint_as_float(rb[k]);
+              const float dk = comp < 0.f ? 1.f : (comp == 0.f ? dx : (comp == 1.f ? dy : dz));
+              const float rk = comp < 0.f ? 0.f : (comp == 0.f ? rt1 : (comp == 1.f ? rt2 : rt3));
+              y = dk * (ga * rt0 + gb * dr) + ga * rk;
+            }
+            float yh, yl;
+            b2_split_rn(y, yh, yl);
+            const int ti = b2_tt_idx(NB, n, p >> 2) + (p & 3);
+            sYh[ti] = yh;
+            sYl[ti] = yl;
+          }
+        }
+      }
+      b2_fence_async_smem();
+      b2_fence_before();
+      __syncthreads();                                              // [4]
+      // ---- V += AO0^T Y (M = 64 orbital rows; a second product covers rows 64..NB-1)
+      if (tid == 0) {
+        b2_fence_after();
+        const uint32_t aH = b2_su32(sTh), aL = b2_su32(sTl), yH = b2_su32(sYh), yL = b2_su32(sYl);
+        constexpr uint32_t LA = b2_lt(NB), SBO = 128;
+        constexpr uint32_t off2 = (uint32_t)((NB > 64 ? (NB - 64) / 8 : 0) * 128);
+#pragma unroll 1
+        for (int s = 0; s < B2_XT_PT / 8; ++s) {
+          const uint64_t ah = b2_sdesc(aH + 2 * s * LA, LA, SBO), al = b2_sdesc(aL + 2 * s * LA, LA, SBO);
+          const uint64_t bh = b2_sdesc(yH + 2 * s * LA, LA, SBO), bl = b2_sdesc(yL + 2 * s * LA, LA, SBO);
+          b2_mma_tf32(tbase + colV, al, bh, id2, (first && s == 0) ? 0u : 1u);
+          b2_mma_tf32(tbase + colV, ah, bl, id2, 1u);
+          b2_mma_tf32(tbase + colV, ah, bh, id2, 1u);
+          if (NB > 64) {
+            const uint64_t ah2 = b2_sdesc(aH + off2 + 2 * s * LA, LA, SBO);
+            const uint64_t al2 = b2_sdesc(aL + off2 + 2 * s * LA, LA, SBO);
+            b2_mma_tf32(tbase + colV2, al2, bh, id2, (first && s == 0) ? 0u : 1u);
+            b2_mma_tf32(tbase + colV2, ah2, bl, id2, 1u);
+            b2_mma_tf32(tbase + colV2, ah2, bh, id2, 1u);
+          }
+        }
+        b2_mma_commit(mbar2);
+      }
+      g2_pending = true;
+      first = false;
+    }
+    // ---- end of the item: wait for its last V product, flush V and the energy
+    if (g2_pending && !sAbort) {
+      if (b2_mbar_wait(mbar2, ph2)) { ph2 ^= 1; g2_pending = false; }
+      else { atomicExch(&g_b2_xt_err, 3); sAbort = 1; }
+    }
+    __syncthreads();
+    if (sAbort) break;
+    if (!first) {
+      b2_fence_after();
+      const int mu = 16 * q4 + lane;               // M=64 layout: row 16 q4 + lane in lanes 0..15
+#pragma unroll 1
+      for (int j4 = 0; j4 < Q; ++j4) {
+        const int n0 = nq0 + 4 * j4;
+        uint32_t v[4];
+        b2_tmem_ld4(tl + colV + n0, v);
+        b2_tmem_wait_ld();
+        if (lane < 16 && mu < N) {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const float f = __uint_as_float(v[u]);
+            if (n0 + u < N && f != 0.f) atomicAdd(&V[md.mat_off + (long long)mu * N + n0 + u], (double)f);
+          }
+        }
+        if (NB > 64) {
+          b2_tmem_ld4(tl + colV2 + n0, v);
+          b2_tmem_wait_ld();
+          const int mu2 = NB - 64 + mu;
+          if (lane < 16 && mu2 >= 64 && mu2 < N) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              const float f = __uint_as_float(v[u]);
+              if (n0 + u < N && f != 0.f) atomicAdd(&V[md.mat_off + (long long)mu2 * N + n0 + u], (double)f);
+            }
+          }
+        }
+      }
+      for (int o = 16; o > 0; o >>= 1) e_part += __shfl_down_sync(0xffffffffu, e_part, o);
+      if (lane == 0) red[warp] = e_part;
+      b2_fence_before();
+      __syncthreads();
+      if (tid == 0) {
+        double sum = 0;
+        for (int i = 0; i < B2_XT_NT / 32; ++i) sum += red[i];
+        atomicAdd(&exc[m], sum);
+      }
+    }
+  }
+  // leaving: a product may still be in flight only after an abort; wait for it (bounded)
+  if (x_pending) b2_mbar_wait(mbar1, ph1);
+  if (g2_pending) b2_mbar_wait(mbar2, ph2);
+  b2_fence_before();
+  __syncthreads();
+  b2_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tbase), "r"(NCOL) : "memory");
+}
+
+template <int Q>
+static int b2_xq_launch(const B2PlanDev &P, const B2XtItem *items, int n_items, int *queue,
+                        const int *active, const double *coords, const double *w, const double *D,
+                        double *V, double *exc, cudaStream_t st) {
+  const size_t sm = sizeof(float) * (size_t)b2_xq_dyn_floats<Q>();
+  static int occ[8] = {0};                      // CTAs per SM (per device, filled on first use)
+  int dev = 0;
+  B2_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 8) return B2_ERR_CUDA;
+  if (!occ[dev]) {
+    B2_CUDA_TRY(cudaFuncSetAttribute(k_xc_tq<Q>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int o = 0, nsm = 0;
+    B2_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_xc_tq<Q>, B2_XT_NT, sm));
+    B2_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    occ[dev] = std::max(1, o) * nsm;
+  }
+  const int grid = std::min(n_items, occ[dev]);
+  k_xc_tq<Q><<<grid, B2_XT_NT, sm, st>>>(P.mols, P.shells, items, n_items, queue, P.g.grid_off,
+                                          P.g.tpc_tc, active, coords, w, D, V, exc);
+  return B2_OK;
+}
+
+int b2_launch_xc_tq(const B2PlanDev &P, const int *active, const double *coords, const double *w,
+                    const double *D, double *V, double *exc, cudaStream_t st) {
+  const bool sub = P.sub.n > 0;
+  const B2XtItem *items = (const B2XtItem *)(sub ? P.sub.xq_items : P.g.xq_items);
+  const std::vector<long long> &off = sub ? P.sub.xq_off_h : P.g.xq_off_h;
+  if (P.h.max_nbas > B2_XT_MAXSH || P.h.max_nao > 80) return B2_ERR_SIZE;
+  if (!items || off.size() != B2_NBKT + 1 || !P.g.xq_queue) return B2_ERR_ARG;
+  if (active) {
+    int rc = b2_zero_active(P, active, V, nullptr, st);
+    if (rc) return rc;
+  } else {
+    B2_CUDA_TRY(cudaMemsetAsync(V, 0, sizeof(double) * P.h.n_mat, st));
+  }
+  int rc = b2_zero_exc(P, active, exc, st);
+  if (rc) return rc;
+  B2_CUDA_TRY(cudaMemsetAsync(P.g.xq_queue, 0, sizeof(int) * B2_NBKT, st));
+  // one launch per bucket on the plan's bucket streams (forked from / joined to `st`)
+  B2_CUDA_TRY(cudaEventRecord(P.bkt_ev[B2_NBKT], st));
+  for (int b = B2_NBKT - 1; b >= 0; --b) {
+    const int n = (int)(off[b + 1] - off[b]);
+    if (n <= 0) continue;
+    cudaStream_t s = P.bkt_stream[b];
+    B2_CUDA_TRY(cudaStreamWaitEvent(s, P.bkt_ev[B2_NBKT], 0));
+    const B2XtItem *it = items + off[b];
+    int *q = P.g.xq_queue + b;
+    switch (b) {
+      case 0: rc = b2_xq_launch<1>(P, it, n, q, active, coords, w, D, V, exc, s); break;
+      case 1: rc = b2_xq_launch<2>(P, it, n, q, active, coords, w, D, V, exc, s); break;
+      case 2: rc = b2_xq_launch<3>(P, it, n, q, active, coords, w, D, V, exc, s); break;
+      case 3: rc = b2_xq_launch<4>(P, it, n, q, active, coords, w, D, V, exc, s); break;
+      default: rc = b2_xq_launch<5>(P, it, n, q, active, coords, w, D, V, exc, s); break;
+    }
+    if (rc) return rc;
+    b2_count_launches(1);
+    B2_CUDA_TRY(cudaGetLastError());
+    B2_CUDA_TRY(cudaEventRecord(P.bkt_ev[b], s));
+    B2_CUDA_TRY(cudaStreamWaitEvent(st, P.bkt_ev[b], 0));
+  }
+  return b2_sym_v(P, active, V, st);
+}
+
+// work items (molecule, first tile) of the per-bucket kernel for the molecules `mols`, grouped
+// by orbital bucket (off: B2_NBKT + 1 bucket starts), `tpc` tiles per item
+static void b2_xq_items(const B2PlanDev &P, const std::vector<int> &mols, int tpc, std::vector<B2XtItem> &items,
+                        std::vector<long long> &off) {
+  off.assign(B2_NBKT + 1, 0);
+  std::vector<std::vector<B2XtItem>> per(B2_NBKT);
+  for (int m : mols) {
+    const int b = std::min(B2_NBKT - 1, (P.h.mols[m].nao - 1) / 16);
+    const long long nt = (P.g.grid_off_h[m + 1] - P.g.grid_off_h[m] + B2_XT_PT - 1) / B2_XT_PT;
+    for (long long t = 0; t < nt; t += tpc) per[b].push_back(B2XtItem{m, (int)t});
+  }
+  items.clear();
+  for (int b = 0; b < B2_NBKT; ++b) {
+    items.insert(items.end(), per[b].begin(), per[b].end());
+    off[b + 1] = (long long)items.size();
+  }
+}
+
 int b2_xc_tc_status_read(int reset) {
   int v = 0;
   if (cudaMemcpyFromSymbol(&v, g_b2_xt_err, sizeof(int)) != cudaSuccess) return -1;
@@ -568,4 +1088,16 @@ int b2_xc_tc_status_read(int reset) {
     cudaMemcpyToSymbol(g_b2_xt_err, &z, sizeof(int));
   }
   return v;
+}
+
+int b2_xq_build(const B2PlanDev &P, const std::vector<int> &mols, void **items, std::vector<long long> &off) {
+  std::vector<B2XtItem> it;
+  b2_xq_items(P, mols, std::max(1, P.g.tpc_tc), it, off);
+  B2XtItem *d = nullptr;
+  B2_CUDA_TRY(b2_dmalloc_t(&d, sizeof(B2XtItem) * std::max<size_t>(1, it.size())));
+  if (!it.empty())
+    B2_CUDA_TRY(cudaMemcpy(d, it.data(), sizeof(B2XtItem) * it.size(), cudaMemcpyHostToDevice));
+  b2_dfree(*items);
+  *items = d;
+  return B2_OK;
 }
