@@ -203,6 +203,31 @@ int b2_grad(b2_plan_t plan, int parts, double hyb, const double *C, const double
             const double *coords, const double *weights, double *D, double *W, double *grad,
             void *stream);
 
+/* Device buffers of a batch's SCF state for b2_scf_iterate (all nmol molecules of the plan,
+ * layouts as for the entries above; matrices float64 at the plan's matrix offsets).
+ * Inputs: Hcore, S, Linv; weights and either coords (AO values generated per grid tile) or ao
+ * (stored AO values, precision `precision`); enuc [nmol]; eri (s8 list, `precision`) and exch
+ * (its exchange list, or NULL to contract the s8 list directly).  State carried between
+ * iterations: D, J, K, Vxc, H, diffJK, ring_err / ring_h (9 n_mat each), bmat (100 nmol),
+ * diis_err, exc, energy (5 nmol), mo_energy (72 nmol), C and eig_ws (may be NULL), iter, active
+ * (int nmol; molecules with active == 0 are skipped), sweeps (may be NULL). */
+typedef struct {
+  const double *Hcore, *S, *Linv, *coords, *weights, *enuc;
+  const void *ao, *eri, *exch;
+  double *D, *J, *K, *Vxc, *H, *diffJK, *ring_err, *ring_h, *bmat, *diis_err, *exc, *energy, *mo_energy, *C,
+      *eig_ws;
+  int *iter, *active, *sweeps;
+  double hyb;
+  int use_diis, precision;
+} b2_scf_state;
+
+/* One SCF iteration of every active molecule (nanoDFT_iteration, nanoDFT.py:40-102): Fock build
+ * + DIIS, orthogonalised eigensolve and new density, V_xc / E_xc, J / K, diff_JK = J - hyb/2 K,
+ * the five energy terms, iter += 1.  Launches kernels only (on `stream` and the plan's bucket
+ * streams, joined back to `stream`), so a call can be captured into a CUDA graph and replayed;
+ * one capture serves every later iteration. */
+int b2_scf_iterate(b2_plan_t plan, const b2_scf_state *state, void *stream);
+
 /* Single-molecule convenience mirroring the reference's native entry int2e_sph
  * (int2e_sph.cpp:6750): host libcint arrays in, all s8 ERIs of the molecule out (device). */
 int b2_int2e_sph_s8(const int *atm, int natm, const int *bas, int nbas, const double *env,

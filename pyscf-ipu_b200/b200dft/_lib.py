@@ -57,7 +57,17 @@ SIGNATURES = {
     "b2_enuc": [_P, _P, _P],
     "b2_grad": [_P, _I, _D, _P, _P, _P, _P, _P, _P, _P, _P],
     "b2_eri_threshold": [_P, _I, _P, _D, _P],
+    "b2_scf_iterate": [_P, _P, _P],
 }
+
+
+class ScfState(ctypes.Structure):
+    """b2_scf_state (include/b200dft.h): device pointers of a batch's SCF state"""
+    _fields_ = ([(n, _P) for n in ("Hcore", "S", "Linv", "coords", "weights", "enuc", "ao", "eri", "exch",
+                                   "D", "J", "K", "Vxc", "H", "diffJK", "ring_err", "ring_h", "bmat",
+                                   "diis_err", "exc", "energy", "mo_energy", "C", "eig_ws",
+                                   "iter", "active", "sweeps")] +
+                [("hyb", _D), ("use_diis", _I), ("precision", _I)])
 
 
 class B200DFTError(RuntimeError):

@@ -14,7 +14,7 @@ import ctypes
 import numpy as np
 import torch
 
-from ._lib import lib, check, ptr, stream_handle, B200DFTError, launch_count
+from ._lib import lib, check, ptr, stream_handle, B200DFTError, launch_count, ScfState
 from .constants import HYB_B3LYP
 from .grids import Grids, atomic_grid
 from .guess import minao
@@ -380,8 +380,31 @@ class RKSEngine:
         self.scf_xc()
         self.jk()
 
+    def scf_state(self, use_diis=True, hyb=HYB_B3LYP):
+        """the b2_scf_state of this engine's device buffers"""
+        st = ScfState()
+        for name, t in (("Hcore", self.Hcore), ("S", self.S), ("Linv", self.Linv), ("coords", self.coords),
+                        ("weights", self.weights), ("enuc", self.enuc), ("eri", self.eri), ("D", self.D),
+                        ("J", self.J), ("K", self.K), ("Vxc", self.Vxc), ("H", self.H), ("diffJK", self.diffJK),
+                        ("ring_err", self.ring_err), ("ring_h", self.ring_h), ("bmat", self.bmat),
+                        ("diis_err", self.diis_err), ("exc", self.exc), ("energy", self.energy),
+                        ("mo_energy", self.mo_energy), ("C", self.C), ("eig_ws", self.eig_ws),
+                        ("iter", self.iter), ("active", self.active), ("sweeps", self.sweeps)):
+            setattr(st, name, t.data_ptr())
+        st.ao = self.ao.data_ptr() if self.ao_stored else None
+        st.exch = self.eri_x.data_ptr() if self.jk_impl == "pairs" else None
+        st.hyb, st.use_diis, st.precision = float(hyb), int(use_diis), self.prec
+        return st
+
     def step(self, use_diis=True):
-        """One SCF iteration for every active molecule (nanoDFT.py:63-80)."""
+        """One SCF iteration for every active molecule (nanoDFT.py:40-102): one b2_scf_iterate
+        call (Fock + DIIS, eigensolve + density, XC, J/K, diff_JK, energies, iteration count)."""
+        st = self.scf_state(use_diis)
+        self._state = st                     # the call reads it synchronously; keep it referenced
+        check(lib().b2_scf_iterate(self.plan.h, ctypes.byref(st), stream_handle()), "b2_scf_iterate")
+
+    def step_entries(self, use_diis=True):
+        """The same iteration as ``step`` through the individual entry points."""
         a = self.active
         self.fock_diis(use_diis)
         self.eigh_density()

@@ -9,6 +9,7 @@
 #include "scf.cuh"
 #include "xc_math.cuh"
 #include "setup.cuh"
+#include "b200dft.h"             // after the enum of status codes in common.cuh (same values)
 
 static thread_local std::string g_last_error;
 #include <atomic>
@@ -452,6 +453,29 @@ int b2_energy(void *plan, const int *active, const double *D, const double *Hcor
   if (!plan || !D || !Hcore || !diffJK || !Exc || !Enuc || !out) return B2_ERR_ARG;
   return b2_launch_energy(*(B2PlanDev *)plan, active, D, Hcore, diffJK, Exc, Enuc, out,
                           (cudaStream_t)stream);
+}
+
+int b2_scf_iterate(void *plan, const b2_scf_state *S, void *stream) {
+  if (!plan || !S) return B2_ERR_ARG;
+  if (!S->Hcore || !S->S || !S->Linv || !S->weights || !S->enuc || !S->eri || !S->D || !S->J || !S->K ||
+      !S->Vxc || !S->H || !S->diffJK || !S->ring_err || !S->ring_h || !S->bmat || !S->diis_err || !S->exc ||
+      !S->energy || !S->mo_energy || !S->iter || !S->active || (!S->ao && !S->coords))
+    return B2_ERR_ARG;
+  if (S->precision != 64 && S->precision != 32) return B2_ERR_ARG;
+  B2PlanDev &P = *(B2PlanDev *)plan;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int *a = S->active;
+  int rc = b2_launch_fock_diis(P, a, S->iter, S->hyb, S->use_diis, S->Hcore, S->S, S->D, S->J, S->K,
+                               S->Vxc, S->H, S->diffJK, S->ring_err, S->ring_h, S->bmat, S->diis_err, st);
+  if (!rc) rc = b2_launch_eigh_density(P, a, S->iter, S->H, S->Linv, S->D, S->mo_energy, S->C, S->eig_ws,
+                                       S->sweeps, st);
+  if (!rc) rc = S->ao ? b2_launch_xc(P, S->precision, a, S->ao, S->weights, S->D, S->Vxc, S->exc, st)
+                      : b2_launch_xc_direct(P, S->precision, a, S->coords, S->weights, S->D, S->Vxc, S->exc, st);
+  if (!rc) rc = S->exch ? b2_launch_jk_symv(P, S->precision, a, S->eri, S->exch, S->D, S->J, S->K, P.sv_work, st)
+                        : b2_launch_jk_s8(P, S->precision, a, S->eri, S->D, S->J, S->K, st);
+  if (!rc) rc = b2_launch_energy_jk(P, a, S->D, S->Hcore, S->J, S->K, S->hyb, S->exc, S->enuc, S->diffJK,
+                                    S->energy, S->iter, st);
+  return rc;
 }
 
 int b2_int2e_sph_s8(const int *atm, int natm, const int *bas, int nbas, const double *env,

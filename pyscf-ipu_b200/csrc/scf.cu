@@ -438,6 +438,50 @@ __global__ void k_energy(const B2MolDev *__restrict__ mols, const int *__restric
   }
 }
 
+// end of one SCF iteration (nanoDFT.py:74-80): diff_JK = J - hyb/2 K of the new density
+// (get_JK, nanoDFT.py:125-139), the five energy terms (nanoDFT.py:20-38) and the molecule's
+// iteration counter advanced; inactive molecules are left untouched
+__global__ void k_energy_jk(const B2MolDev *__restrict__ mols, const int *__restrict__ active,
+                            const double *__restrict__ D, const double *__restrict__ Hcore,
+                            const double *__restrict__ J, const double *__restrict__ K, double hyb,
+                            const double *__restrict__ exc, const double *__restrict__ enuc,
+                            double *__restrict__ diffJK, double *__restrict__ out, int *__restrict__ iter) {
+  const int m = blockIdx.x;
+  if (active && !active[m]) return;
+  __shared__ double red[32];
+  const B2MolDev md = mols[m];
+  const int NN = md.nao * md.nao;
+  double ec = 0, ej = 0;
+  for (int e = threadIdx.x; e < NN; e += blockDim.x) {
+    const long long a = md.mat_off + e;
+    const double d = D[a];
+    const double djk = J[a] - 0.5 * hyb * K[a];
+    diffJK[a] = djk;
+    ec += d * Hcore[a];
+    ej += d * djk;
+  }
+  ec = b2_block_sum(ec, red);
+  ej = b2_block_sum(ej, red);
+  if (threadIdx.x == 0) {
+    double *o = out + (long long)m * 5;
+    o[0] = ec + 0.5 * ej + exc[m] + enuc[m];
+    o[1] = ec;
+    o[2] = 0.5 * ej;
+    o[3] = exc[m];
+    o[4] = enuc[m];
+    if (iter) iter[m] += 1;
+  }
+}
+
+int b2_launch_energy_jk(const B2PlanDev &P, const int *active, const double *D, const double *Hcore,
+                        const double *J, const double *K, double hyb, const double *exc,
+                        const double *enuc, double *diffJK, double *out, int *iter, cudaStream_t st) {
+  k_energy_jk<<<P.h.nmol, 256, 0, st>>>(P.mols, active, D, Hcore, J, K, hyb, exc, enuc, diffJK, out, iter);
+  b2_count_launches(1);
+  B2_CUDA_TRY(cudaGetLastError());
+  return B2_OK;
+}
+
 // L = inv(cholesky(S)) per molecule (FP64), one CTA per molecule (serial-ish, small N)
 __global__ void k_chol_inv(const B2MolDev *__restrict__ mols, const double *__restrict__ S,
                            double *__restrict__ Linv, int *__restrict__ status) {

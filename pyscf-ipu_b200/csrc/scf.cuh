@@ -12,3 +12,6 @@ int b2_launch_energy(const B2PlanDev &P, const int *active, const double *D, con
                      const double *diffJK, const double *exc, const double *enuc, double *out,
                      cudaStream_t st);
 int b2_launch_chol_inv(const B2PlanDev &P, const double *S, double *Linv, int *status, cudaStream_t st);
+int b2_launch_energy_jk(const B2PlanDev &P, const int *active, const double *D, const double *Hcore,
+                        const double *J, const double *K, double hyb, const double *exc,
+                        const double *enuc, double *diffJK, double *out, int *iter, cudaStream_t st);

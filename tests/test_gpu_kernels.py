@@ -196,7 +196,7 @@ def test_xc_tensor_core_vs_cuda_core(cuda):
     eng = RKSEngine(mols, level=0, precision="mixed", setups=setups)
     eng.D.copy_(eng.D0)
     got = {}
-    for impl in (1, 0):
+    for impl in (1, 2, 0):               # CUDA-core, one-launch tensor-core, per-bucket persistent
         check(lib().b2_plan_set_xc_impl(eng.plan.h, impl), "b2_plan_set_xc_impl")
         eng.xc()
         torch.cuda.synchronize()
@@ -213,6 +213,55 @@ def test_xc_tensor_core_vs_cuda_core(cuda):
         np.testing.assert_allclose(Vt, V, atol=2e-5 * np.abs(V).max())
         np.testing.assert_allclose(Vt, Vs, atol=2e-5 * np.abs(V).max())
         np.testing.assert_allclose(Vt, Vt.T, atol=1e-12)
+        assert abs(got[2][0][mi] - exc) < 2e-6 * abs(exc)
+        np.testing.assert_allclose(eng.plan.unpack(got[2][1], mi), V, atol=2e-5 * np.abs(V).max())
+    eng.close()
+
+
+def test_xc_work_queue_items_active_and_subset(cuda):
+    # the per-bucket persistent kernel: several tile counts per work item, inactive molecules
+    # left untouched, and a molecule subset (compacted items) give the same V and E_xc
+    rng = np.random.default_rng(12)
+    mols = [Mole(random_molecule(rng, k)) for k in (9, 1, 5, 3, 7, 2, 8)]
+    eng = RKSEngine(mols, level=0, precision="mixed", guess="minao")
+    eng.device_setup()
+    eng.D.copy_(eng.D0)
+    P = eng.plan
+    eng.xc()
+    torch.cuda.synchronize()
+    ref_e, ref_v = eng.exc.cpu().numpy().copy(), eng.Vxc.cpu().numpy().copy()
+    for tiles in (1, 3, 16):
+        check(lib().b2_plan_set_xc_tiles(P.h, tiles), "b2_plan_set_xc_tiles")
+        eng.xc()
+        torch.cuda.synchronize()
+        np.testing.assert_allclose(eng.exc.cpu().numpy(), ref_e, rtol=1e-6)
+        np.testing.assert_allclose(eng.Vxc.cpu().numpy(), ref_v, atol=1e-5 * np.abs(ref_v).max())
+    check(lib().b2_plan_set_xc_tiles(P.h, 0), "b2_plan_set_xc_tiles")
+    act = torch.tensor([1, 0, 1, 0, 1, 1, 0], dtype=torch.int32, device=cuda)
+    eng.Vxc.fill_(7.0)
+    eng.exc.fill_(7.0)
+    eng.xc(active=act)
+    torch.cuda.synchronize()
+    V, E = eng.Vxc.cpu().numpy(), eng.exc.cpu().numpy()
+    for mi in range(len(mols)):
+        if act[mi].item():
+            assert abs(E[mi] - ref_e[mi]) <= 1e-6 * abs(ref_e[mi])
+            np.testing.assert_allclose(P.unpack(V, mi), P.unpack(ref_v, mi), atol=1e-5 * np.abs(ref_v).max())
+        else:
+            assert E[mi] == 7.0 and np.all(P.unpack(V, mi) == 7.0)
+    idx = np.array([0, 3, 6], np.int32)
+    check(lib().b2_plan_set_subset(P.h, ptr(idx), len(idx)), "b2_plan_set_subset")
+    sub_act = torch.zeros(len(mols), dtype=torch.int32, device=cuda)
+    sub_act[torch.from_numpy(idx.astype(np.int64)).to(cuda)] = 1
+    eng.xc(active=sub_act)
+    torch.cuda.synchronize()
+    check(lib().b2_plan_set_subset(P.h, None, 0), "b2_plan_set_subset")
+    for mi in idx:
+        np.testing.assert_allclose(P.unpack(eng.Vxc.cpu().numpy(), mi), P.unpack(ref_v, mi),
+                                   atol=1e-5 * np.abs(ref_v).max())
+    st = ctypes.c_int(-1)
+    check(lib().b2_xc_tc_status(1, ctypes.byref(st)), "b2_xc_tc_status")
+    assert st.value == 0
     eng.close()
 
 

@@ -170,3 +170,30 @@ def test_nanodft_thresholds(cuda):
     s8[np.abs(s8) <= thr_eri] = 0.0
     ref = rks.scf(s.S, s.T, s.V, s.D0, s8, s.ao, s.weights, mol.nelectron // 2, s.E_nuc, its=12)
     np.testing.assert_allclose(E[:, 0] / HARTREE_TO_EV, ref["energies"][:, 0], atol=1e-6)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_scf_iterate_entry_equals_individual_entries(cuda, precision):
+    # b2_scf_iterate (one C call per SCF iteration, over a b2_scf_state struct) against the same
+    # iteration made of the individual entry points, on an uneven batch with one molecule inactive
+    rng = np.random.default_rng(21)
+    mols = [Mole(random_molecule(rng, k)) for k in (1, 4, 2, 7)]
+    out = {}
+    for path in ("iterate", "entries"):
+        eng = RKSEngine(mols, level=0, precision=precision, guess="minao")
+        eng.prepare()
+        eng.initial()
+        eng.active[2] = 0
+        E = []
+        for _ in range(6):
+            (eng.step if path == "iterate" else eng.step_entries)()
+            E.append(eng.energy.view(len(mols), 5).cpu().numpy().copy())
+        torch.cuda.synchronize()
+        out[path] = (np.array(E), eng.iter.cpu().numpy().copy(), eng.diffJK.cpu().numpy().copy())
+        eng.close()
+    Ei, it_i, dj_i = out["iterate"]
+    Ee, it_e, dj_e = out["entries"]
+    np.testing.assert_array_equal(it_i, [6, 6, 0, 6])
+    np.testing.assert_array_equal(it_i, it_e)
+    np.testing.assert_allclose(Ei, Ee, atol=1e-9, rtol=0)
+    np.testing.assert_allclose(dj_i, dj_e, atol=1e-9, rtol=0)
