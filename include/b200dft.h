@@ -73,6 +73,10 @@ int b2_plan_set_xc_impl(b2_plan_t plan, int impl);
 /* Grid tiles (128 points) per CTA of the tensor-core XC kernel; 0 restores the automatic
  * choice.  Clears any molecule subset set with b2_plan_set_subset.  No reference counterpart. */
 int b2_plan_set_xc_tiles(b2_plan_t plan, int tiles_per_cta);
+/* Grid tiles per work item of the per-bucket tensor-core XC kernel, one value per orbital bucket
+ * (host int[5]: nao <= 16, 32, 48, 64, more; 0 = the plan-wide value).  Set by the autotuner
+ * (b200dft.autotune).  Clears any molecule subset.  No reference counterpart. */
+int b2_plan_set_xc_bucket_tiles(b2_plan_t plan, const int *tiles);
 /* Error code of the tensor-core XC kernel's bounded waits (0 = none); reset != 0 clears it. */
 int b2_xc_tc_status(int reset, int *status);
 

@@ -162,7 +162,7 @@ class RKSEngine:
     """
 
     def __init__(self, mols, level=0, precision="fp64", setups=None, device=None, jk_chunk=None,
-                 plan=None, guess="minao", net=None, eri_threshold=0.0):
+                 plan=None, guess="minao", net=None, eri_threshold=0.0, tuned=True):
         _require_cuda()
         self.mols = list(mols)
         self.level = level
@@ -204,6 +204,9 @@ class RKSEngine:
             self.chol_status = torch.zeros(nm, dtype=torch.int32, device=dev)
             self._tmpl = (tmpl, toff)
             self._setup_done = False
+        if tuned:                           # recorded autotuner choices of this device, if any
+            from .autotune import apply
+            apply(P)
         self.eri = torch.empty(max(1, P.n_eri), dtype=rdt, device=dev)
         self.eri_x = torch.empty(max(1, P.n_eri), dtype=rdt, device=dev)   # exchange list for J/K
         self.jk_impl = "pairs"      # "pairs": two products over the s8 and exchange lists; "s8"

@@ -287,6 +287,19 @@ int b2_plan_set_xc_tiles(void *plan, int tiles_per_cta) {
   return b2_xc_set_tpc(*P, tiles_per_cta);
 }
 
+int b2_plan_set_xc_bucket_tiles(void *plan, const int *tiles) {
+  if (!plan || !tiles) return B2_ERR_ARG;
+  B2PlanDev *P = (B2PlanDev *)plan;
+  if (!P->g.grid_off) return B2_ERR_ARG;
+  for (int b = 0; b < B2_NBKT; ++b)
+    if (tiles[b] < 0 || tiles[b] > 1024) return B2_ERR_ARG;
+  b2_subset_free(P);                  // subset tables derive from the tile split
+  for (int b = 0; b < B2_NBKT; ++b) P->g.xq_tpc[b] = tiles[b];
+  std::vector<int> all(P->h.nmol);
+  for (int m = 0; m < P->h.nmol; ++m) all[m] = m;
+  return b2_xq_build(*P, all, &P->g.xq_items, P->g.xq_off_h);
+}
+
 int b2_xc_tc_status(int reset, int *status) {
   if (!status) return B2_ERR_ARG;
   const int v = b2_xc_tc_status_read(reset);

@@ -7,6 +7,8 @@
 // number of kernels this library has launched (monotonic; read with b2_launch_count)
 void b2_count_launches(long long n);
 
+#define B2_NBKT 5              // orbital buckets nao <= 16, 32, 48, 64, more
+
 struct B2GridDev {             // grid layout registered with b2_grid_set
   long long n_points = 0, n_gblk = 0, n_xblk32 = 0, n_xblk64 = 0, n_xblk_tc = 0, n_ao = 0;
   long long *grid_off = nullptr, *gblk_off = nullptr, *ao_off = nullptr;
@@ -19,9 +21,8 @@ struct B2GridDev {             // grid layout registered with b2_grid_set
   void *xq_items = nullptr;                         // per-bucket XC work items (molecule, tile)
   std::vector<long long> xq_off_h;                  // B2_NBKT + 1 bucket starts in xq_items
   int *xq_queue = nullptr;                          // B2_NBKT work-queue counters
+  int xq_tpc[B2_NBKT] = {0, 0, 0, 0, 0};            // tiles per item per bucket (0: tpc_tc)
 };
-
-#define B2_NBKT 5              // orbital buckets nao <= 16, 32, 48, 64, more
 
 struct B2SubsetDev {           // compacted work tables for a subset of the batch's molecules
   int n = 0;                   // 0: no subset (full tables)

@@ -287,6 +287,7 @@ int b2_grid_setup(B2PlanDev &P, const long long *grid_off_host) {
 
 int b2_xc_set_tpc(B2PlanDev &P, int tpc) {
   if (!P.g.grid_off || tpc < 0) return B2_ERR_ARG;
+  for (int b = 0; b < B2_NBKT; ++b) P.g.xq_tpc[b] = 0;    // one value for every bucket
   std::vector<long long> xtc;
   b2_xc_split(P.g.grid_off_h, P.h.nmol, 128, P.g.tpc_tc, xtc, tpc);
   long long *d = nullptr;

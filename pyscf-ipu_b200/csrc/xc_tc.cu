@@ -1016,8 +1016,9 @@ static int b2_xq_launch(const B2PlanDev &P, const B2XtItem *items, int n_items, 
     occ[dev] = std::max(1, o) * nsm;
   }
   const int grid = std::min(n_items, occ[dev]);
+  const int tpc = P.g.xq_tpc[Q - 1] > 0 ? P.g.xq_tpc[Q - 1] : std::max(1, P.g.tpc_tc);
   k_xc_tq<Q><<<grid, B2_XT_NT, sm, st>>>(P.mols, P.shells, items, n_items, queue, P.g.grid_off,
-                                          P.g.tpc_tc, active, coords, w, D, V, exc);
+                                          tpc, active, coords, w, D, V, exc);
   return B2_OK;
 }
 
@@ -1071,7 +1072,8 @@ static void b2_xq_items(const B2PlanDev &P, const std::vector<int> &mols, int tp
   for (int m : mols) {
     const int b = std::min(B2_NBKT - 1, (P.h.mols[m].nao - 1) / 16);
     const long long nt = (P.g.grid_off_h[m + 1] - P.g.grid_off_h[m] + B2_XT_PT - 1) / B2_XT_PT;
-    for (long long t = 0; t < nt; t += tpc) per[b].push_back(B2XtItem{m, (int)t});
+    const int tb = P.g.xq_tpc[b] > 0 ? P.g.xq_tpc[b] : tpc;
+    for (long long t = 0; t < nt; t += tb) per[b].push_back(B2XtItem{m, (int)t});
   }
   items.clear();
   for (int b = 0; b < B2_NBKT; ++b) {
