@@ -232,6 +232,13 @@ typedef struct {
  * one capture serves every later iteration. */
 int b2_scf_iterate(b2_plan_t plan, const b2_scf_state *state, void *stream);
 
+/* n block copies dst[dst_off[k] .. + len[k]) = src[src_off[k] .. + len[k]) (bytes; the offset and
+ * length arrays are device int64[n]).  Carries the state of molecules still iterating (their
+ * s8 and exchange lists) into the layout of the plan that refills the batch's converged slots.
+ * No reference counterpart. */
+int b2_copy_blocks(int n, const void *src, void *dst, const int64_t *src_off, const int64_t *dst_off,
+                   const int64_t *len, void *stream);
+
 /* Single-molecule convenience mirroring the reference's native entry int2e_sph
  * (int2e_sph.cpp:6750): host libcint arrays in, all s8 ERIs of the molecule out (device). */
 int b2_int2e_sph_s8(const int *atm, int natm, const int *bas, int nbas, const double *env,

@@ -59,6 +59,7 @@ SIGNATURES = {
     "b2_grad": [_P, _I, _D, _P, _P, _P, _P, _P, _P, _P, _P],
     "b2_eri_threshold": [_P, _I, _P, _D, _P],
     "b2_scf_iterate": [_P, _P, _P],
+    "b2_copy_blocks": [_I, _P, _P, _P, _P, _P, _P],
 }
 
 

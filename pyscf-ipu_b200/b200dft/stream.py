@@ -190,14 +190,17 @@ class RowWriter:
 
 def run_stream(n_total, batch=4096, seed=0, level=0, precision="mixed", guess="learned", out=None,
                fmt="parquet", workers=None, max_heavy=9, net=None, e_tol=1e-6, diis_tol=1e-4,
-               rank=0, world=1, gradient=False, resume=False):
+               rank=0, world=1, gradient=False, resume=False, refill=False):
     """Generate ``n_total`` molecules and write one row each; returns throughput and iteration
     statistics (the streaming configuration: molecules/s, p50/p99 iterations).  With
     ``world`` > 1 this process handles the stream chunks of ``rank`` (round robin) only.  With
     ``gradient`` each row also carries the molecule's nuclear gradient (force labels, dE/dR in
     Ha/Bohr, flattened like ``pos``; nanoDFT.py:440-477 on the SCF's final orbitals).  With
     ``resume`` the molecules whose rows ``out`` already holds are not generated again and the new
-    rows are appended (dft.py:247-283)."""
+    rows are appended (dft.py:247-283).  With ``refill`` the batch's slots are refilled from the
+    stream as molecules converge (b200dft.refill.run_refill) instead of running whole batches."""
+    if refill and gradient:
+        raise ValueError("force labels are computed per whole batch: use refill=False with gradient")
     if guess == "learned" and net is None:
         from .train_guess import load
         net = load()
@@ -269,14 +272,34 @@ def run_stream(n_total, batch=4096, seed=0, level=0, precision="mixed", guess="l
             queued.append(items)
             yield [it[2] for it in items]
 
+    byid = {}
+
+    def stream_mols():                    # molecules in stream order, their items kept by index
+        k = 0
+        for ms in batches():
+            for it in queued.popleft():
+                byid[k] = it
+                k += 1
+                yield it[2]
+
+    def results():
+        if refill:
+            from .refill import run_refill
+            for ids, _, res in run_refill(stream_mols(), slots=batch, level=level, precision=precision,
+                                          guess=guess, net=net, e_tol=e_tol, diis_tol=diis_tol):
+                res["host_ms"] = {"scf": res["host_ms"]["iterate"]}
+                yield [byid.pop(int(i)) for i in ids], res
+        else:
+            # run_batches builds each next plan on its worker thread once the current batch's ERI
+            # work is queued, and reuses the engine memory from batch to batch
+            for _, res in run_batches(batches(), level=level, precision=precision, guess=guess, net=net,
+                                      gradient=gradient, e_tol=e_tol, diis_tol=diis_tol):
+                yield queued.popleft(), res
+
     try:
-        # run_batches builds each next plan on its worker thread once the current batch's ERI
-        # work is queued, and reuses the engine memory from batch to batch
-        for _, res in run_batches(batches(), level=level, precision=precision, guess=guess, net=net,
-                                  gradient=gradient, e_tol=e_tol, diis_tol=diis_tol):
-            items = queued.popleft()
+        for items, res in results():
             h = res["host_ms"]
-            stats["gpu_s"] += 1e-3 * (h["engine"] + h["prepare"] + h["scf"] + h.get("gradient", 0.0))
+            stats["gpu_s"] += 1e-3 * (h.get("engine", 0.0) + h.get("prepare", 0.0) + h["scf"] + h.get("gradient", 0.0))
             its = res["iterations"]
             stats["iterations"].append(its)
             stats["converged"] += int((its > 0).sum())
@@ -315,10 +338,11 @@ def main(argv=None):
     ap.add_argument("--workers", type=int, default=None)
     ap.add_argument("--gradient", action="store_true", help="also write each molecule's nuclear gradient")
     ap.add_argument("--resume", action="store_true", help="skip the molecules whose rows --out already holds")
+    ap.add_argument("--refill", action="store_true", help="refill converged slots from the stream")
     a = ap.parse_args(argv)
     fmt = a.format or ("csv" if a.out and a.out.endswith((".csv", ".csv.gz", ".gz")) else "parquet")
     r = run_stream(a.n, batch=a.batch, seed=a.seed, level=a.level, precision=a.precision, guess=a.guess,
-                   out=a.out, fmt=fmt, workers=a.workers, gradient=a.gradient, resume=a.resume)
+                   out=a.out, fmt=fmt, workers=a.workers, gradient=a.gradient, resume=a.resume, refill=a.refill)
     print(json.dumps(r))
     return r
 

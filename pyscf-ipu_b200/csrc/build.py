@@ -21,7 +21,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + HERE, "-I" + INC,
           "--expt-relaxed-constexpr", "-Wno-deprecated-gpu-targets"]
 LIB_SRCS = ["capi.cu", "eri.cu", "jk.cu", "jk_symv.cu", "xc.cu", "scf.cu", "setup.cu", "xc_direct.cu", "xc_tc.cu", "learned.cu",
-            "grad.cu"]
+            "grad.cu", "blocks.cu"]
 
 
 def _newer(target, deps):

@@ -468,6 +468,16 @@ int b2_energy(void *plan, const int *active, const double *D, const double *Hcor
                           (cudaStream_t)stream);
 }
 
+int b2_launch_copy_blocks(int n, const void *src, void *dst, const long long *src_off,
+                          const long long *dst_off, const long long *len, cudaStream_t st);
+
+int b2_copy_blocks(int n, const void *src, void *dst, const int64_t *src_off, const int64_t *dst_off,
+                   const int64_t *len, void *stream) {
+  if (n < 0 || (n > 0 && (!src || !dst || !src_off || !dst_off || !len))) return B2_ERR_ARG;
+  return b2_launch_copy_blocks(n, src, dst, (const long long *)src_off, (const long long *)dst_off,
+                               (const long long *)len, (cudaStream_t)stream);
+}
+
 int b2_scf_iterate(void *plan, const b2_scf_state *S, void *stream) {
   if (!plan || !S) return B2_ERR_ARG;
   if (!S->Hcore || !S->S || !S->Linv || !S->weights || !S->enuc || !S->eri || !S->D || !S->J || !S->K ||

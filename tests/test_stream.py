@@ -271,3 +271,37 @@ def test_stream_force_labels_match_engine(tmp_path):
         assert len(t["gradient"][k]) == 3 * m.natm
         np.testing.assert_allclose(np.array(t["gradient"][k]).reshape(-1, 3), g[a0:a0 + m.natm], atol=1e-6, rtol=0)
         a0 += m.natm
+
+
+def _stub_run_refill(mols, slots=4, **kw):
+    """retires molecules out of stream order (every other slot first), like a refill would"""
+    buf, k = [], 0
+    for m in mols:
+        buf.append((k, m))
+        k += 1
+    order = buf[1::2] + buf[0::2]
+    for s in range(0, len(order), 3):
+        part = order[s:s + 3]
+        n = len(part)
+        mo = np.zeros((n, 72))
+        mo[:, :2] = [-0.5, 0.1]
+        e = np.array([-40.0 - i for i, _ in part])
+        yield np.array([i for i, _ in part]), [m for _, m in part], {
+            "energy": e, "iterations": np.full(n, 6, np.int32), "converged": np.ones(n, bool), "mo_energy": mo,
+            "last5": np.repeat(e[:, None], 5, 1), "diis_err": np.zeros(n), "its_run": 6,
+            "host_ms": {"iterate": 0.0}}
+
+
+def test_stream_refill_rows_follow_their_molecules(tmp_path, monkeypatch):
+    """with slot refill the results come back out of order; each row still carries its own
+    molecule's result"""
+    import pandas as pd
+    from b200dft import refill, stream
+    monkeypatch.setattr(refill, "run_refill", _stub_run_refill)
+    path = str(tmp_path / "rows.parquet")
+    r = stream.run_stream(11, batch=4, seed=3, guess="minao", out=path, workers=2, refill=True)
+    assert r["molecules"] == 11 and r["converged"] == 11
+    t = pd.read_parquet(path)
+    idx = [int(s.split(":")[2]) for s in t["smile"]]
+    assert sorted(idx) == list(range(11)) and idx != list(range(11))
+    np.testing.assert_allclose(t["energy"].to_numpy(), (-40.0 - np.array(idx)) * 27.2114079527)
