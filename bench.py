@@ -302,6 +302,8 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-mode", action="store_true", help="timed steps only (for ncu captures)")
+    ap.add_argument("--stream", type=int, default=204800,
+                    help="streaming leg: molecules through the public stream API with slot refill (0: off)")
     ap.add_argument("--grad", type=int, default=0,
                     help="also time the nuclear gradient (b2_grad) of the first N converged molecules (0: off)")
     a = ap.parse_args()
@@ -424,6 +426,12 @@ def main():
         except Exception as e:  # noqa: BLE001
             cfg2 = {"error": f"{type(e).__name__}: {e}"}
 
+    # ---- streaming generation (config 5): molecules generated on host workers, batched SCF with
+    # slot refill and the learned guess, results to host memory, through b200dft.stream
+    stream = None
+    if rank == 0 and not a.profile_mode and a.stream > 0:
+        stream = stream_leg(a, net, parity)
+
     # ---- plain FP64 per-molecule GPU path on a sample (same convergence rule, minao guess):
     # wall clock per molecule (plan, engine, eager SCF, close) and its device time
     plain = None
@@ -521,13 +529,33 @@ def main():
                     "fallbacks_to_minao": int(res["fell_back"].sum().item()), "mean_its": float(iters[conv].mean()) if conv.any() else None,
                     "p50_its": float(np.percentile(iters[conv], 50)) if conv.any() else None,
                     "p99_its": float(np.percentile(iters[conv], 99)) if conv.any() else None},
-            "plain_fp64_per_molecule": plain, "learned_guess": learned, "config2": cfg2,
+            "plain_fp64_per_molecule": plain, "learned_guess": learned, "config2": cfg2, "stream": stream,
         }
         if grad is not None:
             out["gradient"] = grad
         print(json.dumps(out))
     if world > 1:
         dist.destroy_process_group()
+
+
+def stream_leg(a, net, parity):
+    """config 5: ``a.stream`` seeded molecules of the batched distribution through
+    b200dft.stream.run_stream (host generation workers, 4096 slots refilled as molecules converge,
+    learned guess, rows formed on the host but not written), wall clock; plus whole batches
+    without refill over the first 40960 of them, for comparison.  The plain FP64 path's
+    iterations come from the whole-batch parity run (MINAO guess, same convergence rule)."""
+    from b200dft.stream import run_stream
+    kw = dict(batch=4096, seed=a.seed + 500, level=a.level, precision=a.precision, guess=a.guess, net=net)
+    r = run_stream(a.stream, refill=True, **kw)
+    nb = min(a.stream, 40960)
+    rb = run_stream(nb, refill=False, **kw)
+    keep = ("molecules", "wall_s", "molecules_per_s", "converged", "p50_iterations", "p99_iterations",
+            "mean_iterations", "workers")
+    out = {"refill": {k: r[k] for k in keep}, "whole_batches": {k: rb[k] for k in keep},
+           "api": "b200dft.stream.run_stream (generation workers -> batched SCF -> host rows)"}
+    if parity is not None and "plain_its" in parity:
+        out["plain_fp64_iterations"] = parity["plain_its"]
+    return out
 
 
 def spawn_ranks(n):
@@ -568,7 +596,10 @@ def batch_parity(eng, mols, a, res):
         for o in range(0, n, step):
             dERI = max(dERI, float((eng.eri[o:o + step].double() - e64.eri[o:o + step]).abs().max().item()))
         torch.cuda.synchronize()
-        return {"n": int(len(mols)), "reference": "plain FP64 GPU path (float64 ERIs/J/K/grid, MINAO guess), "
+        it64 = r64["iterations"].cpu().numpy()[c64]
+        plain_its = {"p50": float(np.percentile(it64, 50)), "p99": float(np.percentile(it64, 99)),
+                     "mean": float(it64.mean())} if c64.any() else None
+        return {"plain_its": plain_its, "n": int(len(mols)), "reference": "plain FP64 GPU path (float64 ERIs/J/K/grid, MINAO guess), "
                                                  "same convergence rule",
                 "max_abs_dE_Ha": float(dE.max()), "n_over_1e-4": int((dE > 1e-4).sum()),
                 "mean_abs_dE_Ha": float(dE.mean()), "converged_mixed": int(c32.sum()), "converged_fp64": int(c64.sum()),
