@@ -4,7 +4,8 @@ The reference starts every SCF from MINAO (pyscf_utils/minao.py:5-123, dft.py:22
 predicts D0 per atom-pair block from the geometry instead; the plain SCF still iterates every
 molecule to the same convergence test, and ``RKSEngine.run_converged(fallback=...)`` restarts a
 molecule from MINAO when its DIIS error rises.  Architecture (SchNet-style continuous-filter
-message passing, feature size 128, 4 layers, 32 Gaussians on 0-5 A; ~0.73M parameters):
+message passing, feature size 128, 4 layers, 32 Gaussians on 0-5 A; hidden widths HL (layers,
+site head) and HR (pair head): 384 / 576 give 0.97M parameters, 256 / 512 0.73M):
 
   h^0_a = E[type_a];  phi_p = rbf(r_p) Wf + bf;  m_a = sum_{p -> a} phi_p * h_src
   h^t   = h^{t-1} + silu(m Wa + ba) Wb + bb                                   (t = 1..4)
@@ -25,7 +26,8 @@ import torch
 
 from ._lib import lib, check, ptr, stream_handle
 
-F, R, HL, HR, L = 128, 32, 256, 512, 4
+F, R, L = 128, 32, 4
+HL, HR = 384, 576                       # hidden widths of new networks (a weights file records its own)
 NT = 5
 TYPE = {1: 0, 6: 1, 7: 2, 8: 3, 9: 4}
 RC = 5.0 / 0.52917721092                # 5 Angstrom in Bohr
@@ -61,7 +63,8 @@ def _lib():
     return L_
 
 
-def layout():
+def layout(hl=HL, hr=HR):
+    HL, HR = hl, hr
     shapes = [("E", (NT, F))]
     for t in range(L):
         shapes += [(f"Wf{t}", (R, F)), (f"bf{t}", (F,)), (f"Wa{t}", (F, HL)), (f"ba{t}", (HL,)),
@@ -71,10 +74,10 @@ def layout():
     return shapes
 
 
-def init_params_np(seed=0):
+def init_params_np(seed=0, hl=HL, hr=HR):
     rng = np.random.default_rng(seed)
     p = {}
-    for name, shp in layout():
+    for name, shp in layout(hl, hr):
         if name[0] in "bc":
             p[name] = np.zeros(shp)
         elif name == "E":
@@ -148,18 +151,19 @@ class Batch:
 class GuessNet:
     """Parameters, forward/backward through the CUDA kernels, Adam, D0 prediction."""
 
-    def __init__(self, seed=0, device="cuda", bf16=True, tensor_cores=True):
+    def __init__(self, seed=0, device="cuda", bf16=True, tensor_cores=True, hl=HL, hr=HR):
         self.device = torch.device(device)
+        self.hl, self.hr = hl, hr
         # 0: float32 SIMT (exact, for checks); 1: bf16-rounded SIMT; 2: bf16 tensor cores (mma.sync)
         self.bf16 = (2 if tensor_cores else 1) if bf16 else 0
-        self.shapes = layout()
+        self.shapes = layout(hl, hr)
         self.offsets = {}
         o = 0
         for n, s in self.shapes:
             self.offsets[n] = (o, s)
             o += int(np.prod(s))
         self.n_params = o
-        p = init_params_np(seed)
+        p = init_params_np(seed, hl, hr)
         flat = np.concatenate([p[n].reshape(-1) for n, _ in self.shapes]).astype(np.float32)
         self.params = torch.from_numpy(flat).to(self.device)
         self.grads = torch.zeros_like(self.params)

@@ -84,12 +84,15 @@ def evaluate(net, batches):
 
 def save(net, path=WEIGHTS):
     os.makedirs(os.path.dirname(path), exist_ok=True)
-    np.savez_compressed(path, params=net.params.cpu().numpy(), n_params=net.n_params)
+    np.savez_compressed(path, params=net.params.cpu().numpy(), n_params=net.n_params, hl=net.hl, hr=net.hr)
 
 
 def load(path=WEIGHTS, device="cuda"):
-    net = GuessNet(device=device)
     d = np.load(path)
+    # files written before the hidden widths were recorded hold the 256 / 512 network
+    hl = int(d["hl"]) if "hl" in d else 256
+    hr = int(d["hr"]) if "hr" in d else 512
+    net = GuessNet(device=device, hl=hl, hr=hr)
     if int(d["n_params"]) != net.n_params:
         raise ValueError("weights do not match the network layout")
     net.params.copy_(torch.from_numpy(d["params"]).to(net.device))

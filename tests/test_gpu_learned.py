@@ -18,7 +18,7 @@ def _mols():
 
 def test_forward_matches_reference(cuda):
     mols = _mols()
-    net = GuessNet(seed=0, bf16=False)
+    net = GuessNet(seed=0, bf16=False, hl=nno.HL, hr=nno.HR)
     p = nno.init_params(0)
     B = Batch(mols)
     z, y, _ = net.forward(B)
@@ -33,7 +33,7 @@ def test_forward_matches_reference(cuda):
 
 def test_gradients_match_reference(cuda):
     m = _mols()[0]
-    net = GuessNet(seed=0, bf16=False)
+    net = GuessNet(seed=0, bf16=False, hl=nno.HL, hr=nno.HR)
     p = nno.init_params(0)
     rng = np.random.default_rng(1)
     Dt = rng.normal(size=(m.nao, m.nao))
