@@ -705,17 +705,23 @@ k_xc_tq(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
     // (the D tiles are read only by the X product, issued after the first tile's barrier)
     double e_part = 0.0;
     bool first = true;
+    // point of this thread in the next tile, loaded one tile ahead (the loads' latency overlaps
+    // the current tile's work)
+    double qx = 0, qy = 0, qz = 0, qw = 0;
+    {
+      const long long g1 = (long long)item.t0 * B2_XT_PT + p;
+      if (g1 < G) { qx = cm[3 * g1]; qy = cm[3 * g1 + 1]; qz = cm[3 * g1 + 2]; qw = wm[g1]; }
+    }
     for (int tt = 0; tt < tpc; ++tt) {
       const long long g0 = ((long long)item.t0 + tt) * B2_XT_PT;
       if (g0 >= G) break;
       const int np = (int)min((long long)B2_XT_PT, G - g0);
       const bool valid = p < np;
-      double px = 0, py = 0, pz = 0, wd = 0;
-      if (valid) {
-        px = cm[3 * (g0 + p)];
-        py = cm[3 * (g0 + p) + 1];
-        pz = cm[3 * (g0 + p) + 2];
-        wd = wm[g0 + p];
+      const double px = qx, py = qy, pz = qz, wd = qw;     // zero for points past the grid
+      {
+        const long long g1 = g0 + B2_XT_PT + p;
+        qx = qy = qz = qw = 0.0;
+        if (tt + 1 < tpc && g1 < G) { qx = cm[3 * g1]; qy = cm[3 * g1 + 1]; qz = cm[3 * g1 + 2]; qw = wm[g1]; }
       }
       const float wp = (float)wd;
       // ---- radial factors per orbital (tensor memory) and AO values (registers)
