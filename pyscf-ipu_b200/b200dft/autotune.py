@@ -124,6 +124,7 @@ def main(argv=None):
     ap.add_argument("--nmol", type=int, default=4096)
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--no-save", action="store_true")
+    ap.add_argument("--out", default=TABLE, help="table file to record the choice in")
     a = ap.parse_args(argv)
     mols = [Mole(s) for s in config3_batch(a.nmol, seed=a.seed)]
     eng = RKSEngine(mols, precision="mixed", guess="minao", tuned=False)
@@ -135,7 +136,8 @@ def main(argv=None):
         eng.close()
     print(json.dumps({"choice": choice, "times_ms": times}))
     if not a.no_save:
-        save(choice, times, device_key(), workload=f"{a.nmol} molecules, config-3 distribution, seed {a.seed}")
+        save(choice, times, device_key(), path=a.out,
+             workload=f"{a.nmol} molecules, config-3 distribution, seed {a.seed}")
 
 
 if __name__ == "__main__":
