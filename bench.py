@@ -13,6 +13,7 @@ libcint host arrays, host->device copies, results copied back).
     python bench.py [--gpus N] [--steps K] [--warmup W] [--nmol M] [--impl b200|reference]
 """
 import argparse
+import ctypes
 import json
 import os
 import subprocess
@@ -118,10 +119,23 @@ def kernel_rooflines(eng, precision):
     quartets, prim = quartet_counts(eng.mols)
     prec = 64 if precision == "fp64" else 32
     eri_ms = _timed(lambda: check(lib().b2_eri_s8(P.h, prec, ptr(eng.eri), stream_handle()), "b2_eri_s8"), 3)
-    out.append({"kernel": "k_eri_*", "bound": "fp32 simt", "ms_per_launch": eri_ms,
-                "shell_quartets_per_s": quartets / (eri_ms / 1e3),
-                "primitive_quartets_per_s": prim / (eri_ms / 1e3), "shell_quartets": quartets,
-                "primitive_quartets_unscreened": prim})
+    e = {"kernel": "k_eri_fl / k_eri_sq (16 class kernels)", "bound": "fp32 simt", "ms_per_launch": eri_ms,
+         "shell_quartets_per_s": quartets / (eri_ms / 1e3), "shell_quartets": quartets,
+         "primitive_quartets_unscreened": prim}
+    if prec == 32:
+        # evaluated primitive quartets and their arithmetic by the per-class counts of
+        # csrc/eri_flops.h (generated from the kernels' own code), against the FP32 FMA rate
+        # measured on this GPU by the library's microbenchmark
+        work = np.zeros(3)
+        pk = ctypes.c_double(0.0)
+        check(lib().b2_eri_work(P.h, ptr(work)), "b2_eri_work")
+        check(lib().b2_fp32_peak(ctypes.byref(pk)), "b2_fp32_peak")
+        tf = work[1] / (eri_ms / 1e3) / 1e12
+        e.update({"achieved": tf, "peak": pk.value, "unit": "TFLOP/s", "frac": tf / pk.value,
+                  "peak_kind": "measured FP32 FMA (b2_fp32_peak)", "primitive_quartets": work[0],
+                  "algorithmic_flops_per_launch": work[1], "special_ops_per_launch": work[2],
+                  "primitive_quartets_per_s": work[0] / (eri_ms / 1e3)})
+    out.append(e)
     return out
 
 

@@ -232,6 +232,17 @@ typedef struct {
  * one capture serves every later iteration. */
 int b2_scf_iterate(b2_plan_t plan, const b2_scf_state *state, void *stream);
 
+/* Work of the float32 ERI kernels for this plan (measurement; synchronises the device): out[0] =
+ * primitive quartets evaluated (surviving bra x ket primitive pairs of every shell quartet),
+ * out[1] = their arithmetic by the per-class counts generated from the kernels' own code
+ * (csrc/eri_flops.h), out[2] = their special-function operations.  No reference counterpart. */
+int b2_eri_work(b2_plan_t plan, double *out);
+
+/* Measured FP32 FMA rate of the current GPU in TFLOP/s (every SM full of threads running
+ * independent FMA chains; CUDA events around one launch; synchronises the device).  The
+ * denominator of the ERI kernels' roofline fraction.  No reference counterpart. */
+int b2_fp32_peak(double *tflops);
+
 /* n block copies dst[dst_off[k] .. + len[k]) = src[src_off[k] .. + len[k]) (bytes; the offset and
  * length arrays are device int64[n]).  Carries the state of molecules still iterating (their
  * s8 and exchange lists) into the layout of the plan that refills the batch's converged slots.

@@ -60,6 +60,8 @@ SIGNATURES = {
     "b2_eri_threshold": [_P, _I, _P, _D, _P],
     "b2_scf_iterate": [_P, _P, _P],
     "b2_copy_blocks": [_I, _P, _P, _P, _P, _P, _P],
+    "b2_eri_work": [_P, _P],
+    "b2_fp32_peak": [_P],
 }
 
 

@@ -3,6 +3,7 @@
 // layout into the next plan's when converged molecules retire and new ones take their slots.
 #include <cstdint>
 #include "device_plan.cuh"
+#include "devmem.cuh"
 
 // one CTA per block: 16-byte vectors over the 16-byte-aligned middle, single bytes at the ends
 __global__ void __launch_bounds__(256)
@@ -32,5 +33,52 @@ int b2_launch_copy_blocks(int n, const void *src, void *dst, const long long *sr
   k_copy_blocks<<<n, 256, 0, st>>>((const unsigned char *)src, (unsigned char *)dst, src_off, dst_off, len);
   b2_count_launches(1);
   B2_CUDA_TRY(cudaGetLastError());
+  return B2_OK;
+}
+
+// FP32 FMA peak of this GPU, measured (b2_fp32_peak): every SM full of threads, each running 8
+// independent FMA chains; the result is stored only under a condition no value meets, so the
+// work is kept.  Timed with CUDA events around one launch after a warm-up launch.
+__global__ void __launch_bounds__(256)
+k_fma_peak(int iters, float seed, float *__restrict__ sink) {
+  float a[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) a[c] = seed + 0.001f * (float)(threadIdx.x + c);
+  const float m = 0.9999f, b = 1e-7f;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r)
+#pragma unroll
+      for (int c = 0; c < 8; ++c) a[c] = fmaf(a[c], m, b);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) s += a[c];
+  if (s == -12345.0f) sink[blockIdx.x] = s;
+}
+
+int b2_measure_fp32_peak(double *tflops) {
+  int dev = 0, nsm = 0;
+  B2_CUDA_TRY(cudaGetDevice(&dev));
+  B2_CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+  float *sink = nullptr;
+  B2_CUDA_TRY(b2_dmalloc_t(&sink, sizeof(float) * 8 * nsm));
+  cudaEvent_t e0, e1;
+  B2_CUDA_TRY(cudaEventCreate(&e0));
+  B2_CUDA_TRY(cudaEventCreate(&e1));
+  const int iters = 4096, grid = 8 * nsm;
+  k_fma_peak<<<grid, 256>>>(iters / 8, 1.0f, sink);           // warm-up
+  B2_CUDA_TRY(cudaEventRecord(e0));
+  k_fma_peak<<<grid, 256>>>(iters, 1.0f, sink);
+  B2_CUDA_TRY(cudaEventRecord(e1));
+  b2_count_launches(2);
+  B2_CUDA_TRY(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  B2_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b2_dfree(sink);
+  const double flops = 2.0 * 16 * 8 * (double)iters * 256.0 * grid;
+  *tflops = flops / (ms * 1e-3) / 1e12;
   return B2_OK;
 }

@@ -468,8 +468,15 @@ int b2_energy(void *plan, const int *active, const double *D, const double *Hcor
                           (cudaStream_t)stream);
 }
 
-int b2_launch_copy_blocks(int n, const void *src, void *dst, const long long *src_off,
-                          const long long *dst_off, const long long *len, cudaStream_t st);
+int b2_fp32_peak(double *tflops) {
+  if (!tflops) return B2_ERR_ARG;
+  return b2_measure_fp32_peak(tflops);
+}
+
+int b2_eri_work(void *plan, double *out) {
+  if (!plan || !out) return B2_ERR_ARG;
+  return b2_launch_eri_count(*(B2PlanDev *)plan, out);
+}
 
 int b2_copy_blocks(int n, const void *src, void *dst, const int64_t *src_off, const int64_t *dst_off,
                    const int64_t *len, void *stream) {

@@ -93,3 +93,8 @@ int b2_zero_active(const B2PlanDev &P, const int *active, double *A, double *B, 
 // per-bucket work items of the tensor-core XC kernel for `mols` (device array in *items,
 // bucket starts in off), P.g.tpc_tc tiles per item
 int b2_xq_build(const B2PlanDev &P, const std::vector<int> &mols, void **items, std::vector<long long> &off);
+// measurement and slot-refill helpers (eri.cu, blocks.cu)
+int b2_launch_eri_count(B2PlanDev &P, double *host_out);
+int b2_measure_fp32_peak(double *tflops);
+int b2_launch_copy_blocks(int n, const void *src, void *dst, const long long *src_off,
+                          const long long *dst_off, const long long *len, cudaStream_t st);

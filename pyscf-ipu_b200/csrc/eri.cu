@@ -17,6 +17,7 @@
 #include "eri_sq.cuh"
 #include "device_plan.cuh"
 #include "devmem.cuh"
+#include "eri_flops.h"
 
 template <typename T, int LI, int LJ, int LK, int LL>
 __global__ void __launch_bounds__(128)
@@ -641,4 +642,54 @@ int b2_build_pairs(B2PlanDev &P, cudaStream_t st) {
     B2_CUDA_TRY(cudaGetLastError());
   }
   return B2_OK;
+}
+
+// Work the float32 ERI kernels do for a plan: primitive quartets evaluated (bra survivors x ket
+// survivors of every shell quartet of the task list) and their arithmetic by the per-class
+// counts of eri_flops.h (generated from eri_sq.cuh by eri_flops_count.cu).  One thread per task.
+__global__ void __launch_bounds__(256)
+k_eri_count(const B2EriTask *__restrict__ tasks, long long n, const B2MolDev *__restrict__ mols,
+            const int *__restrict__ cls_list, const unsigned char *__restrict__ ppn, double fl, double sp,
+            double *__restrict__ out) {
+  __shared__ double red[3][8];
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  double q = 0;
+  if (t < n) {
+    const B2EriTask tk = tasks[t];
+    const B2MolDev md = mols[tk.mol];
+    const double nb = ppn[md.sp_off + tk.IJ];
+    int nq = 0;
+    for (int k = 0; k < tk.count; ++k) nq += ppn[md.sp_off + cls_list[md.sp_off + md.cls_start[tk.cls] + tk.start + k]];
+    q = nb * nq;
+  }
+  double v[3] = {q, q * fl, q * sp};
+  for (int c = 0; c < 3; ++c)
+    for (int o = 16; o > 0; o >>= 1) v[c] += __shfl_down_sync(0xffffffffu, v[c], o);
+  if ((threadIdx.x & 31) == 0)
+    for (int c = 0; c < 3; ++c) red[c][threadIdx.x >> 5] = v[c];
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double s = 0;
+    for (int w = 0; w < 8; ++w) s += red[threadIdx.x][w];
+    atomicAdd(&out[threadIdx.x], s);
+  }
+}
+
+int b2_launch_eri_count(B2PlanDev &P, double *host_out) {
+  int rc = b2_eri_task_upload(P, 32, nullptr);
+  if (rc) return rc;
+  double *d = nullptr;
+  B2_CUDA_TRY(b2_dmalloc_t(&d, 3 * sizeof(double)));
+  B2_CUDA_TRY(cudaMemset(d, 0, 3 * sizeof(double)));
+  const std::vector<long long> &g = P.eri_goff32;
+  for (int grp = 0; grp < 16; ++grp) {
+    const long long n = g[grp + 1] - g[grp];
+    if (n <= 0) continue;
+    k_eri_count<<<(unsigned)((n + 255) / 256), 256>>>(P.eri_tasks32 + g[grp], n, P.mols, P.cls_list, P.pp32_n,
+                                                       (double)B2_ERI_FLOPS[grp], (double)B2_ERI_SPECIAL[grp], d);
+    b2_count_launches(1);
+  }
+  rc = cudaMemcpy(host_out, d, 3 * sizeof(double), cudaMemcpyDeviceToHost) == cudaSuccess ? B2_OK : B2_ERR_CUDA;
+  b2_dfree(d);
+  return rc;
 }
