@@ -429,22 +429,19 @@ def main():
     # ---- parity of every molecule of the timed batch against the plain FP64 path
     parity = None
     if rank == 0 and not a.profile_mode:
-        parity = batch_parity(eng, mols, a, res)
+        parity = _guarded(batch_parity, eng, mols, a, res)
     learned = None
     if rank == 0 and not a.profile_mode and a.guess == "learned":
-        learned = learned_guess_criterion(mols, a, net)
+        learned = _guarded(learned_guess_criterion, mols, a, net)
     cfg2 = None
     if rank == 0 and not a.profile_mode:
-        try:
-            cfg2 = config2_report()
-        except Exception as e:  # noqa: BLE001
-            cfg2 = {"error": f"{type(e).__name__}: {e}"}
+        cfg2 = _guarded(config2_report)
 
     # ---- streaming generation (config 5): molecules generated on host workers, batched SCF with
     # slot refill and the learned guess, results to host memory, through b200dft.stream
     stream = None
     if rank == 0 and not a.profile_mode and a.stream > 0:
-        stream = stream_leg(a, net, parity)
+        stream = _guarded(stream_leg, a, net, parity)
 
     # ---- plain FP64 per-molecule GPU path on a sample (same convergence rule, minao guess):
     # wall clock per molecule (plan, engine, eager SCF, close) and its device time
@@ -479,7 +476,7 @@ def main():
     # GPU results of the same molecules (FP64 oracle subset)
     cpu = None
     if rank == 0 and not a.no_cpu and a.cpu_sample > 0:
-        cpu = cpu_leg(a, res, parity)
+        cpu = _guarded(cpu_leg, a, res, parity)
 
     # ---- e2e through the public batch API (b200dft.engine.run_batches): every step builds a
     # plan from the host libcint arrays of the batch's molecules (tables staged in pinned host
@@ -570,6 +567,17 @@ def stream_leg(a, net, parity):
     if parity is not None and "plain_its" in parity:
         out["plain_fp64_iterations"] = parity["plain_its"]
     return out
+
+
+def _guarded(fn, *args):
+    """an optional leg of the bench: a failure is recorded in the JSON line instead of ending the
+    run (the timed value and its checks above stand on their own)"""
+    try:
+        return fn(*args)
+    except Exception as e:  # noqa: BLE001
+        import traceback
+        traceback.print_exc(file=sys.stderr)
+        return {"error": f"{type(e).__name__}: {e}"}
 
 
 def spawn_ranks(n):
