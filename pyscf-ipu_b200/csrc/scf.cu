@@ -378,12 +378,13 @@ k_eigh_density(const B2MolDev *__restrict__ mols, const int *__restrict__ active
   __syncthreads();
   if (ws)
     for (int e = threadIdx.x; e < NN; e += blockDim.x) ws[mo + e] = sA[(e / N) * ld + e % N];
-  // ascending order of eigenvalues
+  // ascending order of eigenvalues: a total order (NaN sorts as +inf, ties by index), so the
+  // ranks are a permutation of 0..n-1 whatever the values (every order[] slot is written)
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
-    const double li = evals[i];
+    const double li = evals[i] == evals[i] ? evals[i] : INFINITY;
     int rank = 0;
     for (int j = 0; j < n; ++j) {
-      const double lj = evals[j];
+      const double lj = evals[j] == evals[j] ? evals[j] : INFINITY;
       rank += (lj < li) || (lj == li && j < i);
     }
     order[rank] = i;

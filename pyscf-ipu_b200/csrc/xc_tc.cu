@@ -702,7 +702,8 @@ k_xc_tq(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
       sDh[idx] = d1;
       sDl[idx] = d2;
     }
-    // (the D tiles are read only by the X product, issued after the first tile's barrier)
+    // the orbital table and shell centres are read by every thread from the first tile on
+    __syncthreads();
     double e_part = 0.0;
     bool first = true;
     // point of this thread in the next tile, loaded one tile ahead (the loads' latency overlaps
@@ -739,7 +740,7 @@ k_xc_tq(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
             if (n < N && valid) {
               const float4 o0 = reinterpret_cast<const float4 *>(sOrb)[3 * n];
               const float4 o1 = reinterpret_cast<const float4 *>(sOrb)[3 * n + 1];
-              const int sh = (int)o0.w;
+              const int sh = min(max((int)o0.w, 0), B2_XT_MAXSH - 1);   // table index (clamped)
               if (sh != s_prev) {        // same for every lane of the warp
                 const float4 o2 = reinterpret_cast<const float4 *>(sOrb)[3 * n + 2];
                 if (!(o2.w != 0.f && sh == s_prev + 1 && s_prev >= 0)) {
@@ -811,18 +812,19 @@ k_xc_tq(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
         }
         b2_mma_commit(mbar1);
       }
-      // ---- rho partials over this thread's orbitals: radial factors first (no MMA wait)
+      // ---- rho partials over this thread's orbitals.  Every tensor-memory load is followed
+      //      by its wait with nothing in between: the destination registers are written
+      //      asynchronously and must not be touched (or moved) before tcgen05.wait::ld.
+      if (b2_mbar_wait(mbar1, ph1)) { ph1 ^= 1; x_pending = false; }
+      else { atomicExch(&g_b2_xt_err, 1); sAbort = 1; }
+      b2_fence_after();
       uint32_t ra[4 * Q], rb[4 * Q], xr[4 * Q];
 #pragma unroll
       for (int j4 = 0; j4 < Q; ++j4) {
         b2_tmem_ld4(tl + colGA + nq0 + 4 * j4, ra + 4 * j4);
         b2_tmem_ld4(tl + colGB + nq0 + 4 * j4, rb + 4 * j4);
+        b2_tmem_ld4(tl + colX + nq0 + 4 * j4, xr + 4 * j4);
       }
-      if (b2_mbar_wait(mbar1, ph1)) { ph1 ^= 1; x_pending = false; }
-      else { atomicExch(&g_b2_xt_err, 1); sAbort = 1; }
-      b2_fence_after();
-#pragma unroll
-      for (int j4 = 0; j4 < Q; ++j4) b2_tmem_ld4(tl + colX + nq0 + 4 * j4, xr + 4 * j4);
       b2_tmem_wait_ld();
       float r0 = 0.f, r1 = 0.f, r2 = 0.f, r3 = 0.f;
       {
@@ -834,7 +836,7 @@ k_xc_tq(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
           if (n < N) {
             const float4 o0 = reinterpret_cast<const float4 *>(sOrb)[3 * n];
             const float comp = reinterpret_cast<const float4 *>(sOrb)[3 * n + 1].w;
-            const int sh = (int)o0.w;
+            const int sh = min(max((int)o0.w, 0), B2_XT_MAXSH - 1);
             if (sh != s_prev) {
               s_prev = sh;
               dx = (float)(px - sR[sh][0]);
@@ -898,7 +900,7 @@ k_xc_tq(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
             if (n < N) {
               const float4 o0 = reinterpret_cast<const float4 *>(sOrb)[3 * n];
               const float comp = reinterpret_cast<const float4 *>(sOrb)[3 * n + 1].w;
-              const int sh = (int)o0.w;
+              const int sh = min(max((int)o0.w, 0), B2_XT_MAXSH - 1);
               if (sh != s_prev) {
                 s_prev = sh;
                 dx = (float)(px - sR[sh][0]);
