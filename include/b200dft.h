@@ -67,7 +67,8 @@ int b2_plan_offsets(b2_plan_t plan, int64_t *eri_off, int64_t *mat_off, int *nao
 /* Re-split the J/K work: `elems` s8 entries per CTA (0 = default policy). */
 int b2_plan_set_jk_chunk(b2_plan_t plan, int64_t elems);
 /* Float32 exchange-correlation implementation used by b2_xc_direct(precision 32):
- * 0 = tcgen05 tensor-core kernel with TMEM accumulators (default), 1 = CUDA-core kernel.
+ * 0 = per-bucket persistent tcgen05 kernel with TMEM accumulators (default), 1 = CUDA-core
+ * kernel, 2 = one-launch tcgen05 kernel.
  * No reference counterpart (replaces the XC einsums of nanoDFT.py:105-123). */
 int b2_plan_set_xc_impl(b2_plan_t plan, int impl);
 /* Grid tiles (128 points) per CTA of the tensor-core XC kernel; 0 restores the automatic

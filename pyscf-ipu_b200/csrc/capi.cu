@@ -275,7 +275,7 @@ int b2_plan_set_jk_chunk(void *plan, int64_t elems) {
 }
 
 int b2_plan_set_xc_impl(void *plan, int impl) {
-  if (!plan || impl < 0 || impl > 1) return B2_ERR_ARG;
+  if (!plan || impl < 0 || impl > 2) return B2_ERR_ARG;
   ((B2PlanDev *)plan)->xc_impl = impl;
   return B2_OK;
 }
