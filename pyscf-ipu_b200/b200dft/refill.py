@@ -37,9 +37,13 @@ _PERMOL = (("diis_err", 1), ("exc", 1), ("energy", 5), ("mo_energy", NMO), ("bma
 
 def _spans(off, size, sel):
     """concatenated index ranges [off[m], off[m] + size[m]) for m in sel"""
+    sel = np.asarray(sel, np.int64)
     if len(sel) == 0:
         return np.zeros(0, np.int64)
-    return np.concatenate([np.arange(off[m], off[m] + size[m], dtype=np.int64) for m in sel])
+    o = np.asarray(off, np.int64)[sel]
+    n = np.asarray(size, np.int64)[sel]
+    first = np.cumsum(n) - n                           # position of each range in the result
+    return np.repeat(o - first, n) + np.arange(int(n.sum()), dtype=np.int64)
 
 
 class _Runner:
@@ -59,6 +63,7 @@ class _Runner:
         self.fell_back = torch.zeros(nm, dtype=torch.bool, device=dev)
         self.use_fb = fallback and eng.D0_minao is not None
         self.graph = None
+        self.keep = None                                  # buffers of queued work (released later)
 
 
 def _carry(old, new, sel, nsel):
@@ -92,30 +97,29 @@ def _carry(old, new, sel, nsel):
 
 
 def _fill_eri(eng, new_slots, mols):
-    """s8 and exchange lists of the new molecules: computed on their own plan, copied into place"""
+    """s8 and exchange lists of the new molecules: computed on their own plan, copied into place.
+    Returns what must outlive the queued work (the plan and its buffers): the caller keeps it
+    until a later synchronisation."""
     if not new_slots:
-        return
+        return None
     P = Plan(mols)
-    try:
-        dt = eng.eri.dtype
-        tmp = torch.empty(max(1, P.n_eri), dtype=dt, device=eng.device)
-        tmpx = torch.empty_like(tmp)
-        check(lib().b2_eri_s8(P.h, eng.prec, ptr(tmp), stream_handle()), "b2_eri_s8")
-        if eng.eri_threshold > 0.0:
-            check(lib().b2_eri_threshold(P.h, eng.prec, ptr(tmp), eng.eri_threshold, stream_handle()),
-                  "b2_eri_threshold")
-        check(lib().b2_jk_exchange(P.h, eng.prec, ptr(tmp), ptr(tmpx), stream_handle()), "b2_jk_exchange")
-        es = tmp.element_size()
-        nao = P.nao.astype(np.int64)
-        n4 = (nao * (nao + 1) // 2) * (nao * (nao + 1) // 2 + 1) // 2
-        offs = torch.from_numpy(np.stack([P.eri_off * es, eng.plan.eri_off[new_slots] * es, n4 * es])
-                                .astype(np.int64)).to(eng.device)
-        for src, dst in ((tmp, eng.eri), (tmpx, eng.eri_x)):
-            check(lib().b2_copy_blocks(len(new_slots), ptr(src), ptr(dst), ptr(offs[0]), ptr(offs[1]),
-                                       ptr(offs[2]), stream_handle()), "b2_copy_blocks")
-        torch.cuda.current_stream(eng.device).synchronize()     # tmp buffers and the plan go away
-    finally:
-        P.close()
+    dt = eng.eri.dtype
+    tmp = torch.empty(max(1, P.n_eri), dtype=dt, device=eng.device)
+    tmpx = torch.empty_like(tmp)
+    check(lib().b2_eri_s8(P.h, eng.prec, ptr(tmp), stream_handle()), "b2_eri_s8")
+    if eng.eri_threshold > 0.0:
+        check(lib().b2_eri_threshold(P.h, eng.prec, ptr(tmp), eng.eri_threshold, stream_handle()),
+              "b2_eri_threshold")
+    check(lib().b2_jk_exchange(P.h, eng.prec, ptr(tmp), ptr(tmpx), stream_handle()), "b2_jk_exchange")
+    es = tmp.element_size()
+    nao = P.nao.astype(np.int64)
+    n4 = (nao * (nao + 1) // 2) * (nao * (nao + 1) // 2 + 1) // 2
+    offs = torch.from_numpy(np.stack([P.eri_off * es, eng.plan.eri_off[new_slots] * es, n4 * es])
+                            .astype(np.int64)).to(eng.device)
+    for src, dst in ((tmp, eng.eri), (tmpx, eng.eri_x)):
+        check(lib().b2_copy_blocks(len(new_slots), ptr(src), ptr(dst), ptr(offs[0]), ptr(offs[1]),
+                                   ptr(offs[2]), stream_handle()), "b2_copy_blocks")
+    return P, tmp, tmpx, offs
 
 
 def _start(mols, ids, carried, level, precision, guess, net, fallback, eri_threshold):
@@ -123,15 +127,18 @@ def _start(mols, ids, carried, level, precision, guess, net, fallback, eri_thres
     place and the new molecules initialised"""
     nc = 0 if carried is None else len(carried[1])
     eng = RKSEngine(mols, level=level, precision=precision, guess=guess, net=net, eri_threshold=eri_threshold)
+    # GPU work first (setup, the new molecules' ERIs), then the host work of the learned guess and
+    # of the carry, which overlaps it
     eng.device_setup()
     new_slots = list(range(nc, len(mols)))
-    _fill_eri(eng, new_slots, mols[nc:])
+    keep = _fill_eri(eng, new_slots, mols[nc:])
     eng._eri_done = True
     eng._start_guess()
     if eng._guess_done is not None:
         torch.cuda.current_stream(eng.device).wait_event(eng._guess_done)
         eng._guess_done = None
     r = _Runner(eng, ids, fallback)
+    r.keep = keep
     eng.D.copy_(eng.D0)
     eng.iter.zero_()
     eng.active.fill_(1)
@@ -223,7 +230,7 @@ def _retire(r, mols_by_id, done_mask):
 
 
 def run_refill(molecules, slots=4096, level=0, precision="mixed", guess="learned", net=None,
-               refill_at=0.5, max_its=40, e_tol=1e-6, diis_tol=1e-4, use_diis=True, fallback=True,
+               refill_at=0.3, max_its=40, e_tol=1e-6, diis_tol=1e-4, use_diis=True, fallback=True,
                rise=3.0, fallback_window=5, eri_threshold=0.0):
     """SCF of every molecule of the iterable ``molecules`` with ``slots`` molecules resident on
     the GPU at a time; whenever at most ``refill_at`` of the slots are still iterating, the
@@ -283,5 +290,6 @@ def run_refill(molecules, slots=4096, level=0, precision="mixed", guess="learned
         old = r
         r = _start(mols, ids, (old, survivors), level, precision, guess, net, fallback, eri_threshold)
         old.graph = None
+        old.keep = None          # its ERI plan's work finished long ago (iterations synchronised since)
         old.eng.close()
     r.eng.close()

@@ -569,20 +569,17 @@ int b2_launch_xc_tc(const B2PlanDev &P, const int *active, const double *coords,
 //   * persistent CTAs pull work items (molecule, block of tiles) from a device queue (one
 //     atomic counter per bucket, cleared before the launch) until it is empty; an item of an
 //     inactive molecule is skipped;
-//   * AO gradients are not stored: per orbital the radial factors ga = sum c e^{-a r^2} and
-//     gb = sum -2 a c e^{-a r^2} go to tensor memory (two columns per orbital) and the rho
-//     gradient and Y use them with the shell's displacement d = r - R:
-//       s:   AO = ga,      grad AO = gb d
-//       p_k: AO = d_k ga,  grad AO = ga e_k + d_k gb d
-//     so rho_c = sum_n X_n grad_c AO_n and Y_n = AO_n rt0 + grad AO_n . rt take a few FMAs per
-//     orbital, with one exponential evaluation per shell and tile (consecutive shells with the
-//     same centre and exponents, the 2s/2p pair of STO-3G, share them);
+//   * the radial factors ga = sum c e^{-a r^2} and gb = sum -2 a c e^{-a r^2} are evaluated once per
+//     shell and tile (consecutive shells with the same centre and exponents, the 2s/2p pair of
+//     STO-3G, share the exponentials); AO values go to the N and T tiles, AO gradients to tensor
+//     memory (three columns per orbital) for the rho and Y phases;
+//   * the next tile's grid point is loaded one tile ahead;
 //   * the AO0^T tile holds NB rows: the M = 64 product's rows >= NB read whatever follows
 //     (the next point chunk, or a pad), which only reaches accumulator rows >= NB, never read;
-//   * 4 CTA barriers per tile (was 6): the tensor-memory stores of the radial factors and the
-//     shell exponentials run before the wait on the previous tile's V product.
-// Tensor memory columns: X [0, NB), ga [NB, 2NB), gb [2NB, 3NB), V [3NB, 4NB) (+ [4NB, 5NB)
-// for NB > 64).
+//   * 4 CTA barriers per tile (was 6): the AO evaluation and the tensor-memory stores of the AO
+//     gradients run before the wait on the previous tile's V product.
+// Tensor memory columns: X [0, NB), AO gradients [NB, 4NB), V [4NB, 5NB) (+ [5NB, 6NB) for
+// NB > 64).
 struct __align__(8) B2XtItem { int m, t0; };
 
 // pad after each T tile: the M = 64 product reads (64 - NB) / 8 row groups past a chunk
@@ -592,8 +589,8 @@ __host__ __device__ constexpr int b2_xq_dyn_floats() {   // D, N / Y^T and T til
   return 2 * (16 * Q) * (16 * Q) + 4 * (32 * b2_lt(16 * Q)) / 4 + 2 * b2_xq_pad<Q>();
 }
 template <int Q> __host__ __device__ constexpr uint32_t b2_xq_tmem_cols() {
-  return (16 * Q > 64 ? 5 : 4) * 16 * Q <= 64 ? 64 : (16 * Q > 64 ? 5 : 4) * 16 * Q <= 128 ? 128
-         : (16 * Q > 64 ? 5 : 4) * 16 * Q <= 256 ? 256 : 512;
+  return (16 * Q > 64 ? 6 : 5) * 16 * Q <= 64 ? 64 : (16 * Q > 64 ? 6 : 5) * 16 * Q <= 128 ? 128
+         : (16 * Q > 64 ? 6 : 5) * 16 * Q <= 256 ? 256 : 512;
 }
 
 template <int Q>
@@ -606,7 +603,7 @@ k_xc_tq(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
   constexpr int NB = 16 * Q;
   constexpr int R1 = (32 * b2_lt(NB)) / 4;          // floats of one N / Y^T / T tile
   constexpr uint32_t NCOL = b2_xq_tmem_cols<Q>();
-  constexpr uint32_t colX = 0, colGA = NB, colGB = 2 * NB, colV = 3 * NB, colV2 = 4 * NB;
+  constexpr uint32_t colX = 0, colA = NB, colV = 4 * NB, colV2 = 5 * NB;
   extern __shared__ __align__(128) float smem_f[];
   __shared__ B2XtOrb sOrb[NB];
   __shared__ double sR[B2_XT_MAXSH][3];
@@ -725,18 +722,18 @@ k_xc_tq(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
         if (tt + 1 < tpc && g1 < G) { qx = cm[3 * g1]; qy = cm[3 * g1 + 1]; qz = cm[3 * g1 + 2]; qw = wm[g1]; }
       }
       const float wp = (float)wd;
-      // ---- radial factors per orbital (tensor memory) and AO values (registers)
+      // ---- AO values (registers) and AO gradients (tensor memory) of this thread's orbitals
       float a0[4 * Q];
       {
         int s_prev = -1;
         float ev0 = 0, ev1 = 0, ev2 = 0, dx = 0, dy = 0, dz = 0, ga = 0, gb = 0;
 #pragma unroll
         for (int j4 = 0; j4 < Q; ++j4) {
-          float g4a[4], g4b[4];
+          float a1[4], a2[4], a3[4];
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
             const int n = nq0 + 4 * j4 + u;
-            float av = 0.f, gav = 0.f, gbv = 0.f;
+            float v0 = 0.f, v1 = 0.f, v2 = 0.f, v3 = 0.f;
             if (n < N && valid) {
               const float4 o0 = reinterpret_cast<const float4 *>(sOrb)[3 * n];
               const float4 o1 = reinterpret_cast<const float4 *>(sOrb)[3 * n + 1];
@@ -757,16 +754,28 @@ k_xc_tq(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
                 gb = o2.x * o1.x * ev0 + o2.y * o1.y * ev1 + o2.z * o1.z * ev2;
               }
               const float comp = o1.w;
-              gav = ga;
-              gbv = gb;
-              av = comp < 0.f ? ga : (comp == 0.f ? dx : (comp == 1.f ? dy : dz)) * ga;
+              if (comp < 0.f) {          // s:   AO = ga, grad AO = gb d
+                v0 = ga;
+                v1 = gb * dx;
+                v2 = gb * dy;
+                v3 = gb * dz;
+              } else {                   // p_k: AO = d_k ga, grad AO = ga e_k + d_k gb d
+                const float dk = comp == 0.f ? dx : (comp == 1.f ? dy : dz);
+                const float t = dk * gb;
+                v0 = dk * ga;
+                v1 = (comp == 0.f ? ga : 0.f) + t * dx;
+                v2 = (comp == 1.f ? ga : 0.f) + t * dy;
+                v3 = (comp == 2.f ? ga : 0.f) + t * dz;
+              }
             }
-            a0[4 * j4 + u] = av;
-            g4a[u] = gav;
-            g4b[u] = gbv;
+            a0[4 * j4 + u] = v0;
+            a1[u] = v1;
+            a2[u] = v2;
+            a3[u] = v3;
           }
-          b2_tmem_st4(tl + colGA + nq0 + 4 * j4, g4a[0], g4a[1], g4a[2], g4a[3]);
-          b2_tmem_st4(tl + colGB + nq0 + 4 * j4, g4b[0], g4b[1], g4b[2], g4b[3]);
+          b2_tmem_st4(tl + colA + nq0 + 4 * j4, a1[0], a1[1], a1[2], a1[3]);
+          b2_tmem_st4(tl + colA + NB + nq0 + 4 * j4, a2[0], a2[1], a2[2], a2[3]);
+          b2_tmem_st4(tl + colA + 2 * NB + nq0 + 4 * j4, a3[0], a3[1], a3[2], a3[3]);
         }
       }
       // the previous tile's V product reads the T / Y^T tiles: wait before overwriting them
@@ -812,49 +821,32 @@ k_xc_tq(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
         }
         b2_mma_commit(mbar1);
       }
-      // ---- rho partials over this thread's orbitals.  Every tensor-memory load is followed
-      //      by its wait with nothing in between: the destination registers are written
-      //      asynchronously and must not be touched (or moved) before tcgen05.wait::ld.
+      // ---- rho partials over this thread's orbitals: X and the AO gradients from tensor memory
+      //      (every load waited with nothing in between: the destination registers are written
+      //      asynchronously), AO values from the N tile
       if (b2_mbar_wait(mbar1, ph1)) { ph1 ^= 1; x_pending = false; }
       else { atomicExch(&g_b2_xt_err, 1); sAbort = 1; }
       b2_fence_after();
-      uint32_t ra[4 * Q], rb[4 * Q], xr[4 * Q];
+      float r0 = 0.f, r1 = 0.f, r2 = 0.f, r3 = 0.f;
 #pragma unroll
       for (int j4 = 0; j4 < Q; ++j4) {
-        b2_tmem_ld4(tl + colGA + nq0 + 4 * j4, ra + 4 * j4);
-        b2_tmem_ld4(tl + colGB + nq0 + 4 * j4, rb + 4 * j4);
-        b2_tmem_ld4(tl + colX + nq0 + 4 * j4, xr + 4 * j4);
-      }
-      b2_tmem_wait_ld();
-      float r0 = 0.f, r1 = 0.f, r2 = 0.f, r3 = 0.f;
-      {
-        int s_prev = -1;
-        float dx = 0, dy = 0, dz = 0;
+        const int n0 = nq0 + 4 * j4;
+        uint32_t x[4], b1[4], b2[4], b3[4];
+        b2_tmem_ld4(tl + colX + n0, x);
+        b2_tmem_ld4(tl + colA + n0, b1);
+        b2_tmem_ld4(tl + colA + NB + n0, b2);
+        b2_tmem_ld4(tl + colA + 2 * NB + n0, b3);
+        b2_tmem_wait_ld();
+        const float4 ah = *reinterpret_cast<const float4 *>(sAh + b2_tile_idx(p, n0));
+        const float4 al = *reinterpret_cast<const float4 *>(sAl + b2_tile_idx(p, n0));
+        const float av[4] = {ah.x + al.x, ah.y + al.y, ah.z + al.z, ah.w + al.w};
 #pragma unroll
-        for (int k = 0; k < 4 * Q; ++k) {
-          const int n = nq0 + k;
-          if (n < N) {
-            const float4 o0 = reinterpret_cast<const float4 *>(sOrb)[3 * n];
-            const float comp = reinterpret_cast<const float4 *>(sOrb)[3 * n + 1].w;
-            const int sh = min(max((int)o0.w, 0), B2_XT_MAXSH - 1);
-            if (sh != s_prev) {
-              s_prev = sh;
-              dx = (float)(px - sR[sh][0]);
-              dy = (float)(py - sR[sh][1]);
-              dz = (float)(pz - sR[sh][2]);
-            }
-            const float xv = __uint_as_float(xr[k]), ga = __uint_as_float(ra[k]), gb = __uint_as_float(rb[k]);
-            const float dk = comp < 0.f ? 1.f : (comp == 0.f ? dx : (comp == 1.f ? dy : dz));
-            const float t = xv * dk * gb;
-            r0 += xv * dk * ga;
-            r1 += t * dx;
-            r2 += t * dy;
-            r3 += t * dz;
-            const float xg = comp < 0.f ? 0.f : xv * ga;
-            r1 += comp == 0.f ? xg : 0.f;
-            r2 += comp == 1.f ? xg : 0.f;
-            r3 += comp == 2.f ? xg : 0.f;
-          }
+        for (int u = 0; u < 4; ++u) {
+          const float xv = __uint_as_float(x[u]);
+          r0 += xv * av[u];
+          r1 += xv * __uint_as_float(b1[u]);
+          r2 += xv * __uint_as_float(b2[u]);
+          r3 += xv * __uint_as_float(b3[u]);
         }
       }
       sRed[(qq * 4 + 0) * B2_XT_PT + p] = r0;
@@ -886,39 +878,31 @@ k_xc_tq(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
       if (qq == 0 && valid) e_part += (double)rho[0] * wd * (double)ex;
       const float rt0 = vrho * 0.5f * wp, f4 = 4.f * vg * wp;
       const float rt1 = f4 * rho[1], rt2 = f4 * rho[2], rt3 = f4 * rho[3];
-      // ---- Y_n = AO_n rt0 + grad AO_n . rt -> Y^T tiles (the X product has finished reading
-      //      the N tiles they overwrite)
-      {
-        int s_prev = -1;
-        float dx = 0, dy = 0, dz = 0, dr = 0;
+      // ---- Y_n = AO_n rt0 + grad AO_n . rt -> Y^T tiles (AO values re-read from the T tile: the
+      //      Y^T tiles overwrite the N tile, which the X product has finished reading)
 #pragma unroll
-        for (int j4 = 0; j4 < Q; ++j4) {
+      for (int j4 = 0; j4 < Q; ++j4) {
+        const int n0 = nq0 + 4 * j4;
+        uint32_t b1[4], b2[4], b3[4];
+        b2_tmem_ld4(tl + colA + n0, b1);
+        b2_tmem_ld4(tl + colA + NB + n0, b2);
+        b2_tmem_ld4(tl + colA + 2 * NB + n0, b3);
+        b2_tmem_wait_ld();
+        float av[4];
 #pragma unroll
-          for (int u = 0; u < 4; ++u) {
-            const int k = 4 * j4 + u, n = nq0 + k;
-            float y = 0.f;
-            if (n < N) {
-              const float4 o0 = reinterpret_cast<const float4 *>(sOrb)[3 * n];
-              const float comp = reinterpret_cast<const float4 *>(sOrb)[3 * n + 1].w;
-              const int sh = min(max((int)o0.w, 0), B2_XT_MAXSH - 1);
-              if (sh != s_prev) {
-                s_prev = sh;
-                dx = (float)(px - sR[sh][0]);
-                dy = (float)(py - sR[sh][1]);
-                dz = (float)(pz - sR[sh][2]);
-                dr = dx * rt1 + dy * rt2 + dz * rt3;
-              }
-              const float ga = __uint_as_float(ra[k]), gb = __uint_as_float(rb[k]);
-              const float dk = comp < 0.f ? 1.f : (comp == 0.f ? dx : (comp == 1.f ? dy : dz));
-              const float rk = comp < 0.f ? 0.f : (comp == 0.f ? rt1 : (comp == 1.f ? rt2 : rt3));
-              y = dk * (ga * rt0 + gb * dr) + ga * rk;
-            }
-            float yh, yl;
-            b2_split_rn(y, yh, yl);
-            const int ti = b2_tt_idx(NB, n, p >> 2) + (p & 3);
-            sYh[ti] = yh;
-            sYl[ti] = yl;
-          }
+        for (int u = 0; u < 4; ++u) {
+          const int ti = b2_tt_idx(NB, n0 + u, p >> 2) + (p & 3);
+          av[u] = sTh[ti] + sTl[ti];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const float y = av[u] * rt0 + __uint_as_float(b1[u]) * rt1 + __uint_as_float(b2[u]) * rt2 +
+                          __uint_as_float(b3[u]) * rt3;
+          float yh, yl;
+          b2_split_rn(y, yh, yl);
+          const int ti = b2_tt_idx(NB, n0 + u, p >> 2) + (p & 3);
+          sYh[ti] = yh;
+          sYl[ti] = yl;
         }
       }
       b2_fence_async_smem();
