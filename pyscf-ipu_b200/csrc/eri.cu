@@ -201,17 +201,35 @@ static void b2_eri_group_batch(const B2PlanDev &P, const B2EriTask *tasks, long 
   }
 }
 
+// The 16 class kernels write disjoint entries of the s8 lists, so they run side by side: each on
+// one of the plan's bucket streams (round robin, forked from and joined back to `st` with
+// events), which fills the GPU across the tails of the individual launches.
 template <typename T>
 static void b2_eri_all(const B2PlanDev &P, const B2EriTask *tasks, const std::vector<long long> &g,
                        const B2PairPrim<T> *pp, T *out, cudaStream_t st) {
+  const bool fork = P.bkt_stream[0] != nullptr;
+  if (fork) cudaEventRecord(P.bkt_ev[B2_NBKT], st);
+  int k = 0;
+  auto sk = [&]() -> cudaStream_t {
+    if (!fork) return st;
+    cudaStream_t s = P.bkt_stream[k % B2_NBKT];
+    if (k < B2_NBKT) cudaStreamWaitEvent(s, P.bkt_ev[B2_NBKT], 0);
+    ++k;
+    return s;
+  };
 #define B2_G(grp, LI, LJ, LK, LL)                                                            \
   if (g[grp + 1] > g[grp])                                                                   \
-    b2_eri_group_batch<T, LI, LJ, LK, LL>(P, tasks + g[grp], g[grp + 1] - g[grp], pp, out, st);
+    b2_eri_group_batch<T, LI, LJ, LK, LL>(P, tasks + g[grp], g[grp + 1] - g[grp], pp, out, sk());
   B2_G(0, 0, 0, 0, 0) B2_G(1, 0, 0, 1, 0) B2_G(2, 0, 0, 0, 1) B2_G(3, 0, 0, 1, 1)
   B2_G(4, 1, 0, 0, 0) B2_G(5, 1, 0, 1, 0) B2_G(6, 1, 0, 0, 1) B2_G(7, 1, 0, 1, 1)
   B2_G(8, 0, 1, 0, 0) B2_G(9, 0, 1, 1, 0) B2_G(10, 0, 1, 0, 1) B2_G(11, 0, 1, 1, 1)
   B2_G(12, 1, 1, 0, 0) B2_G(13, 1, 1, 1, 0) B2_G(14, 1, 1, 0, 1) B2_G(15, 1, 1, 1, 1)
 #undef B2_G
+  if (fork)
+    for (int b = 0; b < B2_NBKT && b < k; ++b) {
+      cudaEventRecord(P.bkt_ev[b], P.bkt_stream[b]);
+      cudaStreamWaitEvent(st, P.bkt_ev[b], 0);
+    }
 }
 
 // Work list on the device.  Item it = 4 sp + c (sp: global bra shell pair, c: ket class) owns
