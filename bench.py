@@ -412,11 +412,12 @@ def main():
     res["D"] = eng.D.clone()                 # converged densities of the timed batch (parity)
 
     # ---- roofline figures of the kernel families (dominant first) on the resident batch
-    rooflines = []
-    try:
-        rooflines = kernel_rooflines(eng, a.precision)
-    except Exception as e:  # noqa: BLE001  (recorded in the line, it does not void it)
-        rooflines = [{"error": f"{type(e).__name__}: {e}"}]
+    rooflines = [{"note": "not measured (profile mode: timed steps only)"}]
+    if not a.profile_mode:
+        try:
+            rooflines = kernel_rooflines(eng, a.precision)
+        except Exception as e:  # noqa: BLE001  (recorded in the line, it does not void it)
+            rooflines = [{"error": f"{type(e).__name__}: {e}"}]
     roofline = rooflines[0]
 
     grad = None
