@@ -50,8 +50,16 @@ class Plan:
         env = np.ascontiguousarray(np.concatenate([m._env for m in self.mols]), dtype=np.float64)
         env_off = np.cumsum([0] + [len(m._env) for m in self.mols[:-1]]).astype(np.int64)
         h = ctypes.c_void_p()
-        check(lib().b2_plan_create(nmol, ptr(natm), ptr(nbas), ptr(atm), ptr(bas), ptr(env),
-                                   ptr(env_off), ctypes.byref(h)), "b2_plan_create")
+        args = (nmol, ptr(natm), ptr(nbas), ptr(atm), ptr(bas), ptr(env), ptr(env_off), ctypes.byref(h))
+        rc = lib().b2_plan_create(*args)
+        if rc == -2:
+            # plan tables come from the driver's memory, which torch's caching allocator may be
+            # holding after earlier batches: return torch's unused blocks and try once more
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+            lib().b2_release_cached_memory()
+            rc = lib().b2_plan_create(*args)
+        check(rc, "b2_plan_create")
         self.h = h
         info = np.zeros(8, np.int64)
         check(lib().b2_plan_info(h, ptr(info)), "b2_plan_info")
@@ -70,7 +78,12 @@ class Plan:
 
     def set_grid(self, npoints):
         goff = np.concatenate([[0], np.cumsum(npoints)]).astype(np.int64)
-        check(lib().b2_grid_set(self.h, ptr(goff)), "b2_grid_set")
+        rc = lib().b2_grid_set(self.h, ptr(goff))
+        if rc == -2:                        # as in plan creation: torch's cache holds the memory
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+            rc = lib().b2_grid_set(self.h, ptr(goff))
+        check(rc, "b2_grid_set")
         npts, nao = ctypes.c_int64(), ctypes.c_int64()
         check(lib().b2_grid_info(self.h, ctypes.byref(npts), ctypes.byref(nao)), "b2_grid_info")
         self.grid_off = goff

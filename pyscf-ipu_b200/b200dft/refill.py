@@ -126,6 +126,11 @@ def _start(mols, ids, carried, level, precision, guess, net, fallback, eri_thres
     """engine for ``mols`` (the carried molecules first, then new ones) with the carried state in
     place and the new molecules initialised"""
     nc = 0 if carried is None else len(carried[1])
+    # every refill allocates lists of a new size: hand torch's cached blocks back to the driver
+    # when they hold most of the device (the plan tables allocate outside torch's cache)
+    free, total = torch.cuda.mem_get_info()
+    if free < 0.3 * total:
+        torch.cuda.empty_cache()
     eng = RKSEngine(mols, level=level, precision=precision, guess=guess, net=net, eri_threshold=eri_threshold)
     # GPU work first (setup, the new molecules' ERIs), then the host work of the learned guess and
     # of the carry, which overlaps it
@@ -287,9 +292,10 @@ def run_refill(molecules, slots=4096, level=0, precision="mixed", guess="learned
             break
         mols = [mols_by_id[int(r.ids[s])] for s in survivors] + [m for _, m in fresh]
         ids = [int(r.ids[s]) for s in survivors] + [i for i, _ in fresh]
+        r.keep = None            # its ERI plan's work finished long ago (iterations synchronised since)
         old = r
         r = _start(mols, ids, (old, survivors), level, precision, guess, net, fallback, eri_threshold)
         old.graph = None
-        old.keep = None          # its ERI plan's work finished long ago (iterations synchronised since)
         old.eng.close()
+        del old
     r.eng.close()
