@@ -84,7 +84,7 @@ def kernel_rooflines(eng, precision):
     """Roofline figures of the three kernel families on the resident batch, each timed with
     CUDA events around repeated calls of the entry the SCF uses (after the timed region, same
     batch and data):
-      * XC (k_xc_tc, tensor bound): algorithmic flops 4 G N^2 per molecule (the rho and V_xc
+      * XC (k_xc_tq, tensor bound): algorithmic flops 4 G N^2 per molecule (the rho and V_xc
         contractions, N = nao unpadded) against the measured sustained bf16 dense peak; the
         operands are split tf32 (nominal tf32 rate = half the bf16 rate).
       * J/K (k_symv, HBM bound): algorithmic bytes n4 x 4 B per molecule (the s8 list read once,
@@ -102,7 +102,8 @@ def kernel_rooflines(eng, precision):
     flops = float((4.0 * G * N * N).sum())
     xc_ms = _timed(lambda: eng.xc(active=None), 5)
     tf = flops / (xc_ms / 1e3) / 1e12
-    out.append({"kernel": "k_xc_tc" if precision == "mixed" else "k_xc_direct", "bound": "tensor",
+    out.append({"kernel": "k_xc_tq (per-bucket persistent)" if precision == "mixed" else "k_xc_direct",
+                "bound": "tensor",
                 "achieved": tf, "peak": tpk, "unit": "TFLOP/s", "frac": tf / tpk, "traffic": None,
                 "peak_kind": f"{tkind} bf16 dense (of measured)", "algorithmic_flops_per_launch": flops,
                 "ms_per_launch": xc_ms, "operands": "split tf32, fp32 accumulate"})

@@ -42,6 +42,7 @@ def tiles_array(choice):
 
 def set_bucket_tiles(plan, choice):
     check(lib().b2_plan_set_xc_bucket_tiles(plan.h, ptr(tiles_array(choice))), "b2_plan_set_xc_bucket_tiles")
+    plan.epoch += 1
 
 
 def tune_xc_tiles(eng, candidates=CANDIDATES, reps=3):

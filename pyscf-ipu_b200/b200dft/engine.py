@@ -72,6 +72,7 @@ class Plan:
         check(lib().b2_plan_offsets(h, ptr(self.eri_off), ptr(self.mat_off), ptr(self.nao),
                                     ptr(self.nocc)), "b2_plan_offsets")
         self.grid_off = None
+        self.epoch = 0                      # bumped by every launch-configuration change
         hb = ctypes.c_int64()
         check(lib().b2_plan_h2d_bytes(h, ctypes.byref(hb)), "b2_plan_h2d_bytes")
         self.h2d_bytes = hb.value
@@ -84,6 +85,7 @@ class Plan:
             torch.cuda.empty_cache()
             rc = lib().b2_grid_set(self.h, ptr(goff))
         check(rc, "b2_grid_set")
+        self.epoch += 1
         npts, nao = ctypes.c_int64(), ctypes.c_int64()
         check(lib().b2_grid_info(self.h, ctypes.byref(npts), ctypes.byref(nao)), "b2_grid_info")
         self.grid_off = goff
@@ -93,6 +95,16 @@ class Plan:
 
     def set_jk_chunk(self, elems):
         check(lib().b2_plan_set_jk_chunk(self.h, int(elems)), "b2_plan_set_jk_chunk")
+        self.epoch += 1
+
+    def set_xc_impl(self, impl):
+        """0 per-bucket persistent tensor-core kernel, 1 CUDA cores, 2 one-launch tensor cores"""
+        check(lib().b2_plan_set_xc_impl(self.h, int(impl)), "b2_plan_set_xc_impl")
+        self.epoch += 1
+
+    def set_xc_tiles(self, tiles):
+        check(lib().b2_plan_set_xc_tiles(self.h, int(tiles)), "b2_plan_set_xc_tiles")
+        self.epoch += 1
 
     def close(self):
         if getattr(self, "h", None) is not None and self.h.value:
@@ -260,6 +272,7 @@ class RKSEngine:
         self.graph_replays = 0              # kernels replayed from graphs are not in launch_count()
         self._captured = 0
         self.graph_kernels_per_step = 0
+        self._graph = None                  # (key, CUDAGraph) of one captured SCF iteration
 
     # --- setup -------------------------------------------------------------------------
     def device_setup(self, stream=None):
@@ -412,6 +425,17 @@ class RKSEngine:
         st.hyb, st.use_diis, st.precision = float(hyb), int(use_diis), self.prec
         return st
 
+    def _graph_key(self, use_diis):
+        """what a captured iteration depends on: the buffers its launches read and write (fixed
+        for the engine's life), the plan and its launch configuration"""
+        st = self.scf_state(use_diis)
+        return (self.plan.h.value, self.plan.epoch, self.ao_stored, self.jk_impl,
+                tuple(getattr(st, f) for f, _ in ScfState._fields_))
+
+    def drop_graph(self):
+        """forget the captured iteration (after changing the plan's knobs through the C ABI)"""
+        self._graph = None
+
     def step(self, use_diis=True):
         """One SCF iteration for every active molecule (nanoDFT.py:40-102): one b2_scf_iterate
         call (Fock + DIIS, eigensolve + density, XC, J/K, diff_JK, energies, iteration count)."""
@@ -482,8 +506,12 @@ class RKSEngine:
         hist = torch.full((nm, 5), float("nan"), dtype=torch.float64, device=dev)   # last 5 energies
         g = None
         t = time.perf_counter()
-        if graph:
+        key = self._graph_key(use_diis) if graph else None
+        if graph and self._graph is not None and self._graph[0] == key:
+            g = self._graph[1]                       # same buffers and launch configuration
+        elif graph:
             # capture one iteration (all launches go to the capture stream); replay per step
+            self._graph = None
             st = torch.cuda.Stream()
             st.wait_stream(torch.cuda.current_stream())
             g = torch.cuda.CUDAGraph()
@@ -501,6 +529,7 @@ class RKSEngine:
             torch.cuda.current_stream().wait_stream(st)
             self.graph_kernels_per_step = launch_count() - c0
             self._captured += self.graph_kernels_per_step
+            self._graph = (key, g)
             # the capture did not execute the step: state is unchanged
         tm["capture"] = 1e3 * (time.perf_counter() - t)
         t = time.perf_counter()
@@ -572,6 +601,7 @@ class RKSEngine:
         return launch_count() - since - self._captured + self.graph_replays * self.graph_kernels_per_step
 
     def close(self):
+        self._graph = None
         self.plan.close()
 
 

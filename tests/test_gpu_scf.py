@@ -126,6 +126,25 @@ def test_converged_graph_equals_eager(cuda):
     assert (a["iterations"].cpu().numpy() == b["iterations"].cpu().numpy()).all()
 
 
+def test_captured_iteration_reused_until_the_plan_changes(cuda):
+    # a second run on the same engine replays the first run's graph; a knob change recaptures
+    rng = np.random.default_rng(9)
+    mols = [Mole(random_molecule(rng, k)) for k in (2, 5, 1)]
+    eng = RKSEngine(mols, level=0, precision="mixed", tuned=False)
+    a = eng.run_converged()
+    g1 = eng._graph[1]
+    eng._eri_done = False
+    b = eng.run_converged()
+    assert eng._graph[1] is g1
+    eng.plan.set_xc_impl(1)
+    c = eng.run_converged()
+    assert eng._graph[1] is not g1
+    for r in (b, c):
+        np.testing.assert_allclose(r["energy"].cpu().numpy(), a["energy"].cpu().numpy(), atol=2e-6)
+        assert (r["iterations"].cpu().numpy() == a["iterations"].cpu().numpy()).all()
+    eng.close()
+
+
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_config2_level3_per_precision(cuda, precision):
     """the seeded 9-heavy-atom molecule (nao 62) on the level-3 grid (426 762 points), plain FP64
