@@ -279,10 +279,13 @@ int b2_int2e_sph_s8_noalloc(const int *atm, int natm, const int *bas, int nbas, 
 
 /* C[M,N] = beta*C + A B (+ bias[N]); A element (i,k) at A[i*sai + k*sak], B (k,j) at
  * B[k*sbk + j*sbj].  bf16: 0 float32, 1 operands rounded to bfloat16 (CUDA cores),
- * 2 bfloat16 tensor-core path (float32 accumulation). */
+ * 2 bfloat16 operands on the tcgen05 tensor cores (float32 accumulation in tensor memory). */
 int b2_nn_gemm(int M, int N, int K, const float *A, int64_t sai, int64_t sak, const float *B,
                int64_t sbk, int64_t sbj, float *C, int64_t ldc, const float *bias, float beta,
                int bf16, void *stream);
+/* *status = 1 if a bounded internal wait of the tcgen05 product gave up since the last reset
+ * (that launch left C untouched), else 0; reset != 0 clears it.  Synchronous. */
+int b2_nn_gemm_status(int reset, int *status);
 /* out[N] (+)= column sums of X[M,N] (row stride ld); accumulate != 0 adds to out. */
 int b2_nn_colsum(int M, int N, const float *X, int64_t ld, float *out, int accumulate, void *stream);
 /* y = x * sigmoid(x) and its backward dx = dy * silu'(x). */

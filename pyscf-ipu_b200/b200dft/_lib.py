@@ -33,6 +33,7 @@ SIGNATURES = {
     "b2_plan_set_xc_tiles": [_P, _I],
     "b2_plan_set_xc_bucket_tiles": [_P, _P],
     "b2_xc_tc_status": [_I, _P],
+    "b2_nn_gemm_status": [_I, _P],
     "b2_jk_status": [_I, _P],
     "b2_plan_set_subset": [_P, _P, _I],
     "b2_eri_s8": [_P, _I, _P, _P],

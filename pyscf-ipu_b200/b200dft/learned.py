@@ -154,7 +154,7 @@ class GuessNet:
     def __init__(self, seed=0, device="cuda", bf16=True, tensor_cores=True, hl=HL, hr=HR):
         self.device = torch.device(device)
         self.hl, self.hr = hl, hr
-        # 0: float32 SIMT (exact, for checks); 1: bf16-rounded SIMT; 2: bf16 tensor cores (mma.sync)
+        # 0: float32 SIMT (exact, for checks); 1: bf16-rounded SIMT; 2: bf16 tcgen05 tensor cores
         self.bf16 = (2 if tensor_cores else 1) if bf16 else 0
         self.shapes = layout(hl, hr)
         self.offsets = {}

@@ -71,90 +71,207 @@ k_nn_gemm(int M, int N, int K, const float *__restrict__ A, long long sai, long 
     }
 }
 
-// Tensor-core form of the same product: bf16 inputs, fp32 accumulation, mma.sync m16n8k16.
-// CTA tile 128x128, 8 warps (2 x 4), each warp 64 x 32 (4 x 4 fragments); K step 32.
-// Fragment layout (PTX ISA, mma.m16n8k16 .bf16): g = lane/4, t = lane%4;
-//   A regs: (g, 2t..2t+1), (g+8, 2t..), (g, 2t+8..), (g+8, 2t+8..)     B regs: (k=2t.., n=g), (k=2t+8.., n=g)
-//   C: (g, 2t..2t+1), (g+8, 2t..2t+1)
-#define TC_BM 128
-#define TC_BN 128
-#define TC_BK 32
-#define TC_LD (TC_BK + 8)
+// Tensor-core form of the same product (the one the network uses): bf16 inputs rounded to nearest even, fp32
+// accumulation in tensor memory.  CTA tile 128 x 128, K step 64, two shared-memory stages: all
+// 256 threads convert the next stage's float32 operands to bf16 while the tensor core works on
+// the current one (one thread issues tcgen05.mma.kind::f16, M = 128, N = 128, K = 16, and commits
+// to the stage's mbarrier).  Operands are K-major without swizzle: 8-row x 16-byte core matrices,
+// element (row r, k) of a stage tile at byte ((k / 8) * 16 + r / 8) * 128 + (r % 8) * 16 + (k % 8) * 2
+// (LBO 2048 B between k chunks, SBO 128 B between row groups).  Epilogue: warp w reads tensor
+// memory lanes 32 (w % 4) .. + 31 (its rows) and columns 64 (w / 4) .. + 63, adds the bias and
+// beta C.  Every mbarrier wait is bounded; a wait that gives up sets an error code (read with
+// b2_nn_gemm_status), the CTA waits (bounded) for its issued products, frees its tensor memory
+// and returns without storing.
+#define T5_BM 128
+#define T5_BN 128
+#define T5_BK 64
+#define T5_STAGE_BYTES ((T5_BM + T5_BN) * T5_BK * 2)
+#define T5_SPIN (1 << 22)
+
+__device__ int g_b2_nn_err = 0;
+
+__device__ __forceinline__ uint32_t b2_nn_su32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ bool b2_nn_mbar_wait(uint32_t a, uint32_t parity) {
+  for (int it = 0; it < T5_SPIN; ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok) : "r"(a), "r"(parity) : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+__device__ __forceinline__ uint64_t b2_nn_sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+__device__ __forceinline__ uint32_t b2_nn_pack_bf16(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);     // .x = lo (low half), .y = hi
+  return *reinterpret_cast<const uint32_t *>(&v);
+}
+// one operand tile (128 rows x 64 k) of a stage.  Thread unit = 8 consecutive k of one row
+// (one 16-byte core-matrix row); lane = 8 a + b takes row 8 R + b and k chunk 4 KC + a, so a
+// warp covers 8 rows x 4 chunks: with k contiguous in memory every row is read as 128
+// contiguous bytes, with rows contiguous every k as 32 contiguous bytes, and each group of 8
+// lanes stores 8 different 16-byte bank groups (no shared-memory conflicts).
+__device__ __forceinline__ void b2_nn_fill(unsigned char *dst, int rows_valid, int k0, int K,
+                                           const float *__restrict__ X, long long s_row, long long s_k,
+                                           bool vec, int tid) {
+#pragma unroll
+  for (int u = 0; u < (128 * 8) / 256; ++u) {
+    const int e = tid + 256 * u;
+    const int r = 8 * ((e >> 5) & 15) + (e & 7), kc = 4 * (e >> 9) + ((e >> 3) & 3);
+    const int gk0 = k0 + 8 * kc;
+    float v[8];
+    if (vec && r < rows_valid && gk0 + 8 <= K) {      // k contiguous and 16-byte aligned
+      const float4 *src = reinterpret_cast<const float4 *>(X + (long long)r * s_row + gk0);
+      const float4 x0 = src[0], x1 = src[1];
+      v[0] = x0.x; v[1] = x0.y; v[2] = x0.z; v[3] = x0.w;
+      v[4] = x1.x; v[5] = x1.y; v[6] = x1.z; v[7] = x1.w;
+    } else {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int gk = gk0 + q;
+        v[q] = (r < rows_valid && gk < K) ? X[(long long)r * s_row + (long long)gk * s_k] : 0.f;
+      }
+    }
+    uint4 w;
+    w.x = b2_nn_pack_bf16(v[0], v[1]);
+    w.y = b2_nn_pack_bf16(v[2], v[3]);
+    w.z = b2_nn_pack_bf16(v[4], v[5]);
+    w.w = b2_nn_pack_bf16(v[6], v[7]);
+    *reinterpret_cast<uint4 *>(dst + ((kc * 16 + (r >> 3)) * 128 + (r & 7) * 16)) = w;
+  }
+}
 
 __global__ void __launch_bounds__(256)
 k_nn_gemm_tc(int M, int N, int K, const float *__restrict__ A, long long sai, long long sak,
              const float *__restrict__ B, long long sbk, long long sbj, float *__restrict__ C,
              long long ldc, const float *__restrict__ bias, float beta) {
-  __shared__ __align__(16) __nv_bfloat16 As[TC_BM][TC_LD];   // [m][k]
-  __shared__ __align__(16) __nv_bfloat16 Bs[TC_BN][TC_LD];   // [n][k]
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int wm = warp >> 2, wn = warp & 3;                     // 2 x 4 warps
-  const int g = lane >> 2, t = lane & 3;
-  const int i0 = blockIdx.y * TC_BM, j0 = blockIdx.x * TC_BN;
-  float acc[4][4][4];
+  extern __shared__ __align__(128) unsigned char t5_smem[];
+  __shared__ __align__(8) unsigned long long sBar[2];
+  __shared__ uint32_t sTmem;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int i0 = blockIdx.y * T5_BM, j0 = blockIdx.x * T5_BN;
+  if (tid == 0) {
 #pragma unroll
-  for (int a = 0; a < 4; ++a)
-#pragma unroll
-    for (int b = 0; b < 4; ++b)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) acc[a][b][c] = 0.f;
-  for (int k0 = 0; k0 < K; k0 += TC_BK) {
-    for (int e = threadIdx.x; e < TC_BM * TC_BK; e += 256) {
-      const int ii = e / TC_BK, kk = e % TC_BK;
-      const int gi = i0 + ii, gk = k0 + kk;
-      As[ii][kk] = __float2bfloat16_rn((gi < M && gk < K) ? A[gi * sai + gk * sak] : 0.f);
+    for (int s = 0; s < 2; ++s) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(b2_nn_su32(&sBar[s])) : "memory");
     }
-    for (int e = threadIdx.x; e < TC_BN * TC_BK; e += 256) {
-      const int jj = e % TC_BN, kk = e / TC_BN;
-      const int gj = j0 + jj, gk = k0 + kk;
-      Bs[jj][kk] = __float2bfloat16_rn((gj < N && gk < K) ? B[gk * sbk + gj * sbj] : 0.f);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int ks = 0; ks < TC_BK; ks += 16) {
-      unsigned af[4][4], bfr[4][2];
-#pragma unroll
-      for (int mt = 0; mt < 4; ++mt) {
-        const int r = wm * 64 + mt * 16 + g;
-        af[mt][0] = *reinterpret_cast<const unsigned *>(&As[r][ks + 2 * t]);
-        af[mt][1] = *reinterpret_cast<const unsigned *>(&As[r + 8][ks + 2 * t]);
-        af[mt][2] = *reinterpret_cast<const unsigned *>(&As[r][ks + 2 * t + 8]);
-        af[mt][3] = *reinterpret_cast<const unsigned *>(&As[r + 8][ks + 2 * t + 8]);
-      }
-#pragma unroll
-      for (int nt = 0; nt < 4; ++nt) {
-        const int cidx = wn * 32 + nt * 8 + g;
-        bfr[nt][0] = *reinterpret_cast<const unsigned *>(&Bs[cidx][ks + 2 * t]);
-        bfr[nt][1] = *reinterpret_cast<const unsigned *>(&Bs[cidx][ks + 2 * t + 8]);
-      }
-#pragma unroll
-      for (int mt = 0; mt < 4; ++mt)
-#pragma unroll
-        for (int nt = 0; nt < 4; ++nt)
-          asm volatile(
-              "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-              "{%0,%1,%2,%3};\n"
-              : "+f"(acc[mt][nt][0]), "+f"(acc[mt][nt][1]), "+f"(acc[mt][nt][2]), "+f"(acc[mt][nt][3])
-              : "r"(af[mt][0]), "r"(af[mt][1]), "r"(af[mt][2]), "r"(af[mt][3]), "r"(bfr[nt][0]), "r"(bfr[nt][1]));
-    }
-    __syncthreads();
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 128;"
+                 :: "r"(b2_nn_su32(&sTmem)) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tacc = sTmem;
+  // instruction descriptor: f32 accumulator, bf16 A and B, both K-major, N = 128, M = 128
+  const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(T5_BN >> 3) << 17) |
+                         ((uint32_t)(T5_BM >> 4) << 24);
+  const int mv = min(T5_BM, M - i0), nv = min(T5_BN, N - j0);
+  const float *Ab = A + (long long)i0 * sai;
+  const float *Bb = B + (long long)j0 * sbj;
+  const int nk = (K + T5_BK - 1) / T5_BK;
+  // 16-byte vector loads where k is contiguous and every row starts 16-byte aligned
+  const bool vecA = sak == 1 && (sai & 3) == 0 && ((uintptr_t)Ab & 15) == 0;
+  const bool vecB = sbk == 1 && (sbj & 3) == 0 && ((uintptr_t)Bb & 15) == 0;
+  uint32_t ph = 0u, pend = 0u;          // per stage (bit s): mbarrier phase, product not yet seen complete
+  bool fail = false;
+  for (int kt = 0; kt < nk; ++kt) {
+    const int s = kt & 1;
+    unsigned char *sa = t5_smem + s * T5_STAGE_BYTES, *sb = sa + T5_BM * T5_BK * 2;
+    if ((pend >> s) & 1u) {            // the product issued two steps ago read this stage
+      if (b2_nn_mbar_wait(b2_nn_su32(&sBar[s]), (ph >> s) & 1u)) { ph ^= 1u << s; pend &= ~(1u << s); }
+      else fail = true;
+    }
+    if (__syncthreads_or(fail)) break;
+    b2_nn_fill(sa, mv, kt * T5_BK, K, Ab, sai, sak, vecA, tid);
+    b2_nn_fill(sb, nv, kt * T5_BK, K, Bb, sbj, sbk, vecB, tid);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t a0 = b2_nn_su32(sa), b0 = b2_nn_su32(sb);
 #pragma unroll
-  for (int mt = 0; mt < 4; ++mt)
+      for (int kk = 0; kk < T5_BK / 16; ++kk) {
+        const uint64_t ad = b2_nn_sdesc(a0 + kk * 2 * 2048, 2048, 128);
+        const uint64_t bd = b2_nn_sdesc(b0 + kk * 2 * 2048, 2048, 128);
+        const uint32_t acc = (kt > 0 || kk > 0) ? 1u : 0u;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+            :: "r"(tacc), "l"(ad), "l"(bd), "r"(idesc), "r"(acc) : "memory");
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                   :: "r"(b2_nn_su32(&sBar[s])) : "memory");
+    }
+    pend |= 1u << s;
+  }
+  // wait for every issued product (the last one completes after all earlier ones)
 #pragma unroll
-    for (int nt = 0; nt < 4; ++nt)
+  for (int s = 0; s < 2; ++s)
+    if ((pend >> s) & 1u) {
+      if (b2_nn_mbar_wait(b2_nn_su32(&sBar[s]), (ph >> s) & 1u)) { ph ^= 1u << s; pend &= ~(1u << s); }
+      else fail = true;
+    }
+  if (fail && lane == 0) atomicExch(&g_b2_nn_err, 1);
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  const bool any_fail = __syncthreads_or(fail);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (!any_fail && nk > 0) {
+    // tensor memory -> shared memory (row stride 65 floats: conflict-free both ways) -> C, one
+    // 64-column half at a time, stored row by row (coalesced)
+    float *stile = reinterpret_cast<float *>(t5_smem);
+    const int r = 32 * (warp & 3) + lane;
+#pragma unroll 1
+    for (int h = 0; h < 2; ++h) {
+      if ((warp >> 2) == h) {
+#pragma unroll 1
+        for (int cc = 0; cc < 64; cc += 16) {
+          uint32_t v[16];
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+              : "r"(tacc + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)(64 * h + cc)));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-      for (int h = 0; h < 2; ++h)
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-          const int gi = i0 + wm * 64 + mt * 16 + g + 8 * h;
-          const int gj = j0 + wn * 32 + nt * 8 + 2 * t + q;
-          if (gi < M && gj < N) {
-            const float v = acc[mt][nt][2 * h + q] + (bias ? bias[gj] : 0.f);
-            float *dst = C + gi * ldc + gj;
-            *dst = beta != 0.f ? beta * *dst + v : v;
-          }
+          for (int q = 0; q < 16; ++q) stile[r * 65 + cc + q] = __uint_as_float(v[q]);
         }
+      }
+      __syncthreads();
+      for (int e = tid; e < T5_BM * 64; e += 256) {
+        const int rr = e >> 6, c = e & 63;
+        const int gi = i0 + rr, gj = j0 + 64 * h + c;
+        if (gi < M && gj < N) {
+          const float x = stile[rr * 65 + c] + (bias ? bias[gj] : 0.f);
+          float *dst = C + (long long)gi * ldc + gj;
+          *dst = beta != 0.f ? beta * *dst + x : x;
+        }
+      }
+      __syncthreads();
+    }
+  } else if (!any_fail && nk == 0) {                  // K = 0: C = beta C + bias
+    for (int e = tid; e < T5_BM * T5_BN; e += 256) {
+      const int gi = i0 + e / T5_BN, gj = j0 + e % T5_BN;
+      if (gi < M && gj < N) {
+        float *dst = C + (long long)gi * ldc + gj;
+        const float x = bias ? bias[gj] : 0.f;
+        *dst = beta != 0.f ? beta * *dst + x : x;
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 128;" :: "r"(tacc) : "memory");
 }
 
 // column sums (bias gradients): out[j] (+)= sum_i X[i*ld + j]
@@ -404,10 +521,20 @@ int b2_nn_gemm(int M, int N, int K, const float *A, int64_t sai, int64_t sak, co
                int64_t sbj, float *C, int64_t ldc, const float *bias, float beta, int bf16, void *stream) {
   if (M < 0 || N < 0 || K < 0 || !A || !B || !C) return B2_ERR_ARG;
   if (M == 0 || N == 0) return B2_OK;
-  if (bf16 == 2) {                       // tensor cores (bf16 inputs, fp32 accumulation)
-    dim3 grid((N + TC_BN - 1) / TC_BN, (M + TC_BM - 1) / TC_BM);
+  if (bf16 == 2) {                       // tcgen05 tensor cores (bf16 inputs, fp32 accumulation)
+    dim3 grid((N + T5_BN - 1) / T5_BN, (M + T5_BM - 1) / T5_BM);
     if (grid.y > 65535) return B2_ERR_SIZE;
-    k_nn_gemm_tc<<<grid, 256, 0, (cudaStream_t)stream>>>(M, N, K, A, sai, sak, B, sbk, sbj, C, ldc, bias, beta);
+    static bool attr[8] = {false};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 8) return B2_ERR_CUDA;
+    if (!attr[dev]) {
+      if (cudaFuncSetAttribute(k_nn_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * T5_STAGE_BYTES) !=
+          cudaSuccess)
+        return B2_ERR_CUDA;
+      attr[dev] = true;
+    }
+    k_nn_gemm_tc<<<grid, 256, 2 * T5_STAGE_BYTES, (cudaStream_t)stream>>>(M, N, K, A, sai, sak, B, sbk, sbj, C,
+                                                                          ldc, bias, beta);
     b2_count_launches(1);
     return cudaGetLastError() == cudaSuccess ? B2_OK : B2_ERR_CUDA;
   }
@@ -416,6 +543,16 @@ int b2_nn_gemm(int M, int N, int K, const float *A, int64_t sai, int64_t sak, co
   k_nn_gemm<<<grid, 256, 0, (cudaStream_t)stream>>>(M, N, K, A, sai, sak, B, sbk, sbj, C, ldc, bias, beta, bf16);
   b2_count_launches(1);
   return cudaGetLastError() == cudaSuccess ? B2_OK : B2_ERR_CUDA;
+}
+
+int b2_nn_gemm_status(int reset, int *status) {
+  if (!status) return B2_ERR_ARG;
+  if (cudaMemcpyFromSymbol(status, g_b2_nn_err, sizeof(int)) != cudaSuccess) return B2_ERR_CUDA;
+  if (reset) {
+    const int z = 0;
+    if (cudaMemcpyToSymbol(g_b2_nn_err, &z, sizeof(int)) != cudaSuccess) return B2_ERR_CUDA;
+  }
+  return B2_OK;
 }
 
 int b2_nn_colsum(int M, int N, const float *X, int64_t ld, float *out, int accumulate, void *stream) {

@@ -130,6 +130,10 @@ __device__ __forceinline__ int b2_tt_idx(int R, int r, int pc) {
   return (pc * b2_lt(R) + (r >> 3) * 128 + (r & 7) * 16) >> 2;
 }
 
+// named barrier of the 4 warps sharing TMEM lane quarter q (ids 1..4; 0 is __syncthreads)
+__device__ __forceinline__ void b2_bar_quarter(int q) {
+  asm volatile("bar.sync %0, 128;" :: "r"(q + 1) : "memory");
+}
 // 4-register TMEM load (this thread's lane, 4 consecutive columns)
 __device__ __forceinline__ void b2_tmem_ld4(uint32_t ta, uint32_t *r) {
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];"
@@ -778,10 +782,13 @@ k_xc_tq(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
           b2_tmem_st4(tl + colA + 2 * NB + nq0 + 4 * j4, a3[0], a3[1], a3[2], a3[3]);
         }
       }
-      // the previous tile's V product reads the T / Y^T tiles: wait before overwriting them
+      // the previous tile's V product reads the T / Y^T tiles: wait before overwriting them.
+      // A wait that gives up is combined over the CTA at the next CTA barrier, so every thread
+      // leaves at the same point.
+      bool fail = false;
       if (g2_pending) {
         if (b2_mbar_wait(mbar2, ph2)) { ph2 ^= 1; g2_pending = false; }
-        else { atomicExch(&g_b2_xt_err, 2); sAbort = 1; }
+        else { atomicExch(&g_b2_xt_err, 2); fail = true; }
       }
 #pragma unroll
       for (int j4 = 0; j4 < Q; ++j4) {
@@ -801,8 +808,7 @@ k_xc_tq(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
       b2_tmem_wait_st();
       b2_fence_async_smem();
       b2_fence_before();
-      __syncthreads();                                              // [1]
-      if (sAbort) break;
+      if (__syncthreads_or(fail)) { sAbort = 1; break; }            // [1]
       x_pending = true;
       // ---- X = AO0 D = (A_h + A_l)(D_1 + D_2): three TF32 products per K step
       if (tid == 0) {
@@ -823,9 +829,9 @@ k_xc_tq(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
       }
       // ---- rho partials over this thread's orbitals: X and the AO gradients from tensor memory
       //      (every load waited with nothing in between: the destination registers are written
-      //      asynchronously), AO values from the N tile
+      //      asynchronously), AO values from registers
       if (b2_mbar_wait(mbar1, ph1)) { ph1 ^= 1; x_pending = false; }
-      else { atomicExch(&g_b2_xt_err, 1); sAbort = 1; }
+      else { atomicExch(&g_b2_xt_err, 1); fail = true; }
       b2_fence_after();
       float r0 = 0.f, r1 = 0.f, r2 = 0.f, r3 = 0.f;
 #pragma unroll
@@ -837,13 +843,10 @@ k_xc_tq(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
         b2_tmem_ld4(tl + colA + NB + n0, b2);
         b2_tmem_ld4(tl + colA + 2 * NB + n0, b3);
         b2_tmem_wait_ld();
-        const float4 ah = *reinterpret_cast<const float4 *>(sAh + b2_tile_idx(p, n0));
-        const float4 al = *reinterpret_cast<const float4 *>(sAl + b2_tile_idx(p, n0));
-        const float av[4] = {ah.x + al.x, ah.y + al.y, ah.z + al.z, ah.w + al.w};
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const float xv = __uint_as_float(x[u]);
-          r0 += xv * av[u];
+          r0 += xv * a0[4 * j4 + u];
           r1 += xv * __uint_as_float(b1[u]);
           r2 += xv * __uint_as_float(b2[u]);
           r3 += xv * __uint_as_float(b3[u]);
@@ -853,15 +856,17 @@ k_xc_tq(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
       sRed[(qq * 4 + 1) * B2_XT_PT + p] = r1;
       sRed[(qq * 4 + 2) * B2_XT_PT + p] = r2;
       sRed[(qq * 4 + 3) * B2_XT_PT + p] = r3;
-      b2_fence_before();
-      __syncthreads();                                              // [2]
-      if (sAbort) break;
+      // from here to the V product a point's four threads (warps q4, q4+4, q4+8, q4+12) exchange
+      // data only among themselves through sRed / sFn entries of their own points: a barrier per
+      // lane quarter (128 threads) instead of the whole CTA.  The N tile is no longer read (the AO
+      // values come from registers), so a quarter may start writing Y^T over it.
+      b2_bar_quarter(q4);                                           // [2]
       float rho[4];
 #pragma unroll
       for (int c = 0; c < 4; ++c)
         rho[c] = ((sRed[c * B2_XT_PT + p] + sRed[(4 + c) * B2_XT_PT + p]) + sRed[(8 + c) * B2_XT_PT + p]) +
                  sRed[(12 + c) * B2_XT_PT + p];
-      if (kAlias) __syncthreads();                                  // sFn overwrites sRed
+      if (kAlias) b2_bar_quarter(q4);                               // sFn overwrites sRed
       // ---- B3LYP in three parts: Slater + B88 (qq 0), VWN (qq 1), LYP (qq 2)
       if (qq < 3) {
         const B2XcPoint<float> o = qq == 0 ? b2_b3lyp_x<float>(rho[0], rho[1], rho[2], rho[3])
@@ -871,7 +876,7 @@ k_xc_tq(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
         sFn[(qq * 3 + 1) * B2_XT_PT + p] = o.vrho;
         sFn[(qq * 3 + 2) * B2_XT_PT + p] = o.vgamma;
       }
-      __syncthreads();                                              // [3]
+      b2_bar_quarter(q4);                                           // [3]
       const float ex = sFn[0 * B2_XT_PT + p] + (sFn[3 * B2_XT_PT + p] + sFn[6 * B2_XT_PT + p]);
       const float vrho = sFn[1 * B2_XT_PT + p] + (sFn[4 * B2_XT_PT + p] + sFn[7 * B2_XT_PT + p]);
       const float vg = sFn[2 * B2_XT_PT + p] + (sFn[5 * B2_XT_PT + p] + sFn[8 * B2_XT_PT + p]);
@@ -907,7 +912,7 @@ k_xc_tq(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
       }
       b2_fence_async_smem();
       b2_fence_before();
-      __syncthreads();                                              // [4]
+      if (__syncthreads_or(fail)) { sAbort = 1; break; }            // [4]
       // ---- V += AO0^T Y (M = 64 orbital rows; a second product covers rows 64..NB-1)
       if (tid == 0) {
         b2_fence_after();

@@ -92,27 +92,40 @@ def test_trained_guess_gains_over_minao(cuda):
     assert np.abs(e1 - e0).max() <= 1e-4             # the plain SCF judges: same converged energies
 
 
-@pytest.mark.parametrize("shape", [(1000, 512, 288), (37, 10, 512), (300, 128, 32), (513, 257, 129)])
+@pytest.mark.parametrize("shape", [(1000, 512, 288), (37, 10, 512), (300, 128, 32), (513, 257, 129),
+                                   (128, 128, 64), (129, 130, 65)])
 def test_tensor_core_gemm_matches_bf16_simt(cuda, shape):
-    """mma.sync bf16 product == bf16-rounded SIMT product (same inputs, fp32 accumulation)"""
+    """tcgen05 bf16 product (mode 2) == bf16-rounded SIMT product (same inputs, fp32
+    accumulation), with bias, transposed operands and beta accumulation"""
     from b200dft.learned import _lib
     from b200dft._lib import ptr, stream_handle
+    import ctypes
     M, N, K = shape
     g = torch.Generator(device="cuda").manual_seed(0)
     A = torch.randn(M, K, device="cuda", generator=g)
     B = torch.randn(K, N, device="cuda", generator=g)
     bias = torch.randn(N, device="cuda", generator=g)
-    out = {}
+    C0 = torch.randn(M, N, device="cuda", generator=g)
+    st = ctypes.c_int(-1)
+    assert _lib().b2_nn_gemm_status(1, ctypes.byref(st)) == 0
+    out, acc = {}, {}
     for mode in (1, 2):
         C = torch.zeros(M, N, device="cuda")
         assert _lib().b2_nn_gemm(M, N, K, ptr(A), K, 1, ptr(B), N, 1, ptr(C), N, ptr(bias), 0.0, mode,
                                  stream_handle()) == 0
         out[mode] = C
-    # transposed operand through the strides
+        Cb = C0.clone()
+        assert _lib().b2_nn_gemm(M, N, K, ptr(A), K, 1, ptr(B), N, 1, ptr(Cb), N, None, 0.5, mode,
+                                 stream_handle()) == 0
+        acc[mode] = Cb
+    # transposed operands through the strides
     Ct = torch.zeros(N, M, device="cuda")
     assert _lib().b2_nn_gemm(N, M, K, ptr(B), 1, N, ptr(A), 1, K, ptr(Ct), M, None, 0.0, 2, stream_handle()) == 0
     torch.cuda.synchronize()
+    assert _lib().b2_nn_gemm_status(1, ctypes.byref(st)) == 0 and st.value == 0
     ref = out[1]
     scale = ref.abs().max().item()
-    assert (out[2] - ref).abs().max().item() <= 1e-4 * scale
+    for mode in (2,):
+        assert (out[mode] - ref).abs().max().item() <= 1e-4 * scale
+        assert (acc[mode] - acc[1]).abs().max().item() <= 1e-4 * scale
     assert (Ct.T - (ref - bias)).abs().max().item() <= 1e-4 * scale
