@@ -28,11 +28,11 @@ B2_HD constexpr int b2g_cstart(int l) { return l * (l + 1) * (l + 2) / 6; }
 B2_HD constexpr int b2g_ncart(int l) { return (l + 1) * (l + 2) * (l + 3) / 6; }   // components of 0..l
 // index of the Cartesian (x, y, z) among all components of l = 0..3 (order within a shell:
 // x descending, then y descending)
-B2_HD int b2g_cidx(int x, int y, int z) {
+B2_HD constexpr int b2g_cidx(int x, int y, int z) {
   const int l = x + y + z;
   return b2g_cstart(l) + (l - x) * (l - x + 1) / 2 + z;
 }
-B2_HD void b2g_cart(int idx, int &x, int &y, int &z) {
+B2_HD constexpr void b2g_cart(int idx, int &x, int &y, int &z) {
   int l = 0;
   while (b2g_cstart(l + 1) <= idx) ++l;
   int r = idx - b2g_cstart(l);
