@@ -322,8 +322,9 @@ def main():
     ap.add_argument("--profile-mode", action="store_true", help="timed steps only (for ncu captures)")
     ap.add_argument("--stream", type=int, default=204800,
                     help="streaming leg: molecules through the public stream API with slot refill (0: off)")
-    ap.add_argument("--grad", type=int, default=512,
-                    help="also time the nuclear gradient (b2_grad) of the first N converged molecules (0: off)")
+    ap.add_argument("--grad", type=int, default=None,
+                    help="also time the nuclear gradient (b2_grad) of the first N converged molecules "
+                         "(0: off; default 512, or off with --profile-mode)")
     a = ap.parse_args()
     if a.impl == "reference":
         return run_reference(a)
@@ -425,7 +426,9 @@ def main():
     roofline = rooflines[0]
 
     grad = None
-    if a.grad > 0 and rank == 0 and not a.profile_mode:
+    if a.grad is None:
+        a.grad = 0 if a.profile_mode else 512
+    if a.grad > 0 and rank == 0:
         grad = _guarded(gradient_timing, mols[:a.grad], a, net)
 
     if a.profile_mode:
