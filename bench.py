@@ -438,39 +438,13 @@ def main():
     parity = None
     if rank == 0 and not a.profile_mode:
         parity = _guarded(batch_parity, eng, mols, a, res)
-    learned = None
-    if rank == 0 and not a.profile_mode and a.guess == "learned":
-        learned = _guarded(learned_guess_criterion, mols, a, net)
-    cfg2 = None
-    if rank == 0 and not a.profile_mode:
-        cfg2 = _guarded(config2_report)
-
-    # ---- streaming generation (config 5): molecules generated on host workers, batched SCF with
-    # slot refill and the learned guess, results to host memory, through b200dft.stream
-    stream = None
-    torch.cuda.empty_cache()
-    if rank == 0 and not a.profile_mode and a.stream > 0:
-        stream = _guarded(stream_leg, a, net, parity)
-
-    # ---- plain FP64 per-molecule GPU path on a sample (same convergence rule, minao guess):
-    # wall clock per molecule (plan, engine, eager SCF, close) and its device time
-    plain = None
-    if rank == 0 and a.plain_sample > 0:
-        plain = _guarded(plain_leg, mols, a, res)
-
-    # ---- CPU baseline: the reference's compiled int2e_sph + the FP64 port of its SCF on a
-    # bounded sample of the batch, on a pool of the host's cores; its energies also check the
-    # GPU results of the same molecules (FP64 oracle subset)
-    cpu = None
-    if rank == 0 and not a.no_cpu and a.cpu_sample > 0:
-        cpu = _guarded(cpu_leg, a, res, parity)
-
     # ---- e2e through the public batch API (b200dft.engine.run_batches): every step builds a
     # plan from the host libcint arrays of the batch's molecules (tables staged in pinned host
     # memory and copied to the device), runs the batch to convergence and copies its results to
     # host memory; the next step's plan is built on a worker thread while the GPU runs the
     # current batch.  The steps reuse the same 4096 host Mole objects (their libcint arrays are
-    # built once, before timing).  The device-timed engine is released first.
+    # built once, before timing).  The device-timed engine is released first.  This leg runs
+    # before the host-heavy ones (stream workers, the CPU pool), on a quiet host.
     eng.close()
     del eng
     e2e = None
@@ -510,6 +484,33 @@ def main():
         # per-step detail goes to stderr, keeping the JSON line short
         print(json.dumps({"e2e_step_ms": steps_ms, "e2e_step_host_ms": host, "gc_gen2_pauses_ms": gc_pauses}),
               file=sys.stderr)
+
+    learned = None
+    if rank == 0 and not a.profile_mode and a.guess == "learned":
+        learned = _guarded(learned_guess_criterion, mols, a, net)
+    cfg2 = None
+    if rank == 0 and not a.profile_mode:
+        cfg2 = _guarded(config2_report)
+
+    # ---- streaming generation (config 5): molecules generated on host workers, batched SCF with
+    # slot refill and the learned guess, results to host memory, through b200dft.stream
+    stream = None
+    torch.cuda.empty_cache()
+    if rank == 0 and not a.profile_mode and a.stream > 0:
+        stream = _guarded(stream_leg, a, net, parity)
+
+    # ---- plain FP64 per-molecule GPU path on a sample (same convergence rule, minao guess):
+    # wall clock per molecule (plan, engine, eager SCF, close) and its device time
+    plain = None
+    if rank == 0 and a.plain_sample > 0:
+        plain = _guarded(plain_leg, mols, a, res)
+
+    # ---- CPU baseline: the reference's compiled int2e_sph + the FP64 port of its SCF on a
+    # bounded sample of the batch, on a pool of the host's cores; its energies also check the
+    # GPU results of the same molecules (FP64 oracle subset)
+    cpu = None
+    if rank == 0 and not a.no_cpu and a.cpu_sample > 0:
+        cpu = _guarded(cpu_leg, a, res, parity)
 
     if rank == 0:
         out = {
