@@ -325,9 +325,14 @@ def main():
     ap.add_argument("--grad", type=int, default=None,
                     help="also time the nuclear gradient (b2_grad) of the first N converged molecules "
                          "(0: off; default 512, or off with --profile-mode)")
+    ap.add_argument("--config2-only", action="store_true",
+                    help="only the single-molecule level-3 report (for per-kernel ncu captures)")
     a = ap.parse_args()
     if a.impl == "reference":
         return run_reference(a)
+    if a.config2_only:
+        print(json.dumps({"config2": config2_report()}))
+        return None
 
     import torch
     import torch.distributed as dist
