@@ -56,9 +56,25 @@ template <> __device__ __forceinline__ void b2_inv_rsqrt<float>(float t, float &
 }
 #endif
 
+// float32 F_0 alone (the (ss|ss) class) from the error function instead of the table:
+// F_0(T) = sqrt(pi)/2 erf(sqrt T) / sqrt T, one hardware reciprocal square root and erff
+// (relative error a few 1e-7, like the table path) and no table reads
+template <typename T> struct B2BoysErfF0 { static constexpr bool value = false; };
+template <> struct B2BoysErfF0<float> { static constexpr bool value = true; };
+
 // F[0..L] at T; `table` is the table in double (float64 kernels) or float (float32 kernels).
 template <typename T, int L, typename TT>
 B2_HD void b2_boys(T t, const TT *__restrict__ table, T *F) {
+  if constexpr (L == 0 && B2BoysErfF0<T>::value) {
+    if (t < (T)1e-6) {                                // F_0 = 1 - T/3 + T^2/10 - ...
+      F[0] = (T)1 - t * (T)(1.0 / 3.0);
+    } else {
+      T inv, rt;                                      // 1 / T, 1 / sqrt(T)
+      b2_inv_rsqrt<T>(t, inv, rt);
+      F[0] = (T)0.886226925452758014 * rt * erf(t * rt);
+    }
+    return;
+  }
   if (t < (T)B2_BOYS_TMAX) {
     int k = (int)(t * (T)B2_BOYS_INV_DT + (T)0.5);
     T dt = (T)(k * B2_BOYS_DT) - t;           // T_k - T

@@ -8,7 +8,8 @@
 // the reciprocal square root count one each (special-function unit); operations whose operands
 // are compile-time constants of the template (the zeros and ones the class's angular momenta fix)
 // are folded, as the compiler folds them, and not counted; comparisons and index arithmetic are
-// not counted.  The Boys function is counted on its table branch (T < 40), the common one.
+// not counted.  The Boys function is counted on its table branch (T < 40), the common one, and
+// F_0 alone on its error-function branch (erf counts as one special function).
 #include <cstdio>
 #include <cmath>
 #include "eri_sq.cuh"
@@ -58,9 +59,11 @@ inline bool operator==(CF a, CF b) { return a.v == b.v; }
 inline bool operator!=(CF a, CF b) { return a.v != b.v; }
 inline CF sqrt(CF a) { if (!a.k) ++g_special; CF c = a; c.v = std::sqrt(a.v); return c; }
 inline CF exp(CF a) { if (!a.k) ++g_special; CF c = a; c.v = std::exp(a.v); return c; }
+inline CF erf(CF a) { if (!a.k) ++g_special; CF c = a; c.v = std::erf(a.v); return c; }
 
-// the float32 kernels' Taylor length of the Boys table branch
+// the float32 kernels' Taylor length of the Boys table branch, and their error-function F_0
 template <> struct B2BoysTerms<CF> { static constexpr int n = B2BoysTerms<float>::n; };
+template <> struct B2BoysErfF0<CF> { static constexpr bool value = B2BoysErfF0<float>::value; };
 
 template <int LI, int LJ, int LK, int LL>
 static void count(long long &fl, long long &sp) {
