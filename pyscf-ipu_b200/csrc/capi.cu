@@ -105,6 +105,7 @@ static void b2_subset_free(B2PlanDev *P) {
 static void b2_plan_free(B2PlanDev *P) {
   if (!P) return;
   for (int b = 0; b < B2_NBKT; ++b) if (P->bkt_stream[b]) cudaStreamSynchronize(P->bkt_stream[b]);
+  if (P->jk_stream) cudaStreamSynchronize(P->jk_stream);
   b2_subset_free(P);
   b2_grid_free(*P);
   b2_dfree(P->mols); b2_dfree(P->row_off); b2_dfree(P->shells); b2_dfree(P->pinfo);
@@ -115,6 +116,8 @@ static void b2_plan_free(B2PlanDev *P) {
   b2_dfree(P->sv_off); b2_dfree(P->sv_work); b2_dfree(P->bkt_map);
   for (int b = 0; b < B2_NBKT; ++b) if (P->bkt_stream[b]) cudaStreamDestroy(P->bkt_stream[b]);
   for (int b = 0; b <= B2_NBKT; ++b) if (P->bkt_ev[b]) cudaEventDestroy(P->bkt_ev[b]);
+  if (P->jk_stream) cudaStreamDestroy(P->jk_stream);
+  for (int k = 0; k < 2; ++k) if (P->jk_ev[k]) cudaEventDestroy(P->jk_ev[k]);
   delete P;
 }
 
@@ -166,6 +169,8 @@ static int b2_set_sv(B2PlanDev *P, B2Upload *u) {
   b2_buckets(P, all, P->bkt_map_h, P->bkt_off_h);
   for (int b = 0; b < B2_NBKT; ++b) B2_TRY(cudaStreamCreateWithFlags(&P->bkt_stream[b], cudaStreamNonBlocking));
   for (int b = 0; b <= B2_NBKT; ++b) B2_TRY(cudaEventCreateWithFlags(&P->bkt_ev[b], cudaEventDisableTiming));
+  B2_TRY(cudaStreamCreateWithFlags(&P->jk_stream, cudaStreamNonBlocking));
+  for (int k = 0; k < 2; ++k) B2_TRY(cudaEventCreateWithFlags(&P->jk_ev[k], cudaEventDisableTiming));
   return b2_upload(&P->bkt_map, P->bkt_map_h, u);
 }
 
@@ -499,10 +504,22 @@ int b2_scf_iterate(void *plan, const b2_scf_state *S, void *stream) {
                                S->Vxc, S->H, S->diffJK, S->ring_err, S->ring_h, S->bmat, S->diis_err, st);
   if (!rc) rc = b2_launch_eigh_density(P, a, S->iter, S->H, S->Linv, S->D, S->mo_energy, S->C, S->eig_ws,
                                        S->sweeps, st);
+  // XC (issue-bound, on the bucket streams forked from st) and J/K (HBM-bound) both read only the
+  // new density: J/K runs beside XC on the plan's J/K stream, forked after the eigensolver and
+  // joined before the energies
+  cudaStream_t js = P.jk_stream ? P.jk_stream : st;
+  if (!rc && js != st) {
+    rc = b2_note(cudaEventRecord(P.jk_ev[0], st));
+    if (!rc) rc = b2_note(cudaStreamWaitEvent(js, P.jk_ev[0], 0));
+  }
   if (!rc) rc = S->ao ? b2_launch_xc(P, S->precision, a, S->ao, S->weights, S->D, S->Vxc, S->exc, st)
                       : b2_launch_xc_direct(P, S->precision, a, S->coords, S->weights, S->D, S->Vxc, S->exc, st);
-  if (!rc) rc = S->exch ? b2_launch_jk_symv(P, S->precision, a, S->eri, S->exch, S->D, S->J, S->K, P.sv_work, st)
-                        : b2_launch_jk_s8(P, S->precision, a, S->eri, S->D, S->J, S->K, st);
+  if (!rc) rc = S->exch ? b2_launch_jk_symv(P, S->precision, a, S->eri, S->exch, S->D, S->J, S->K, P.sv_work, js)
+                        : b2_launch_jk_s8(P, S->precision, a, S->eri, S->D, S->J, S->K, js);
+  if (!rc && js != st) {
+    rc = b2_note(cudaEventRecord(P.jk_ev[1], js));
+    if (!rc) rc = b2_note(cudaStreamWaitEvent(st, P.jk_ev[1], 0));
+  }
   if (!rc) rc = b2_launch_energy_jk(P, a, S->D, S->Hcore, S->J, S->K, S->hyb, S->exc, S->enuc, S->diffJK,
                                     S->energy, S->iter, st);
   return rc;

@@ -71,6 +71,8 @@ struct B2PlanDev {
   std::vector<int> bkt_off_h;             // B2_NBKT + 1 bucket starts in bkt_map
   cudaStream_t bkt_stream[B2_NBKT] = {};  // per-bucket streams (forked from / joined to the caller's)
   cudaEvent_t bkt_ev[B2_NBKT + 1] = {};
+  cudaStream_t jk_stream = nullptr;       // J/K beside XC in an SCF iteration (forked / joined)
+  cudaEvent_t jk_ev[2] = {};
 };
 
 int b2_launch_eri_s8(B2PlanDev &P, int precision, void *out, cudaStream_t st);
