@@ -43,7 +43,8 @@ def _peaks():
 
 
 def _tensor_peak(sustained=True):
-    """bf16 dense peak: the sustained figure for a kernel timed inside a long SCF step"""
+    """bf16 dense peak: the sustained figure for a kernel timed inside a long step, the burst
+    figure for a kernel timed alone"""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         d = json.load(open(p))
@@ -85,8 +86,9 @@ def kernel_rooflines(eng, precision):
     CUDA events around repeated calls of the entry the SCF uses (after the timed region, same
     batch and data):
       * XC (k_xc_tq, tensor bound): algorithmic flops 4 G N^2 per molecule (the rho and V_xc
-        contractions, N = nao unpadded) against the measured sustained bf16 dense peak; the
-        operands are split tf32 (nominal tf32 rate = half the bf16 rate).
+        contractions, N = nao unpadded) against the measured burst bf16 dense peak (the calls are
+        timed alone, back to back); the operands are split tf32 (nominal tf32 rate = half the
+        bf16 rate).
       * J/K (k_symv, HBM bound): algorithmic bytes n4 x 4 B per molecule (the s8 list read once,
         D/J/K on chip) against the measured HBM copy rate.
       * ERI (k_eri_*, float32 SIMT): shell and primitive quartets per second.
@@ -94,7 +96,7 @@ def kernel_rooflines(eng, precision):
     from b200dft._lib import lib, check, ptr, stream_handle
     P = eng.plan
     hbm, hbm_kind = _peaks()
-    tpk, tkind = _tensor_peak(sustained=True)
+    tpk, tkind = _tensor_peak(sustained=False)     # the kernel is timed alone (back-to-back calls)
     rbytes = 4 if precision == "mixed" else 8
     out = []
     G = np.diff(P.grid_off).astype(np.float64)
