@@ -457,6 +457,15 @@ def main():
     e2e = None
     if not a.profile_mode:
         from b200dft.engine import run_batches
+        from b200dft._lib import lib as _lib
+        # start from a clean device: the legs before (the float64 parity engine's 29 GB of lists)
+        # leave blocks in torch's cache that the plans' own memory would otherwise have to
+        # reclaim mid-run (synchronising the device)
+        import gc
+        gc.collect()
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        _lib().b2_release_cached_memory()
         kw = dict(level=a.level, precision=a.precision, guess=a.guess, net=net)
         for _ in run_batches([mols] * max(1, min(a.warmup, 2)), **kw):
             pass
