@@ -883,8 +883,8 @@ k_xc_tq(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
       if (qq == 0 && valid) e_part += (double)rho[0] * wd * (double)ex;
       const float rt0 = vrho * 0.5f * wp, f4 = 4.f * vg * wp;
       const float rt1 = f4 * rho[1], rt2 = f4 * rho[2], rt3 = f4 * rho[3];
-      // ---- Y_n = AO_n rt0 + grad AO_n . rt -> Y^T tiles (AO values re-read from the T tile: the
-      //      Y^T tiles overwrite the N tile, which the X product has finished reading)
+      // ---- Y_n = AO_n rt0 + grad AO_n . rt -> Y^T tiles (AO values from registers; the Y^T
+      //      tiles overwrite the N tile, which the X product has finished reading)
 #pragma unroll
       for (int j4 = 0; j4 < Q; ++j4) {
         const int n0 = nq0 + 4 * j4;
@@ -893,15 +893,9 @@ k_xc_tq(const B2MolDev *__restrict__ mols, const B2Shell *__restrict__ shells,
         b2_tmem_ld4(tl + colA + NB + n0, b2);
         b2_tmem_ld4(tl + colA + 2 * NB + n0, b3);
         b2_tmem_wait_ld();
-        float av[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-          const int ti = b2_tt_idx(NB, n0 + u, p >> 2) + (p & 3);
-          av[u] = sTh[ti] + sTl[ti];
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const float y = av[u] * rt0 + __uint_as_float(b1[u]) * rt1 + __uint_as_float(b2[u]) * rt2 +
+          const float y = a0[4 * j4 + u] * rt0 + __uint_as_float(b1[u]) * rt1 + __uint_as_float(b2[u]) * rt2 +
                           __uint_as_float(b3[u]) * rt3;
           float yh, yl;
           b2_split_rn(y, yh, yl);
