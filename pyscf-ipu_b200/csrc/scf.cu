@@ -249,12 +249,32 @@ k_fock_diis(const B2MolDev *__restrict__ mols, const int *__restrict__ active,
   emax = b2_block_max(emax, red);
   __syncthreads();
   const int nfill = min(it + 1, nd);
-  for (int k = 0; k < nd; ++k) {
-    double s = 0;
-    if (k < nfill)
-      for (int e = threadIdx.x; e < NN; e += blockDim.x) s += er[(long long)k * NN + e] * sT[e];
-    s = b2_block_sum(s, red);
-    if (threadIdx.x == 0) stmp[k] = (k < nfill) ? s : 0.0;
+  // the nine dot products <err_k, err_new> in one pass and one reduction (each thread's partial
+  // sums, the warp shuffles and the sum over warps add in the same order as nine block sums)
+  {
+    __shared__ double red9[9][8];                   // 256 threads: 8 warps
+    double s9[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) s9[k] = 0.0;
+    for (int e = threadIdx.x; e < NN; e += blockDim.x) {
+      const double t = sT[e];
+#pragma unroll
+      for (int k = 0; k < 9; ++k)
+        if (k < nfill) s9[k] += er[(long long)k * NN + e] * t;
+    }
+    const int w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      double v = s9[k];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+      if ((threadIdx.x & 31) == 0) red9[k][w] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < nd) {
+      double sum = 0;
+      for (int i = 0; i < nw; ++i) sum += red9[threadIdx.x][i];
+      stmp[threadIdx.x] = (threadIdx.x < nfill) ? sum : 0.0;
+    }
   }
   __syncthreads();
   if (threadIdx.x < 32) {
