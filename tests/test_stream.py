@@ -190,7 +190,8 @@ def test_run_batches_order_and_prefetch_points(monkeypatch, prefetch):
     out = list(engine.run_batches(iter(batches), guess="minao", prefetch=prefetch, e_tol=1e-7))
     assert [m for m, _ in out] == batches                       # in order, one result per batch
     assert [float(r["energy"][0]) for _, r in out] == [0, 1, 2, 3, 4]
-    assert all(r["kw"] == {"e_tol": 1e-7} and "plan_wait" in r["host_ms"] for _, r in out)
+    # run_kw reaches each batch's SCF, with eager iterations unless the caller asks for a graph
+    assert all(r["kw"] == {"e_tol": 1e-7, "graph": False} and "plan_wait" in r["host_ms"] for _, r in out)
     assert all(r["gradient"] is False for _, r in out)
     plans = [e for e in log if e[0] == "plan"]
     assert [e[1] for e in plans] == [0, 1, 2, 3, 4]
@@ -206,7 +207,8 @@ def test_run_batches_order_and_prefetch_points(monkeypatch, prefetch):
 def test_run_batches_passes_gradient(monkeypatch):
     engine, _ = _fake_engine(monkeypatch)
     out = list(engine.run_batches(iter([[0], [1]]), guess="minao", gradient=True, e_tol=1e-7))
-    assert [r["gradient"] for _, r in out] == [True, True] and out[0][1]["kw"] == {"e_tol": 1e-7}
+    assert [r["gradient"] for _, r in out] == [True, True]
+    assert out[0][1]["kw"] == {"e_tol": 1e-7, "graph": False}
 
 
 def test_run_batches_empty_and_plan_errors(monkeypatch):
