@@ -3,8 +3,9 @@ their slots while the others keep iterating.
 
 ``run_batches`` (engine.py) holds a batch until its slowest molecule has converged, so the last
 iterations of every batch run with most slots empty.  Here a batch of ``slots`` molecules
-iterates (one captured CUDA graph per iteration, as ``RKSEngine.run_converged``) until at most
-``refill_at`` of them are still active; then
+iterates (the SCF step of ``RKSEngine.run_converged``: eager launches, or with ``graph`` one
+captured CUDA graph replayed per iteration) until at most ``refill_at`` of them are still active;
+then
 
   * the molecules that converged (or reached ``max_its``) retire: their results go to the host;
   * the molecules still iterating are carried into a new plan, first, with their whole SCF state
@@ -172,9 +173,9 @@ def _capture(r, use_diis):
     r.graph = g
 
 
-def _iterate(r, stop_at, max_its, e_tol, diis_tol, use_diis, rise, fallback_window):
-    """iterate (graph replays) until at most ``stop_at`` molecules are active; molecules that
-    reach ``max_its`` stop as unconverged"""
+def _iterate(r, stop_at, max_its, e_tol, diis_tol, use_diis, rise, fallback_window, graph=False):
+    """iterate (eager steps, or graph replays) until at most ``stop_at`` molecules are active;
+    molecules that reach ``max_its`` stop as unconverged"""
     eng = r.eng
     nm = eng.plan.nmol
     its_run = 0
@@ -182,10 +183,13 @@ def _iterate(r, stop_at, max_its, e_tol, diis_tol, use_diis, rise, fallback_wind
         n_act = int(eng.active.sum().item())
         if n_act == 0 or n_act <= stop_at:
             return its_run
-        if r.graph is None:
-            _capture(r, use_diis)
-        r.graph.replay()
-        eng.graph_replays += 1
+        if graph:
+            if r.graph is None:
+                _capture(r, use_diis)
+            r.graph.replay()
+            eng.graph_replays += 1
+        else:
+            eng.step(use_diis)
         its_run += 1
         act = eng.active > 0
         e = eng.energy.view(nm, 5)[:, 0]
@@ -236,13 +240,14 @@ def _retire(r, mols_by_id, done_mask):
 
 def run_refill(molecules, slots=4096, level=0, precision="mixed", guess="learned", net=None,
                refill_at=0.3, max_its=40, e_tol=1e-6, diis_tol=1e-4, use_diis=True, fallback=True,
-               rise=3.0, fallback_window=5, eri_threshold=0.0):
+               rise=3.0, fallback_window=5, eri_threshold=0.0, graph=False):
     """SCF of every molecule of the iterable ``molecules`` with ``slots`` molecules resident on
     the GPU at a time; whenever at most ``refill_at`` of the slots are still iterating, the
     retired slots are refilled from the stream.  Yields ``(ids, mols, result)`` per refill:
     stream indices, molecules and host arrays of the retired molecules (energy, iterations
     (-1: not converged within ``max_its``), converged, mo_energy, diis_err, last5, fell_back,
-    its_run, host_ms)."""
+    its_run, host_ms).  Every refill makes a new plan, so the SCF steps run eager unless ``graph``
+    (a captured graph then serves one plan's iterations)."""
     if guess == "learned" and net is None:
         from .train_guess import load
         net = load()
@@ -275,7 +280,7 @@ def run_refill(molecules, slots=4096, level=0, precision="mixed", guess="learned
         # molecules) so the last iterations launch only their work; small batches drain in place
         nm = r.eng.plan.nmol
         stop_at = int(refill_at * (nm if exhausted else slots)) if (not exhausted or nm > 64) else -1
-        n = _iterate(r, stop_at, max_its, e_tol, diis_tol, use_diis, rise, fallback_window)
+        n = _iterate(r, stop_at, max_its, e_tol, diis_tol, use_diis, rise, fallback_window, graph)
         t_iter = time.perf_counter() - th
         act = r.eng.active.cpu().numpy() > 0
         got = _retire(r, mols_by_id, ~act)
