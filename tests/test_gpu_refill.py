@@ -11,8 +11,9 @@ from b200dft.refill import run_refill
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("guess", ["minao", "learned"])
-def test_refill_matches_whole_batches(cuda, guess):
+@pytest.mark.parametrize("guess,graph", [("minao", False), ("learned", False), ("learned", True)])
+def test_refill_matches_whole_batches(cuda, guess, graph):
+    # eager SCF steps (the default) and one captured graph per refill plan give the same results
     mols = [Mole(s) for s in config3_batch(320, seed=5)]
     ref = np.zeros(len(mols))
     rconv = np.zeros(len(mols), bool)
@@ -24,7 +25,7 @@ def test_refill_matches_whole_batches(cuda, guess):
     got = np.full(len(mols), np.nan)
     conv = np.zeros(len(mols), bool)
     refills = 0
-    for ids, ms, out in run_refill(iter(mols), slots=96, refill_at=0.5, guess=guess):
+    for ids, ms, out in run_refill(iter(mols), slots=96, refill_at=0.5, guess=guess, graph=graph):
         got[ids] = out["energy"]
         conv[ids] = out["converged"]
         assert all(mols[i] is m for i, m in zip(ids, ms))
