@@ -12,6 +12,13 @@
 template <typename T>
 struct B2XcPoint { T exc, vrho, vgamma; };
 
+// a / b: exact for float64; for float32 on the GPU the two-instruction approximate division
+// (2 ulp; the functional's denominators stay far inside its range)
+template <typename T> B2_HD T b2x_div(T a, T b) { return a / b; }
+#ifdef __CUDA_ARCH__
+template <> __device__ __forceinline__ float b2x_div<float>(float a, float b) { return __fdividef(a, b); }
+#endif
+
 // Exchange part (0.08 Slater + 0.72 B88) and correlation parts (0.19 VWN, 0.81 LYP);
 // b2_b3lyp_point is their sum.  The split lets several threads share one grid point.
 template <typename T>
@@ -20,7 +27,7 @@ B2_HD B2XcPoint<T> b2_b3lyp_x(T r0, T r1, T r2, T r3) {
   const T gx = r1 + r1, gy = r2 + r2, gz = r3 + r3;
   const T sig = gx * gx + gy * gy + gz * gz + (T)1e-20;
   const T lr = log(rho);
-  const T inv_rho = (T)1 / rho;
+  const T inv_rho = b2x_div<T>((T)1, rho);
 
   // --- Slater * 0.08: e = -exp(log(rho)/3 - 0.30305460484554375); d(rho e)/drho = 4/3 e
   const T e_lda = (T)-0.08 * exp(lr * (T)(1.0 / 3.0) - (T)0.30305460484554375);
@@ -42,15 +49,15 @@ B2_HD B2XcPoint<T> b2_b3lyp_x(T r0, T r1, T r2, T r3) {
   const T x = sqrt(x2);
   const T ash = asinh(x);
   const T Dn = (T)1 + (T)6 * d * x * ash;
-  const T Dnp = (T)6 * d * (ash + x / sqrt((T)1 + x2));
-  const T h = x2 / Dn;
+  const T Dnp = (T)6 * d * (ash + b2x_div<T>(x, sqrt((T)1 + x2)));
+  const T h = b2x_div<T>(x2, Dn);
   const T E_b88 = c3 * n43 - (T)2 * d * n43 * h;
-  const T hmxh = x2 * (x * Dnp - Dn) / (Dn * Dn);
-  const T hpx = ((T)2 * Dn - x * Dnp) / (Dn * Dn);
+  const T hmxh = b2x_div<T>(x2 * (x * Dnp - Dn), Dn * Dn);
+  const T hpx = b2x_div<T>((T)2 * Dn - x * Dnp, Dn * Dn);
   const T dEdn = (T)(4.0 / 3.0) * c3 * n13 - (T)(8.0 / 3.0) * d * n13 * hmxh;
   const T e_b88 = (T)0.72 * E_b88;
   const T v_b88 = (T)0.72 * (T)0.5 * dEdn;
-  const T g_b88 = (T)0.72 * (-d * (T)0.25 * hpx / n43);
+  const T g_b88 = (T)0.72 * b2x_div<T>(-d * (T)0.25 * hpx, n43);
 
   B2XcPoint<T> o;
   o.exc = e_lda + e_b88 * inv_rho;
@@ -66,7 +73,7 @@ B2_HD B2XcPoint<T> b2_b3lyp_vwn(T r0, T r1, T r2, T r3) {
   const T sig = gx * gx + gy * gy + gz * gz + (T)1e-20;
   const T lr = log(rho);
   const T rho13 = exp(lr * (T)(1.0 / 3.0));
-  const T inv_rho = (T)1 / rho;
+  const T inv_rho = b2x_div<T>((T)1, rho);
 
   // --- VWN * 0.19: vwn(n) = n p1 G(s), s = (3/(4 pi n))^{1/6}
   //     G = log s + f [ log(s^2+p2 s+p3)/2 - (1/f+1) log(s-p0) ] + pre atan(c/(2s+p2))
@@ -80,10 +87,11 @@ B2_HD B2XcPoint<T> b2_b3lyp_vwn(T r0, T r1, T r2, T r3) {
   const T s = exp(log_s);
   const T X = s * s + p2 * s + p3;
   const T den = (T)2 * s + p2;
-  const T z = c / den;
+  const T z = b2x_div<T>(c, den);
   const T G = log_s + f * ((T)0.5 * log(X) - (T)(1.0 / -1.0311676086789439 + 1.0) * log(s - p0)) + pre * atan(z);
-  const T Gp = (T)1 / s + f * (den / ((T)2 * X) - (T)(1.0 / -1.0311676086789439 + 1.0) / (s - p0)) +
-               pre * ((T)-2 * c / (den * den)) / ((T)1 + z * z);
+  const T Gp = b2x_div<T>((T)1, s) +
+               f * (b2x_div<T>(den, (T)2 * X) - b2x_div<T>((T)(1.0 / -1.0311676086789439 + 1.0), s - p0)) +
+               pre * b2x_div<T>(b2x_div<T>((T)-2 * c, den * den), (T)1 + z * z);
   const T e_vwn = (T)0.19 * rho * p1 * G;                      // per volume
   const T v_vwn = (T)0.19 * p1 * (G - s * (T)(1.0 / 6.0) * Gp);
 
@@ -101,15 +109,15 @@ B2_HD B2XcPoint<T> b2_b3lyp_lyp(T r0, T r1, T r2, T r3) {
   const T sig = gx * gx + gy * gy + gz * gz + (T)1e-20;
   const T lr = log(rho);
   const T rho13 = exp(lr * (T)(1.0 / 3.0));
-  const T inv_rho = (T)1 / rho;
+  const T inv_rho = b2x_div<T>((T)1, rho);
 
   // --- LYP * 0.81: t = n^{-1/3}, P = 1/(1 + D t), w = exp(-C t) P, dl = t (C + D P)
   //     R = -A n P - A B CF w n + (A B / 72) w sigma n^{-5/3} (3 + 7 dl)
   //     P' = D P^2 t/(3n), w' = w dl/(3n), dl' = (D^2 P^2 t^2 - dl)/(3n)
   const T A = (T)0.04918, B = (T)0.132, C = (T)0.2533, D = (T)0.349;
   const T CF = (T)2.8712340001881918;                 // 0.3 (3 pi^2)^{2/3}
-  const T t = (T)1 / rho13;
-  const T P = (T)1 / ((T)1 + D * t);
+  const T t = b2x_div<T>((T)1, rho13);
+  const T P = b2x_div<T>((T)1, (T)1 + D * t);
   const T w = exp(-C * t) * P;
   const T dl = t * (C + D * P);
   const T n53 = t * t * t * t * t;                     // rho^{-5/3}
