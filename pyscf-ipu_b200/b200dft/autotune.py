@@ -18,7 +18,7 @@ import numpy as np
 from ._lib import lib, check, ptr
 
 NBKT = 5
-CANDIDATES = (1, 2, 4, 8, 16, 32)
+CANDIDATES = (1, 2, 4, 8, 16, 32, 64)
 TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned.json")
 
 
