@@ -68,74 +68,6 @@ k_grad_dm(const B2MolDev *__restrict__ mols, const double *__restrict__ C, const
 //     (the latter by translation invariance) are reduced over the warp per quartet, the bra
 //     centres' once per task.
 // Same formulas as the serial b2g_canonical_quartet (grad_math.cuh), which the host build runs.
-struct B2gOp {                      // one recursion step: v[dst + m] from v[s1..], v[s2..], v[s3..]
-  short dst, s1, s2, s3;            // flat offsets (s2 / s3 < 0: term absent)
-  signed char dd, c1, c3, mmax;     // direction, integer factors of the s2 / s3 terms, last m
-};
-template <int LE, int LF, int L>
-struct B2gVrr {                     // the recursion for [e0|f0]^(m), e up to LE, f up to LF
-  static constexpr int NE = b2g_ncart(LE), NF = b2g_ncart(LF), SM = L + 1, SE = NF * SM;
-  static constexpr int NV = NE * SE;                        // doubles of v[e][f][m]
-  static constexpr int NOB = NE - 1;                        // bra steps: e = 1..NE-1, f = 0
-  static constexpr int NOK = (NF - 1) * NE;                 // ket steps: f = 1..NF-1, every e
-  static constexpr int NOP = NOB + NOK;
-  static constexpr int NACC = NE * NF;                      // (e, f) entries of the result
-  // step o of the table (bra steps by e, then ket steps by f with e inner: levels in order)
-  B2_HD static constexpr B2gOp op(int o) {
-    B2gOp r{};
-    r.s3 = -1;
-    r.c3 = 0;
-    if (o < NOB) {
-      const int ie = o + 1;
-      int ex = 0, ey = 0, ez = 0;
-      b2g_cart(ie, ex, ey, ez);
-      const int e[3] = {ex, ey, ez};
-      const int dd = ex ? 0 : (ey ? 1 : 2);
-      int e1[3] = {e[0], e[1], e[2]};
-      e1[dd]--;
-      r.dst = (short)(ie * SE);
-      r.s1 = (short)(b2g_cidx(e1[0], e1[1], e1[2]) * SE);
-      r.s2 = -1;
-      r.c1 = (signed char)e1[dd];
-      if (e1[dd] > 0) {
-        int e2[3] = {e1[0], e1[1], e1[2]};
-        e2[dd]--;
-        r.s2 = (short)(b2g_cidx(e2[0], e2[1], e2[2]) * SE);
-      }
-      r.dd = (signed char)dd;
-      r.mmax = (signed char)(L - (ex + ey + ez));
-    } else {
-      const int q = o - NOB, jf = 1 + q / NE, ie = q - (q / NE) * NE;
-      int fx = 0, fy = 0, fz = 0, ex = 0, ey = 0, ez = 0;
-      b2g_cart(jf, fx, fy, fz);
-      b2g_cart(ie, ex, ey, ez);
-      const int dd = fx ? 0 : (fy ? 1 : 2);
-      int f1[3] = {fx, fy, fz};
-      f1[dd]--;
-      const int j1 = b2g_cidx(f1[0], f1[1], f1[2]);
-      const int ec[3] = {ex, ey, ez};
-      r.dst = (short)(ie * SE + jf * SM);
-      r.s1 = (short)(ie * SE + j1 * SM);
-      r.s2 = -1;
-      r.c1 = (signed char)f1[dd];
-      if (f1[dd] > 0) {
-        int f2[3] = {f1[0], f1[1], f1[2]};
-        f2[dd]--;
-        r.s2 = (short)(ie * SE + b2g_cidx(f2[0], f2[1], f2[2]) * SM);
-      }
-      if (ec[dd] > 0) {
-        int e3[3] = {ex, ey, ez};
-        e3[dd]--;
-        r.s3 = (short)(b2g_cidx(e3[0], e3[1], e3[2]) * SE + j1 * SM);
-        r.c3 = (signed char)ec[dd];
-      }
-      r.dd = (signed char)dd;
-      r.mmax = (signed char)(L - (ex + ey + ez) - (fx + fy + fz));   // < 0: nothing to do
-    }
-    return r;
-  }
-};
-
 // v[e][f][m] of NCB primitive quartets at once (buffer c at v + c NV; v[0][0][m] already set),
 // lanes over (step, quartet) pairs level by level.  Quartet c's scalars: cs + c B2G_CS (W - P,
 // W - Q, rho/zeta, rho/eta, 1/(2 zeta), 1/(2 eta), 1/(2 (zeta + eta))) and its pair records

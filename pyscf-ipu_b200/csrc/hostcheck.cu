@@ -5,12 +5,14 @@
 #include "eri_sq.cuh"
 #include "grad_math.cuh"
 #include "xc_math.cuh"
+#include <algorithm>
 #include <vector>
 
-// The two-electron gradient kernel's traversal on the host: the float32 ERI work list (32 kets
-// per task, grouped by class combination), canonical quartets only, each lane's quartet through
-// b2g_canonical_quartet with the class its group fixes.  bad counts quartets whose shells do not
-// have the group's angular momenta.
+// The two-electron gradient kernels' traversal on the host: the float32 ERI work list (32 kets
+// per task, grouped by class combination), canonical quartets only, each quartet through the
+// serial b2g_canonical_quartet with the class its group fixes (the GPU kernels split the same
+// recursions over a warp's lanes; b2hc_grad_vrr_tables checks their step tables).  bad counts
+// quartets whose shells do not have the group's angular momenta.
 template <int G>
 static void b2hc_2e_group(const B2PlanHost &P, const std::vector<B2EriTask> &tasks, const std::vector<long long> &goff,
                           const double *D, double hyb, const double *tab, double *g, int *bad) {
@@ -36,6 +38,104 @@ static void b2hc_2e_group(const B2PlanHost &P, const std::vector<B2EriTask> &tas
     }
   }
   if constexpr (G < 15) b2hc_2e_group<G + 1>(P, tasks, goff, D, hyb, tab, g, bad);
+}
+
+// The GPU kernels' tabulated vertical recursion (B2gVrr, grad_math.cuh) run on the host: every
+// step of the table in order (an order the kernels' level-by-level lane split respects), summed
+// over the quartet's primitive quartets with the kernels' weights, against the serial b2g_e0f0
+// of the same quartet.  Returns the largest difference relative to max |entry|.
+template <int LE, int LF, bool KET>
+static double b2hc_vrr_table(const B2Shell &a, const B2Shell &b, const B2Shell &c, const B2Shell &d,
+                             const double *tab) {
+  using S = B2gVrr<LE, LF, LE + LF>;
+  constexpr int L = LE + LF, NW = KET ? 2 : 3;
+  double ser[NW][S::NE][S::NF];
+  b2g_e0f0<double, LE, LF, KET>(a, b, c, d, tab, ser);
+  std::vector<double> acc(NW * S::NACC, 0.0), v(S::NV, 0.0);
+  double AB2 = 0, CD2 = 0;
+  for (int x = 0; x < 3; ++x) {
+    AB2 += (a.R[x] - b.R[x]) * (a.R[x] - b.R[x]);
+    CD2 += (c.R[x] - d.R[x]) * (c.R[x] - d.R[x]);
+  }
+  for (int pa = 0; pa < a.nprim; ++pa)
+    for (int pb = 0; pb < b.nprim; ++pb) {
+      const double al = a.exp[pa], be = b.exp[pb], z = al + be;
+      double P[3], PA[3];
+      for (int x = 0; x < 3; ++x) {
+        P[x] = (al * a.R[x] + be * b.R[x]) / z;
+        PA[x] = P[x] - a.R[x];
+      }
+      const double Kab = exp(-al * be / z * AB2) * a.coef[pa] * b.coef[pb];
+      for (int pc = 0; pc < c.nprim; ++pc)
+        for (int pd = 0; pd < d.nprim; ++pd) {
+          const double ga = c.exp[pc], de = d.exp[pd], e = ga + de;
+          double Q[3], QC[3], WP[3], WQ[3], PQ2 = 0;
+          for (int x = 0; x < 3; ++x) {
+            Q[x] = (ga * c.R[x] + de * d.R[x]) / e;
+            QC[x] = Q[x] - c.R[x];
+            const double W = (z * P[x] + e * Q[x]) / (z + e);
+            WP[x] = W - P[x];
+            WQ[x] = W - Q[x];
+            PQ2 += (P[x] - Q[x]) * (P[x] - Q[x]);
+          }
+          const double rho = z * e / (z + e);
+          const double Kcd = exp(-ga * de / e * CD2) * c.coef[pc] * d.coef[pd];
+          const double pref = 34.98683665524972 / (z * e * sqrt(z + e)) * Kab * Kcd;
+          double F[L + 1];
+          b2_boys<double, L, double>(rho * PQ2, tab, F);
+          std::fill(v.begin(), v.end(), 0.0);
+          for (int m = 0; m <= L; ++m) v[m] = pref * F[m];
+          const double hb = 0.5 / z, rb = rho / z, hk = 0.5 / e, rk = rho / e, h3 = 0.5 / (z + e);
+          for (int o = 0; o < S::NOP; ++o) {
+            const B2gOp op = S::op(o);
+            if (op.mmax < 0) continue;
+            const bool bra = o < S::NOB;
+            const double X = bra ? PA[op.dd] : QC[op.dd], Y = bra ? WP[op.dd] : WQ[op.dd];
+            const double cc = (double)op.c1 * (bra ? hb : hk), r = bra ? rb : rk, c3 = (double)op.c3 * h3;
+            for (int m = 0; m <= op.mmax; ++m) {
+              double t = X * v[op.s1 + m] + Y * v[op.s1 + m + 1];
+              if (op.s2 >= 0) t += cc * (v[op.s2 + m] - r * v[op.s2 + m + 1]);
+              if (op.s3 >= 0) t += c3 * v[op.s3 + m + 1];
+              v[op.dst + m] = t;
+            }
+          }
+          const double w[3] = {1.0, KET ? 2 * ga : 2 * al, 2 * be};
+          for (int q = 0; q < NW; ++q)
+            for (int t = 0; t < S::NACC; ++t) {
+              const int ie = t / S::NF, jf = t % S::NF;
+              acc[q * S::NACC + t] += w[q] * v[ie * S::SE + jf * S::SM];
+            }
+        }
+    }
+  double big = 0, diff = 0;
+  for (int q = 0; q < NW; ++q)
+    for (int ie = 0; ie < S::NE; ++ie)
+      for (int jf = 0; jf < S::NF; ++jf) {
+        big = std::max(big, fabs(ser[q][ie][jf]));
+        diff = std::max(diff, fabs(ser[q][ie][jf] - acc[q * S::NACC + ie * S::NF + jf]));
+      }
+  return big > 0 ? diff / big : diff;
+}
+
+// every class combination G: both passes of the two-electron gradient (bra raised, ket raised)
+// on a fixed quartet of s / p shells with the class's angular momenta
+template <int G>
+static void b2hc_vrr_all(const double *tab, double *rel) {
+  B2Shell sh[4] = {};
+  const double R[4][3] = {{0.1, -0.2, 0.3}, {1.4, 0.5, -0.6}, {-0.9, 1.1, 0.8}, {0.7, -1.3, 1.9}};
+  const double ex[4][3] = {{5.0, 0.9, 0.25}, {3.1, 0.7, 0.2}, {7.2, 1.3, 0.35}, {2.2, 0.5, 0.15}};
+  const double cf[4][3] = {{0.15, 0.53, 0.44}, {0.2, 0.6, 0.35}, {0.1, 0.5, 0.5}, {0.3, 0.55, 0.3}};
+  for (int k = 0; k < 4; ++k) {
+    sh[k].l = b2g_group_l(G, k);
+    sh[k].nprim = 3;
+    sh[k].atom = k;
+    for (int x = 0; x < 3; ++x) sh[k].R[x] = R[k][x];
+    for (int p = 0; p < 3; ++p) { sh[k].exp[p] = ex[k][p]; sh[k].coef[p] = cf[k][p]; }
+  }
+  constexpr int LA = b2g_group_l(G, 0), LB = b2g_group_l(G, 1), LC = b2g_group_l(G, 2), LD = b2g_group_l(G, 3);
+  rel[2 * G] = b2hc_vrr_table<LA + LB + 1, LC + LD, false>(sh[0], sh[1], sh[2], sh[3], tab);
+  rel[2 * G + 1] = b2hc_vrr_table<LA + LB, LC + LD + 1, true>(sh[0], sh[1], sh[2], sh[3], tab);
+  if constexpr (G < 15) b2hc_vrr_all<G + 1>(tab, rel);
 }
 
 extern "C" {
@@ -275,6 +375,16 @@ int b2hc_b3lyp_f32(int n, const double *rho, double *exc, double *vrho, double *
     exc[g] = o.exc; vrho[g] = o.vrho; vgamma[g] = o.vgamma;
   }
   return B2_OK;
+}
+
+// the tabulated recursion of the GPU two-electron gradient kernels against the serial one, for
+// every class combination: rel[2 G] (bra raised) and rel[2 G + 1] (ket raised), each the largest
+// difference relative to the largest entry
+int b2hc_grad_vrr_tables(double *rel) {
+  std::vector<double> tab(B2_BOYS_NT * B2_BOYS_NM);
+  b2_boys_fill_table(tab.data());
+  b2hc_vrr_all<0>(tab.data(), rel);
+  return 0;
 }
 
 }  // extern "C"

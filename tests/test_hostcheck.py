@@ -140,10 +140,9 @@ def test_two_electron_gradient_vs_finite_differences():
 
 
 def test_two_electron_gradient_kernel_traversal():
-    """the GPU kernel's traversal of the two-electron gradient (canonical shell quartets of the
-    float32 ERI work list, degeneracy weights, symmetrised Gamma, class fixed by the task group;
-    the same lane code as k_grad_2e) equals the sum over all ordered quartets, molecule by
-    molecule in a batch"""
+    """the GPU kernels' traversal of the two-electron gradient (canonical shell quartets of the
+    float32 ERI work list, degeneracy weights, symmetrised Gamma, class fixed by the task group)
+    equals the sum over all ordered quartets, molecule by molecule in a batch"""
     hc = _hc()
     mols = [Mole("O 0 0 0.1173; H 0 0.7572 -0.4692; H 0 -0.7532 -0.4792"), Mole(methane(1.05)),
             Mole("N 0 0 0; C 0 0 2.6; O 2.1 0 3.9; H 0 1.9 -0.8", unit="Bohr")]
@@ -176,6 +175,17 @@ def test_two_electron_gradient_kernel_traversal():
                                _p(D, ctypes.c_double), ctypes.c_double(hyb), _p(ref, ctypes.c_double)) == 0
         np.testing.assert_allclose(g[a0:a0 + m.natm], ref, atol=1e-10 * max(1.0, np.abs(ref).max()), rtol=0)
         a0 += m.natm
+
+
+def test_two_electron_gradient_recursion_tables():
+    """the step tables the GPU two-electron gradient kernels split over a warp's lanes (target,
+    sources, direction, factors, last m of every Obara-Saika step), run in table order on the
+    host, give the serial recursion's weighted [e0|f0] sums for every class combination, with the
+    bra raised by one and with the ket raised by one"""
+    hc = _hc()
+    rel = np.full(32, np.nan)
+    assert hc.b2hc_grad_vrr_tables(_p(rel, ctypes.c_double)) == 0
+    assert np.all(rel < 1e-12), rel
 
 
 def test_one_electron_gradient_vs_finite_differences():
