@@ -104,9 +104,13 @@ def kernel_rooflines(eng, precision):
     flops = float((4.0 * G * N * N).sum())
     xc_ms = _timed(lambda: eng.xc(active=None), 5)
     tf = flops / (xc_ms / 1e3) / 1e12
+    # DRAM bytes per launch: the ncu capture of the NB = 64 bucket's launch on the 512-molecule
+    # batch (57.83 MB read + 0.19 MB written for 1 601 800 grid points: 36.2 B per point, the
+    # point's coordinates and weight plus its share of D and V), scaled by the batch's points
+    xc_traffic = 36.22 * float(G.sum()) if precision == "mixed" else None
     out.append({"kernel": "k_xc_tq (per-bucket persistent)" if precision == "mixed" else "k_xc_direct",
                 "bound": "tensor",
-                "achieved": tf, "peak": tpk, "unit": "TFLOP/s", "frac": tf / tpk, "traffic": None,
+                "achieved": tf, "peak": tpk, "unit": "TFLOP/s", "frac": tf / tpk, "traffic": xc_traffic,
                 "peak_kind": f"{tkind} bf16 dense (of measured)", "algorithmic_flops_per_launch": flops,
                 "ms_per_launch": xc_ms, "operands": "split tf32, fp32 accumulate"})
     eng.D.copy_(eng.D0)
