@@ -53,3 +53,22 @@ def test_reference_arm_other_ranks_exit_quietly():
     r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--impl", "reference", "--gpus", "2",
                         "--steps", "1", "--warmup", "0"], capture_output=True, text=True, timeout=300, cwd=root, env=env)
     assert r.returncode == 0 and not [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+
+
+def test_parity_eri_difference_skips_padding():
+    """max |dERI| of the parity leg covers each molecule's s8 entries and skips the padding to the
+    next 32-entry offset (never written by the kernels)"""
+    import types
+    import torch
+    plan = types.SimpleNamespace(eri_off=np.array([0, 32, 96]), nao=np.array([2, 3, 2], np.int32))
+    # n2 = 3, 6, 3 -> n4 = 6, 21, 6 entries per molecule
+    x = torch.zeros(128, dtype=torch.float32)
+    y = torch.zeros(128, dtype=torch.float64)
+    x[6:32] = 5.0                  # padding of molecule 0
+    x[32 + 21:96] = 7.0            # padding of molecule 1
+    x[96 + 6:] = 9.0               # past the last molecule
+    x[40] = 0.25                   # a real difference in molecule 1
+    y[100] = -0.5                  # and one in molecule 2
+    assert bench._max_abs_diff_lists(x, y, plan, step=50) == 0.5
+    y[100] = 0.0
+    assert bench._max_abs_diff_lists(x, y, plan, step=7) == 0.25
